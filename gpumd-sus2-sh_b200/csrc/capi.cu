@@ -1,0 +1,831 @@
+// Handle, CG-program compiler and the extern "C" entry points of sus2sh.h /
+// sus2sh_tools.h.
+#include "../../include/sus2sh.h"
+#include "../../include/sus2sh_tools.h"
+#include "engine.cuh"
+#include "mtp_model.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace sus2sh {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void resize(size_t count) {
+    if (count == n) return;
+    release();
+    if (count) ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    n = count;
+  }
+  void upload(const std::vector<T>& v) {
+    resize(v.size());
+    if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  }
+};
+
+// ---------------------------------------------------------------------------
+// CG program: the layered rows of the saved sh_products compiled to the
+// slot machine executed by k_product (see engine.cu for the row kinds).
+// Forward rows follow build_explicit_sh_graph_metadata's layers
+// (sus2_sh.cu:1913-2093); terminal scalar rows are fused into the energy and
+// seed their sources directly (terminal-scalar fusion, sus2_sh.cu:5674-5778,
+// 8149-8196); back rows are grouped by source per layer with duplicate
+// (target, other) terms merged (sus2_sh.cu:2050-2092, 8966-8981).
+// ---------------------------------------------------------------------------
+struct ProgramHost {
+  std::vector<uint32_t> code;
+  std::vector<double> coef;
+  int nrows = 0, nvalue = 0, nbasic = 0, ncanon = 0;
+  std::vector<int> basic_canon, canon_basic;
+  int terminal_rows = 0;
+};
+
+uint32_t header(int kind, size_t nt, int dst) {
+  if (nt >= (1u << 14)) throw InputError("SUS2_SH product row has too many terms for the program.");
+  return (static_cast<uint32_t>(kind) << 30) | (static_cast<uint32_t>(nt) << 16) |
+         static_cast<uint32_t>(dst);
+}
+
+uint32_t pack2(int a, int b) { return static_cast<uint32_t>(a) | (static_cast<uint32_t>(b) << 16); }
+
+ProgramHost compile_program(const HostModel& m, const Layered& lay) {
+  ProgramHost P;
+  const int M = m.moments, B = m.basic_count;
+  const int C = (m.l_max + 1) * (m.l_max + 1);
+  P.nbasic = B;
+  P.ncanon = m.k_max * C;
+  P.canon_basic.assign(P.ncanon, -1);
+  for (int b = 0; b < B; ++b) {
+    const int l = m.basic_l[b];
+    const int k = (m.basic_mu[b] - l) / (m.l_max + 1);
+    const int c = k * C + l * l + l + m.basic_m[b];
+    if (P.canon_basic[c] >= 0) throw InputError("SUS2_SH alpha_index_basic lists a (k,l,m) twice.");
+    P.canon_basic[c] = b;
+    P.basic_canon.push_back(c);
+  }
+  // weight of every moment = sum of its scalar coefficients
+  std::vector<double> weight(M, 0.0);
+  std::vector<char> is_scalar(M, 0);
+  for (int s = 0; s < m.scalar_count; ++s) {
+    weight[m.moment_mapping[s]] += m.moment_coeffs[s];
+    is_scalar[m.moment_mapping[s]] = 1;
+  }
+  std::vector<char> used(M, 0);
+  for (const Row& r : lay.rows)
+    for (size_t t = 0; t < r.left.size(); ++t) used[r.left[t]] = used[r.right[t]] = 1;
+  // value slots: basics, then non-terminal live targets in row order
+  std::vector<int> slot(M, -1);
+  for (int b = 0; b < B; ++b) slot[b] = b;
+  int nv = B;
+  for (const Row& r : lay.rows)
+    if (!lay.terminal[r.target] && (used[r.target] || is_scalar[r.target])) slot[r.target] = nv++;
+  P.nvalue = nv;
+  if (2 * nv >= 65536) throw InputError("SUS2_SH product graph exceeds 32767 live moments.");
+
+  auto emit = [&](int kind, int dst, const std::vector<int>& a, const std::vector<int>& b,
+                  const std::vector<double>& c) {
+    P.code.push_back(header(kind, a.size(), dst));
+    for (size_t t = 0; t < a.size(); ++t) {
+      P.code.push_back(pack2(a[t], b[t]));
+      P.coef.push_back(c[t]);
+    }
+    ++P.nrows;
+  };
+  // forward rows
+  for (const Row& r : lay.rows) {
+    if (slot[r.target] < 0) continue;
+    std::vector<int> a, b;
+    for (size_t t = 0; t < r.left.size(); ++t) {
+      a.push_back(slot[r.left[t]]);
+      b.push_back(slot[r.right[t]]);
+    }
+    emit(0, slot[r.target], a, b, r.coeff);
+  }
+  // terminal scalar rows: energy + seeds of their sources
+  for (const Row& r : lay.rows) {
+    if (!lay.terminal[r.target]) continue;
+    const double w = weight[r.target];
+    if (w == 0.0) continue;
+    std::vector<int> a, b;
+    std::vector<double> c;
+    for (size_t t = 0; t < r.left.size(); ++t) {
+      a.push_back(slot[r.left[t]]);
+      b.push_back(slot[r.right[t]]);
+      c.push_back(r.coeff[t] * w);
+    }
+    emit(1, 0, a, b, c);
+    ++P.terminal_rows;
+  }
+  // seeds of non-terminal scalars (basics included)
+  for (int mm = 0; mm < M; ++mm) {
+    if (!is_scalar[mm] || lay.terminal[mm] || weight[mm] == 0.0) continue;
+    emit(2, 0, {slot[mm]}, {0}, {weight[mm]});
+  }
+  // back rows, layers descending, grouped by source, duplicates merged
+  for (int layer = lay.max_layer; layer >= 1; --layer) {
+    std::map<int, std::vector<std::pair<std::pair<int, int>, double>>> by_src;
+    for (const Row& r : lay.rows) {
+      if (r.layer != layer || slot[r.target] < 0 || lay.terminal[r.target]) continue;
+      for (size_t t = 0; t < r.left.size(); ++t) {
+        by_src[r.left[t]].push_back({{r.target, r.right[t]}, r.coeff[t]});
+        by_src[r.right[t]].push_back({{r.target, r.left[t]}, r.coeff[t]});
+      }
+    }
+    for (auto& kv : by_src) {
+      std::vector<int> a, b;
+      std::vector<double> c;
+      std::map<std::pair<int, int>, size_t> seen;
+      for (auto& term : kv.second) {
+        auto it = seen.find(term.first);
+        if (it != seen.end()) {
+          c[it->second] += term.second;
+          continue;
+        }
+        seen[term.first] = c.size();
+        a.push_back(slot[term.first.first]);
+        b.push_back(slot[term.first.second]);
+        c.push_back(term.second);
+      }
+      emit(3, slot[kv.first], a, b, c);
+    }
+  }
+  return P;
+}
+
+// ---------------------------------------------------------------------------
+// box geometry
+// ---------------------------------------------------------------------------
+void invert3(const double* h, double* inv) {
+  const double det = h[0] * (h[4] * h[8] - h[5] * h[7]) - h[1] * (h[3] * h[8] - h[5] * h[6]) +
+                     h[2] * (h[3] * h[7] - h[4] * h[6]);
+  if (!(std::abs(det) > 0.0)) throw InputError("SUS2_SH box matrix is singular.");
+  const double id = 1.0 / det;
+  inv[0] = (h[4] * h[8] - h[5] * h[7]) * id;
+  inv[1] = (h[2] * h[7] - h[1] * h[8]) * id;
+  inv[2] = (h[1] * h[5] - h[2] * h[4]) * id;
+  inv[3] = (h[5] * h[6] - h[3] * h[8]) * id;
+  inv[4] = (h[0] * h[8] - h[2] * h[6]) * id;
+  inv[5] = (h[2] * h[3] - h[0] * h[5]) * id;
+  inv[6] = (h[3] * h[7] - h[4] * h[6]) * id;
+  inv[7] = (h[1] * h[6] - h[0] * h[7]) * id;
+  inv[8] = (h[0] * h[4] - h[1] * h[3]) * id;
+}
+
+// Cell grid with cells at least `cutoff` thick in every direction.
+int make_geometry(const double* h, const int* pbc, double cutoff, int N, BoxGeom& g) {
+  std::memcpy(g.h, h, sizeof(g.h));
+  invert3(h, g.hinv);
+  const double a[3] = {h[0], h[3], h[6]}, b[3] = {h[1], h[4], h[7]}, c[3] = {h[2], h[5], h[8]};
+  auto cross_norm = [](const double* u, const double* v) {
+    const double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2], z = u[0] * v[1] - u[1] * v[0];
+    return std::sqrt(x * x + y * y + z * z);
+  };
+  const double vol = std::abs(a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) +
+                              a[2] * (b[0] * c[1] - b[1] * c[0]));
+  const double thick[3] = {vol / cross_norm(b, c), vol / cross_norm(c, a), vol / cross_norm(a, b)};
+  long long total = 1;
+  for (int d = 0; d < 3; ++d) {
+    g.pbc[d] = pbc[d] ? 1 : 0;
+    int n = static_cast<int>(std::floor(thick[d] / cutoff));
+    n = std::max(1, std::min(n, 1024));
+    g.ncell[d] = n;
+    total *= n;
+  }
+  const long long limit = std::max<long long>(64, 4LL * N);
+  while (total > limit) {
+    int d = 0;
+    for (int e = 1; e < 3; ++e)
+      if (g.ncell[e] > g.ncell[d]) d = e;
+    total /= g.ncell[d];
+    g.ncell[d] = std::max(1, g.ncell[d] / 2);
+    total *= g.ncell[d];
+  }
+  for (int d = 0; d < 3; ++d) {
+    const double w = thick[d] / g.ncell[d];
+    int r = static_cast<int>(std::ceil(cutoff / w - 1e-12));
+    r = std::max(1, r);
+    if (!g.pbc[d]) r = std::min(r, std::max(1, g.ncell[d] - 1));
+    if (g.pbc[d] && r > 2)
+      throw InputError("SUS2_SH periodic box is thinner than half the neighbour cutoff (rc + skin).");
+    g.reach[d] = r;
+  }
+  for (int tx = -2; tx <= 2; ++tx)
+    for (int ty = -2; ty <= 2; ++ty)
+      for (int tz = -2; tz <= 2; ++tz) {
+        const int code = (tx + 2) * 25 + (ty + 2) * 5 + (tz + 2);
+        for (int k = 0; k < 3; ++k) g.shift[code][k] = tx * a[k] + ty * b[k] + tz * c[k];
+      }
+  return static_cast<int>(total);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// the handle
+// ---------------------------------------------------------------------------
+struct Engine {
+  HostModel model;
+  Options opt;
+  Layered lay;
+  ProgramHost prog;
+  bool use_float = true;
+  RadialSetup rs{};
+  std::vector<double> coef;        // [kmu][rb] unscaled
+  std::vector<double> pair_table;  // [S*S][stride]
+
+  // model on device
+  DevBuf<uint32_t> d_code;
+  DevBuf<float> d_coef_f;
+  DevBuf<double> d_coef_d;
+  DevBuf<int> d_basic_canon, d_canon_basic;
+  DevBuf<double> d_shift, d_species;
+  DevBuf<float> d_pair_f;
+  DevBuf<double> d_pair_d;
+
+  // per-size work
+  int N = 0, cap = 0, ncells = 0, cells_alloc = 0;
+  BoxGeom geom{};
+  BoxGeom* h_geom = nullptr;  // pinned staging
+  DevBuf<BoxGeom> d_geom;
+  double last_h[9] = {0};
+  int last_pbc[3] = {-1, -1, -1};
+  bool have_ref = false;
+  bool force_next = true;
+  int calls_since_build = 0;
+  DevBuf<double4> pos4, ref4;
+  DevBuf<int> nbr, ncount, cell_count, cell_start, cell_atoms, atom_cell, atom_rank;
+  DevBuf<unsigned char> Bbuf, Gbuf, scratch, ftmp;
+  DevBuf<Status> d_status;
+  Status* h_status = nullptr;  // pinned
+  cudaStream_t last_stream = nullptr;
+  size_t prod_smem = 0;
+  int prod_tile = 32;
+  bool prod_global = false;
+  // host-buffer path
+  DevBuf<double> io_pos, io_pe, io_f, io_vir, io_red;
+  DevBuf<int> io_type;
+  // forward state
+  int fwd_N = 0;
+
+  ~Engine() {
+    if (h_geom) cudaFreeHost(h_geom);
+    if (h_status) cudaFreeHost(h_status);
+  }
+
+  size_t elem() const { return use_float ? sizeof(float) : sizeof(double); }
+
+  void init(const char* path, int num_atoms, int nopts, const char** opts) {
+    model = load_model(path);
+    opt = parse_options(model, nopts, opts);
+    use_float = opt.use_float;
+    lay = layer_products(model);
+    prog = compile_program(model, lay);
+    if (!shape_supported(model.l_max, model.k_max, model.rb_size)) {
+      throw InputError("SUS2_SH engine has no compiled kernel for sh_l_max=" + std::to_string(model.l_max) +
+                       ", sh_k_max=" + std::to_string(model.k_max) +
+                       ", radial_basis_size=" + std::to_string(model.rb_size) + ".");
+    }
+    const int S = model.species_count, kmu = model.radial_funcs, rb = model.rb_size;
+    // radial tables: unscaled c[mu][n] uniform; per-pair (scal, shift) and
+    // the LK scale scaling*rtc[zi]*rtc[zj] (sus2_sh.cu:2484-2517)
+    coef = model.radial_coeffs;
+    rs.species = S;
+    rs.kmu = kmu;
+    rs.rb = rb;
+    rs.rational = model.radial_map == RadialMap::Rational;
+    rs.pair_stride = 2 * kmu + 1;
+    rs.rc = model.rc;
+    bool shared = true;
+    pair_table.assign(static_cast<size_t>(S) * S * rs.pair_stride, 0.0);
+    for (int zi = 0; zi < S; ++zi)
+      for (int zj = 0; zj < S; ++zj) {
+        const int pair = zi * S + zj;
+        double* row = &pair_table[static_cast<size_t>(pair) * rs.pair_stride];
+        for (int mu = 0; mu < kmu; ++mu) {
+          const int off = 2 * mu * S * S + S * zi + zj;
+          row[2 * mu] = model.scal_coeffs[off];
+          row[2 * mu + 1] = model.scal_coeffs[off + S * S];
+          if (row[2 * mu] != row[0] || row[2 * mu + 1] != row[1]) shared = false;
+        }
+        row[2 * kmu] = model.scaling * model.radial_type_coeffs[zi] * model.radial_type_coeffs[zj];
+      }
+    rs.shared_xi = shared;
+    if (opt.reference_rounding) {
+      // the reference's FP32 radial tables (sus2_sh.cu:2499-2512)
+      for (double& x : coef) x = static_cast<double>(static_cast<float>(x));
+      for (double& x : pair_table) x = static_cast<double>(static_cast<float>(x));
+    }
+    if (pair_table.size() > static_cast<size_t>(kMaxPairTable))
+      throw InputError("SUS2_SH radial pair table too large (species_count^2 * (2*radial_funcs+1) > 8192).");
+    // device uploads
+    d_code.upload(prog.code);
+    if (use_float) {
+      d_coef_f.upload(std::vector<float>(prog.coef.begin(), prog.coef.end()));
+      d_pair_f.upload(std::vector<float>(pair_table.begin(), pair_table.end()));
+    } else {
+      d_coef_d.upload(prog.coef);
+      d_pair_d.upload(pair_table);
+    }
+    d_basic_canon.upload(prog.basic_canon);
+    d_canon_basic.upload(prog.canon_basic);
+    d_shift.upload(model.shift_coeffs);
+    d_species.upload(model.species_coeffs);
+    ck(cudaMallocHost(&h_geom, sizeof(BoxGeom)), "cudaMallocHost");
+    ck(cudaMallocHost(&h_status, sizeof(Status)), "cudaMallocHost");
+    std::memset(h_status, 0, sizeof(Status));
+    d_geom.resize(1);
+    d_status.resize(1);
+    ck(cudaMemset(d_status.p, 0, sizeof(Status)), "cudaMemset");
+    // product kernel launch shape: lane = atom, slots in shared memory when
+    // they fit, else in an HBM scratch [slot][N]
+    const size_t per_atom = 2ull * prog.nvalue * elem();
+    int best_tile = 0, best_threads = 0;
+    for (int tile : {32, 64, 128}) {
+      const size_t bytes = per_atom * tile;
+      if (bytes > 227 * 1024) continue;
+      const int ctas = std::min<int>(static_cast<int>((227 * 1024) / bytes), 2048 / tile);
+      if (ctas * tile > best_threads) {
+        best_threads = ctas * tile;
+        best_tile = tile;
+      }
+    }
+    prod_global = best_tile == 0;
+    prod_tile = best_tile ? best_tile : 128;
+    prod_smem = per_atom * prod_tile;
+    if (num_atoms > 0) ensure_size(num_atoms);
+  }
+
+  void ensure_size(int n) {
+    if (n == N) return;
+    if (n <= 0 || n >= (1 << 24)) throw InputError("SUS2_SH engine supports 1 <= N < 16777216 atoms.");
+    if (last_stream) cudaStreamSynchronize(last_stream);
+    N = n;
+    const size_t nb = static_cast<size_t>(model.k_max) * (model.l_max + 1) * (model.l_max + 1);
+    pos4.resize(N);
+    ref4.resize(N);
+    ncount.resize(N);
+    atom_cell.resize(N);
+    atom_rank.resize(N);
+    cell_atoms.resize(N);
+    Bbuf.resize(nb * N * elem());
+    Gbuf.resize(nb * N * elem());
+    ftmp.resize(static_cast<size_t>(N) * (use_float ? sizeof(float4) : sizeof(double4)));
+    if (prod_global) scratch.resize(2ull * prog.nvalue * N * elem());
+    cap = 0;
+    nbr.release();
+    have_ref = false;
+    force_next = true;
+  }
+
+  template <typename T>
+  EdgeArgs<T> edge_args() const {
+    EdgeArgs<T> a{};
+    a.N = N;
+    a.cap = cap;
+    a.l_max = model.l_max;
+    a.k_max = model.k_max;
+    a.rs = rs;
+    a.pos4 = pos4.p;
+    a.nbr = nbr.p;
+    a.ncount = ncount.p;
+    a.pair_table = use_float ? static_cast<const void*>(d_pair_f.p) : static_cast<const void*>(d_pair_d.p);
+    a.shift = d_geom.p->shift;
+    for (size_t k = 0; k < coef.size(); ++k) a.coef[k] = static_cast<T>(coef[k]);
+    return a;
+  }
+
+  ProgramDev program_dev() const {
+    ProgramDev p{};
+    p.nrows = prog.nrows;
+    p.nvalue = prog.nvalue;
+    p.nbasic = prog.nbasic;
+    p.ncanon = prog.ncanon;
+    p.code = d_code.p;
+    p.coef = use_float ? static_cast<const void*>(d_coef_f.p) : static_cast<const void*>(d_coef_d.p);
+    p.basic_canon = d_basic_canon.p;
+    p.canon_basic = d_canon_basic.p;
+    return p;
+  }
+
+  // Positions -> pos4, conditional neighbour build.
+  void prepare(cudaStream_t s, int n, const double* h, const int* pbc, const int* type, const double* x) {
+    ensure_size(n);
+    last_stream = s;
+    bool box_changed = false;
+    for (int k = 0; k < 9; ++k) box_changed |= h[k] != last_h[k];
+    for (int k = 0; k < 3; ++k) box_changed |= (pbc[k] ? 1 : 0) != last_pbc[k];
+    const double cutoff = model.rc + opt.skin;
+    if (box_changed) {
+      ncells = make_geometry(h, pbc, cutoff, N, geom);
+      std::memcpy(last_h, h, sizeof(last_h));
+      for (int k = 0; k < 3; ++k) last_pbc[k] = pbc[k] ? 1 : 0;
+      if (ncells + 1 > cells_alloc) {
+        cell_count.resize(ncells + 1);
+        cell_start.resize(ncells + 1);
+        cells_alloc = ncells + 1;
+      }
+      // the pinned staging buffer may still feed an earlier queued copy
+      ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+      *h_geom = geom;
+      ck(cudaMemcpyAsync(d_geom.p, h_geom, sizeof(BoxGeom), cudaMemcpyHostToDevice, s), "geom upload");
+      force_next = true;
+    }
+    bool force = force_next;
+    if (opt.rebuild_interval > 0 && calls_since_build + 1 >= opt.rebuild_interval) force = true;
+    ck(cudaMemsetAsync(&d_status.p->maxdisp2_bits, 0, sizeof(unsigned int), s), "memset");
+    launch_pack(s, N, x, type, ref4.p, pos4.p, d_geom.p, have_ref ? 1 : 0, d_status.p);
+    const float half_skin2 = static_cast<float>(0.25 * opt.skin * opt.skin);
+    const double cutoff2 = cutoff * cutoff;
+    if (cap == 0) {
+      // first build: count pass, size the list, then fill
+      ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
+      launch_build(s, N, 1, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p, cell_start.p,
+                   cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nullptr, ncount.p, 0, 1, d_status.p);
+      Status st{};
+      ck(cudaMemcpyAsync(&st, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
+      ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+      grow_capacity(st.max_count);
+      force = true;
+    }
+    launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
+                 cell_start.p, cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
+                 d_status.p);
+    ck(cudaGetLastError(), "neighbour build launch");
+    have_ref = true;
+    force_next = false;
+    calls_since_build = force ? 0 : calls_since_build + 1;
+  }
+
+  void grow_capacity(int max_count) {
+    int c = static_cast<int>(std::ceil(max_count * 1.25)) + 8;
+    c = (c + 3) & ~3;
+    if (c <= cap) return;
+    cap = c;
+    nbr.resize(static_cast<size_t>(cap) * N);
+  }
+
+  template <typename T>
+  void forward_impl(cudaStream_t s, double* pe, int pe_assign) {
+    const EdgeArgs<T> a = edge_args<T>();
+    if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p)) != 0)
+      throw InputError("SUS2_SH basic kernel shape not compiled.");
+    launch_product<T>(s, N, program_dev(), pos4.p, reinterpret_cast<const T*>(Bbuf.p),
+                      reinterpret_cast<T*>(Gbuf.p),
+                      prod_global ? reinterpret_cast<T*>(scratch.p) : nullptr, prod_smem, prod_tile,
+                      d_shift.p, d_species.p, pe, pe_assign);
+  }
+
+  template <typename T>
+  void backward_impl(cudaStream_t s, const double* weight, double* force, double* virial, double sign) {
+    const EdgeArgs<T> a = edge_args<T>();
+    ck(cudaMemsetAsync(ftmp.p, 0, ftmp.n, s), "memset");
+    if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign) != 0)
+      throw InputError("SUS2_SH force kernel shape not compiled.");
+    launch_finalize<T>(s, N, ftmp.p, force, sign);
+  }
+
+  void finish(cudaStream_t s) {
+    ck(cudaMemcpyAsync(h_status, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
+    ck(cudaGetLastError(), "kernel launch");
+  }
+
+  void compute(cudaStream_t s, int n, const double* h, const int* pbc, const int* type, const double* x,
+               double* pe, double* f, double* vir) {
+    prepare(s, n, h, pbc, type, x);
+    if (use_float) {
+      forward_impl<float>(s, pe, 0);
+      backward_impl<float>(s, nullptr, f, vir, 1.0);
+    } else {
+      forward_impl<double>(s, pe, 0);
+      backward_impl<double>(s, nullptr, f, vir, 1.0);
+    }
+    finish(s);
+  }
+
+  int sync(int* flags) {
+    if (last_stream) ck(cudaStreamSynchronize(last_stream), "cudaStreamSynchronize");
+    else ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    int f = 0;
+    if (h_status->overflow) {
+      f |= SUS2SH_STATUS_OVERFLOW;
+      grow_capacity(h_status->max_count);
+      const int zero = 0;
+      ck(cudaMemcpy(&d_status.p->overflow, &zero, sizeof(int), cudaMemcpyHostToDevice), "status reset");
+      h_status->overflow = 0;
+      force_next = true;
+    }
+    if (flags) *flags = f;
+    return (f & SUS2SH_STATUS_OVERFLOW) ? SUS2SH_E_NEIGHBOR : SUS2SH_OK;
+  }
+};
+
+}  // namespace sus2sh
+
+struct sus2sh_handle {
+  sus2sh::Engine e;
+};
+
+using sus2sh::CudaError;
+using sus2sh::InputError;
+
+namespace {
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return SUS2SH_OK;
+  } catch (const InputError& ex) {
+    sus2sh::g_last_error = ex.what();
+    return SUS2SH_E_INPUT;
+  } catch (const CudaError& ex) {
+    sus2sh::g_last_error = ex.what();
+    return SUS2SH_E_CUDA;
+  } catch (const std::exception& ex) {
+    sus2sh::g_last_error = ex.what();
+    return SUS2SH_E_ARG;
+  }
+}
+
+bool check_box(const double* h, const int* pbc) {
+  if (!h || !pbc) {
+    sus2sh::g_last_error = "box_h and pbc must not be NULL";
+    return false;
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
+int sus2sh_is_sus2_sh_file(const char* path) {
+  return path && sus2sh::is_sus2_sh_file(path) ? 1 : 0;
+}
+
+int sus2sh_create(const char* path, int num_atoms, int nopts, const char** opts, sus2sh_handle** out) {
+  if (!path || !out) {
+    sus2sh::g_last_error = "sus2sh_create: NULL path or output handle";
+    return SUS2SH_E_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<sus2sh_handle> h(new sus2sh_handle());
+  const int rc = guarded([&] { h->e.init(path, num_atoms, nopts, opts); });
+  if (rc == SUS2SH_OK) *out = h.release();
+  return rc;
+}
+
+int sus2sh_compute(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3], const int* type,
+                   const double* position, double* potential, double* force, double* virial, void* stream) {
+  if (!h || !type || !position || !potential || !force || !virial || N <= 0) {
+    sus2sh::g_last_error = "sus2sh_compute: invalid argument";
+    return SUS2SH_E_ARG;
+  }
+  if (!check_box(box_h, pbc)) return SUS2SH_E_ARG;
+  return guarded([&] {
+    h->e.compute(static_cast<cudaStream_t>(stream), N, box_h, pbc, type, position, potential, force, virial);
+  });
+}
+
+int sus2sh_forward(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3], const int* type,
+                   const double* position, double* potential, void* stream) {
+  if (!h || !type || !position || !potential || N <= 0) {
+    sus2sh::g_last_error = "sus2sh_forward: invalid argument";
+    return SUS2SH_E_ARG;
+  }
+  if (!check_box(box_h, pbc)) return SUS2SH_E_ARG;
+  return guarded([&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->e.prepare(s, N, box_h, pbc, type, position);
+    if (h->e.use_float) h->e.forward_impl<float>(s, potential, 1);
+    else h->e.forward_impl<double>(s, potential, 1);
+    h->e.finish(s);
+    h->e.fwd_N = N;
+  });
+}
+
+int sus2sh_backward(sus2sh_handle* h, const double* grad_potential, double* grad_position, double* virial,
+                    void* stream) {
+  if (!h || !grad_position || h->e.fwd_N != h->e.N || h->e.N == 0) {
+    sus2sh::g_last_error = "sus2sh_backward: invalid argument or no matching forward";
+    return SUS2SH_E_ARG;
+  }
+  return guarded([&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int N = h->e.N;
+    sus2sh::ck(cudaMemsetAsync(grad_position, 0, sizeof(double) * 3 * N, s), "memset");
+    if (virial) sus2sh::ck(cudaMemsetAsync(virial, 0, sizeof(double) * 9 * N, s), "memset");
+    if (h->e.use_float) h->e.backward_impl<float>(s, grad_potential, grad_position, virial, -1.0);
+    else h->e.backward_impl<double>(s, grad_potential, grad_position, virial, -1.0);
+    h->e.finish(s);
+  });
+}
+
+int sus2sh_compute_host(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3], const int* type,
+                        const double* position, double* potential, double* force, double* virial_total,
+                        void* stream) {
+  if (!h || !type || !position || !potential || !force || N <= 0) {
+    sus2sh::g_last_error = "sus2sh_compute_host: invalid argument";
+    return SUS2SH_E_ARG;
+  }
+  if (!check_box(box_h, pbc)) return SUS2SH_E_ARG;
+  return guarded([&] {
+    sus2sh::Engine& e = h->e;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    e.io_pos.resize(3ull * N);
+    e.io_type.resize(N);
+    e.io_pe.resize(N);
+    e.io_f.resize(3ull * N);
+    e.io_vir.resize(9ull * N);
+    e.io_red.resize(10);
+    using sus2sh::ck;
+    ck(cudaMemcpyAsync(e.io_pos.p, position, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s), "H2D");
+    ck(cudaMemcpyAsync(e.io_type.p, type, sizeof(int) * N, cudaMemcpyHostToDevice, s), "H2D");
+    ck(cudaMemsetAsync(e.io_pe.p, 0, sizeof(double) * N, s), "memset");
+    ck(cudaMemsetAsync(e.io_f.p, 0, sizeof(double) * 3 * N, s), "memset");
+    ck(cudaMemsetAsync(e.io_vir.p, 0, sizeof(double) * 9 * N, s), "memset");
+    e.compute(s, N, box_h, pbc, e.io_type.p, e.io_pos.p, e.io_pe.p, e.io_f.p, e.io_vir.p);
+    sus2sh::launch_reduce(s, N, e.io_pe.p, e.io_vir.p, e.io_red.p);
+    ck(cudaMemcpyAsync(potential, e.io_pe.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s), "D2H");
+    ck(cudaMemcpyAsync(force, e.io_f.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s), "D2H");
+    if (virial_total) {
+      double red[10];
+      ck(cudaMemcpyAsync(red, e.io_red.p, sizeof(red), cudaMemcpyDeviceToHost, s), "D2H");
+      ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+      std::memcpy(virial_total, red + 1, 9 * sizeof(double));
+    } else {
+      ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+  });
+}
+
+void sus2sh_destroy(sus2sh_handle* h) {
+  if (!h) return;
+  if (h->e.last_stream) cudaStreamSynchronize(h->e.last_stream);
+  delete h;
+}
+
+double sus2sh_cutoff(const sus2sh_handle* h) { return h ? h->e.model.rc : 0.0; }
+
+const char* sus2sh_last_error(void) { return sus2sh::g_last_error.c_str(); }
+
+int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
+  if (!h) return SUS2SH_E_ARG;
+  int rc = SUS2SH_OK;
+  const int g = guarded([&] { rc = h->e.sync(status_flags); });
+  return g != SUS2SH_OK ? g : rc;
+}
+
+int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
+  if (!h || !out) return 0;
+  const sus2sh::Engine& e = h->e;
+  const int v[18] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+                     e.model.rb_size, e.model.basic_count, e.model.moments,
+                     static_cast<int>(e.model.products.size()), e.model.scalar_count,
+                     static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
+                     e.prog.nvalue, e.prog.nrows, e.model.standard_graph_matched ? 1 : 0,
+                     e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0};
+  const int k = std::min(n, 18);
+  for (int i = 0; i < k; ++i) out[i] = v[i];
+  return k;
+}
+
+// ---- tools -----------------------------------------------------------------
+int sus2sh_write_synthetic_model(const char* path, int species, int l_max, int k_max, int body_order,
+                                 const int* body_l_max, int n_body_l_max, int rb_size, double r_min, double rc,
+                                 int rational, const double* shift_coeffs, double radial_sigma,
+                                 double moment_sigma, double scal, double rshift, unsigned long long seed) {
+  if (!path || !shift_coeffs) return SUS2SH_E_ARG;
+  return guarded([&] {
+    sus2sh::SynthSpec sp;
+    sp.species = species;
+    sp.l_max = l_max;
+    sp.k_max = k_max;
+    sp.body_order = body_order;
+    sp.rb_size = rb_size;
+    sp.r_min = r_min;
+    sp.rc = rc;
+    sp.rational = rational;
+    if (body_l_max)
+      for (int i = 0; i < n_body_l_max; ++i) sp.body_l_max_list.push_back(body_l_max[i]);
+    sp.shift.assign(shift_coeffs, shift_coeffs + species);
+    sp.radial_sigma = radial_sigma;
+    sp.moment_sigma = moment_sigma;
+    sp.scal = scal;
+    sp.rshift = rshift;
+    sp.seed = seed;
+    sus2sh::write_synthetic_model(path, sp);
+  });
+}
+
+int sus2sh_standard_graph_counts(int l_max, int k_max, int body_order, const int* body_l_max, int n_body_l_max,
+                                 int* out) {
+  if (!out) return SUS2SH_E_ARG;
+  return guarded([&] {
+    std::vector<int> bl = sus2sh::default_body_l_max(l_max);
+    if (body_l_max)
+      for (int i = 0; i < n_body_l_max && 2 + i < 7; ++i) bl[2 + i] = body_l_max[i];
+    const sus2sh::StandardGraph g = sus2sh::build_standard_graph(l_max, k_max, body_order, bl);
+    out[0] = g.node_count;
+    out[1] = static_cast<int>(g.basic_k.size());
+    out[2] = static_cast<int>(g.products.size());
+    out[3] = static_cast<int>(g.scalars.size());
+    out[4] = g.tensor_blocks;
+    out[5] = g.cg_blocks;
+    out[6] = g.cg_terms;
+    out[7] = g.max_layer;
+  });
+}
+
+int sus2sh_md_kick_drift(int N, double dt, const double* inv_mass_type, const int* type, double* force,
+                         double* velocity, double* position, double* potential, double* virial, void* stream) {
+  sus2sh::launch_nve_kick_drift(static_cast<cudaStream_t>(stream), N, dt, inv_mass_type, type, force, velocity,
+                                position, potential, virial);
+  return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
+}
+
+int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* type, const double* force,
+                   double* velocity, void* stream) {
+  sus2sh::launch_nve_kick(static_cast<cudaStream_t>(stream), N, dt, inv_mass_type, type, force, velocity);
+  return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
+}
+
+int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream) {
+  sus2sh::launch_reduce(static_cast<cudaStream_t>(stream), N, potential, virial, out);
+  return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
+}
+
+int sus2sh_random_insertion(int N, double lx, double ly, double lz, double dmin, unsigned long long seed,
+                            double* position) {
+  if (N <= 0 || !position || !(dmin > 0.0)) return SUS2SH_E_ARG;
+  // grid of cells >= dmin; each cell holds few points
+  const int nx = std::max(1, static_cast<int>(lx / dmin)), ny = std::max(1, static_cast<int>(ly / dmin)),
+            nz = std::max(1, static_cast<int>(lz / dmin));
+  const double cx = lx / nx, cy = ly / ny, cz = lz / nz;
+  std::vector<std::vector<int>> cells(static_cast<size_t>(nx) * ny * nz);
+  std::mt19937_64 rng(seed);
+  std::uniform_real_distribution<double> U(0.0, 1.0);
+  const double d2 = dmin * dmin;
+  long long attempts = 0;
+  const long long budget = 2000LL * N + 1000000LL;
+  int placed = 0;
+  while (placed < N) {
+    if (++attempts > budget) return -5;
+    const double x = U(rng) * lx, y = U(rng) * ly, z = U(rng) * lz;
+    const int ix = std::min(nx - 1, static_cast<int>(x / cx)), iy = std::min(ny - 1, static_cast<int>(y / cy)),
+              iz = std::min(nz - 1, static_cast<int>(z / cz));
+    bool ok = true;
+    for (int oz = -1; oz <= 1 && ok; ++oz)
+      for (int oy = -1; oy <= 1 && ok; ++oy)
+        for (int ox = -1; ox <= 1 && ok; ++ox) {
+          const int jx = (ix + ox + nx) % nx, jy = (iy + oy + ny) % ny, jz = (iz + oz + nz) % nz;
+          for (int p : cells[(static_cast<size_t>(jz) * ny + jy) * nx + jx]) {
+            double dx = position[p] - x, dy = position[p + N] - y, dz = position[p + 2 * N] - z;
+            dx -= lx * std::round(dx / lx);
+            dy -= ly * std::round(dy / ly);
+            dz -= lz * std::round(dz / lz);
+            if (dx * dx + dy * dy + dz * dz < d2) {
+              ok = false;
+              break;
+            }
+          }
+        }
+    if (!ok) continue;
+    position[placed] = x;
+    position[placed + N] = y;
+    position[placed + 2 * N] = z;
+    cells[(static_cast<size_t>(iz) * ny + iy) * nx + ix].push_back(placed);
+    ++placed;
+  }
+  return SUS2SH_OK;
+}
+
+}  // extern "C"

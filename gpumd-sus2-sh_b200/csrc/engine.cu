@@ -1,0 +1,818 @@
+// SUS2-SH engine kernels for sm_100a.
+//
+// Kernel map (reference stage in brackets, src/force/sus2_sh.cu):
+//   k_pack        positions -> unwrapped double4 + species, displacement max
+//   k_decide      rebuild flag (skin/2 displacement rule or host-forced)
+//   k_bin/k_scan/k_scatter/k_sort_cells/k_fill
+//                 cell-list Verlet list with explicit image codes
+//                 [build_neighbor_list :9547-9618, image kernels :7668-7769]
+//   k_basic       B[k,l,m] = sum_j R_kl(r_ij) Y_lm(r_ij)      [gpu_sh_compute_basic :3486-3550]
+//   k_product     layered CG program: forward, site energy, adjoint
+//                 [gpu_sh_forward_energy_backward_compact_rows :5592-5964]
+//   k_force       dE/dr_ij = sum_b g_b (R' u Y + R grad Y), F_i += dE,
+//                 F_j -= dE, W_i -= r_ij (x) dE        [gpu_sh_compute_forces :6347-6446]
+//   k_finalize    scatter buffer -> FP64 force          [gpu_accumulate_float_to_double :7629-7655]
+// One thread owns one centre atom in the edge kernels (lane = atom), so all
+// per-atom sums are private and only the F_j scatter uses atomics (one
+// 128-bit vector red per edge in FP32).
+#include "engine.cuh"
+#include "sh_math.cuh"
+
+#include <cstdio>
+
+namespace sus2sh {
+namespace {
+
+constexpr int kEdgeBlock = 128;
+constexpr int kCenterCode = 62;  // image (0,0,0) in base-5 codes
+
+__device__ __forceinline__ int type_of(const double4& p) {
+  return static_cast<int>(__double_as_longlong(p.w));
+}
+
+// ---------------------------------------------------------------------------
+// positions
+// ---------------------------------------------------------------------------
+__global__ void k_pack(int N, const double* __restrict__ x, const int* __restrict__ type,
+                       const double4* __restrict__ ref4, double4* __restrict__ pos4,
+                       const BoxGeom* __restrict__ g, int have_ref, Status* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float d2 = 0.0f;
+  if (i < N) {
+    double px = x[i], py = x[i + N], pz = x[i + 2 * N];
+    if (have_ref) {
+      const double4 r = ref4[i];
+      const double dx = px - r.x, dy = py - r.y, dz = pz - r.z;
+      double s[3];
+      for (int a = 0; a < 3; ++a) {
+        s[a] = g->hinv[3 * a] * dx + g->hinv[3 * a + 1] * dy + g->hinv[3 * a + 2] * dz;
+        s[a] = g->pbc[a] ? rint(s[a]) : 0.0;
+      }
+      // u = p - h * round(h^-1 (p - ref)): undo wraps applied by the caller.
+      px -= g->h[0] * s[0] + g->h[1] * s[1] + g->h[2] * s[2];
+      py -= g->h[3] * s[0] + g->h[4] * s[1] + g->h[5] * s[2];
+      pz -= g->h[6] * s[0] + g->h[7] * s[1] + g->h[8] * s[2];
+      const double ex = px - r.x, ey = py - r.y, ez = pz - r.z;
+      d2 = static_cast<float>(ex * ex + ey * ey + ez * ez);
+    }
+    pos4[i] = make_double4(px, py, pz, __longlong_as_double(static_cast<long long>(type[i])));
+  }
+  // block max of the displacement, one atomic per block
+  __shared__ float red[32];
+  float v = d2;
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.0f) atomicMax(&st->maxdisp2_bits, __float_as_uint(v));
+  }
+}
+
+__global__ void k_decide(Status* st, int force, float half_skin2) {
+  const float d2 = __uint_as_float(st->maxdisp2_bits);
+  const int need = force || (d2 > half_skin2);
+  st->rebuilt = need;
+  if (need) st->builds += 1;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour list (all kernels return immediately when no rebuild is due)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int floor_div(int a, int n) {
+  return a >= 0 ? a / n : -((-a + n - 1) / n);
+}
+
+__global__ void k_bin(int N, const Status* __restrict__ st, const BoxGeom* __restrict__ g,
+                      const double4* __restrict__ pos4, double4* __restrict__ ref4,
+                      int* __restrict__ cell_count, int* __restrict__ atom_cell,
+                      int* __restrict__ atom_rank) {
+  if (!st->rebuilt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double4 p = pos4[i];
+  double s[3];
+  int c[3];
+  for (int a = 0; a < 3; ++a) {
+    s[a] = g->hinv[3 * a] * p.x + g->hinv[3 * a + 1] * p.y + g->hinv[3 * a + 2] * p.z;
+    double w = g->pbc[a] ? floor(s[a]) : 0.0;
+    s[a] -= w;
+    int ci = static_cast<int>(floor(s[a] * g->ncell[a]));
+    ci = ci < 0 ? 0 : (ci >= g->ncell[a] ? g->ncell[a] - 1 : ci);
+    c[a] = ci;
+    s[a] = w;  // reuse: wrap count
+  }
+  const double wx = p.x - (g->h[0] * s[0] + g->h[1] * s[1] + g->h[2] * s[2]);
+  const double wy = p.y - (g->h[3] * s[0] + g->h[4] * s[1] + g->h[5] * s[2]);
+  const double wz = p.z - (g->h[6] * s[0] + g->h[7] * s[1] + g->h[8] * s[2]);
+  ref4[i] = make_double4(wx, wy, wz, p.w);
+  const int cell = (c[2] * g->ncell[1] + c[1]) * g->ncell[0] + c[0];
+  atom_cell[i] = cell;
+  atom_rank[i] = atomicAdd(&cell_count[cell], 1);
+}
+
+// Exclusive scan of cell counts, one block.
+__global__ void k_scan(const Status* __restrict__ st, const int* __restrict__ cnt,
+                       int* __restrict__ start, int ncells) {
+  if (!st->rebuilt) return;
+  __shared__ int part[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (ncells + nt - 1) / nt;
+  const int b0 = t * chunk, b1 = min(ncells, b0 + chunk);
+  int sum = 0;
+  for (int c = b0; c < b1; ++c) sum += cnt[c];
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < nt; o <<= 1) {
+    int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int c = b0; c < b1; ++c) {
+    start[c] = run;
+    run += cnt[c];
+  }
+  if (t == nt - 1) start[ncells] = part[t];
+}
+
+__global__ void k_scatter(int N, const Status* __restrict__ st, const int* __restrict__ start,
+                          const int* __restrict__ atom_cell, const int* __restrict__ atom_rank,
+                          int* __restrict__ cell_atoms) {
+  if (!st->rebuilt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  cell_atoms[start[atom_cell[i]] + atom_rank[i]] = i;
+}
+
+// Sort each cell's atoms by index so the neighbour order (and every FP sum)
+// is deterministic.
+__global__ void k_sort_cells(int ncells, const Status* __restrict__ st, const int* __restrict__ start,
+                             int* __restrict__ cell_atoms) {
+  if (!st->rebuilt) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const int b = start[c], e = start[c + 1];
+  for (int a = b + 1; a < e; ++a) {
+    const int v = cell_atoms[a];
+    int k = a - 1;
+    while (k >= b && cell_atoms[k] > v) {
+      cell_atoms[k + 1] = cell_atoms[k];
+      --k;
+    }
+    cell_atoms[k + 1] = v;
+  }
+}
+
+__global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict__ g,
+                       double cutoff2, const double4* __restrict__ ref4,
+                       const int* __restrict__ start, const int* __restrict__ cell_atoms,
+                       const int* __restrict__ atom_cell, int* __restrict__ nbr,
+                       int* __restrict__ ncount, double4* __restrict__ pos4, int cap, int count_only) {
+  if (!st->rebuilt) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double4 p = ref4[i];
+  const int cell = atom_cell[i];
+  const int cx = cell % g->ncell[0];
+  const int cy = (cell / g->ncell[0]) % g->ncell[1];
+  const int cz = cell / (g->ncell[0] * g->ncell[1]);
+  int k = 0;
+  for (int oz = -g->reach[2]; oz <= g->reach[2]; ++oz) {
+    int nz = cz + oz, tz = 0;
+    if (g->pbc[2]) {
+      tz = floor_div(nz, g->ncell[2]);
+      nz -= tz * g->ncell[2];
+    } else if (nz < 0 || nz >= g->ncell[2]) {
+      continue;
+    }
+    for (int oy = -g->reach[1]; oy <= g->reach[1]; ++oy) {
+      int ny = cy + oy, ty = 0;
+      if (g->pbc[1]) {
+        ty = floor_div(ny, g->ncell[1]);
+        ny -= ty * g->ncell[1];
+      } else if (ny < 0 || ny >= g->ncell[1]) {
+        continue;
+      }
+      for (int ox = -g->reach[0]; ox <= g->reach[0]; ++ox) {
+        int nx = cx + ox, tx = 0;
+        if (g->pbc[0]) {
+          tx = floor_div(nx, g->ncell[0]);
+          nx -= tx * g->ncell[0];
+        } else if (nx < 0 || nx >= g->ncell[0]) {
+          continue;
+        }
+        const int code = (tx + 2) * 25 + (ty + 2) * 5 + (tz + 2);
+        const double sx = g->shift[code][0], sy = g->shift[code][1], sz = g->shift[code][2];
+        const int nc = (nz * g->ncell[1] + ny) * g->ncell[0] + nx;
+        const int a1 = start[nc + 1];
+        for (int a = start[nc]; a < a1; ++a) {
+          const int j = cell_atoms[a];
+          if (j == i && code == kCenterCode) continue;
+          const double4 q = ref4[j];
+          const double dx = q.x - p.x + sx, dy = q.y - p.y + sy, dz = q.z - p.z + sz;
+          if (dx * dx + dy * dy + dz * dz < cutoff2) {
+            if (!count_only && k < cap) nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
+            ++k;
+          }
+        }
+      }
+    }
+  }
+  ncount[i] = k;
+  atomicMax(&st->max_count, k);
+  if (k > cap && !count_only) st->overflow = 1;
+  if (!count_only) pos4[i] = p;
+}
+
+// ---------------------------------------------------------------------------
+// per-edge geometry and radial basis
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Edge {
+  T r, rinv, ux, uy, uz, dr;  // dr = r - rc (computed from r^2 - rc^2 in FP64)
+  T dx, dy, dz;
+};
+
+template <typename T>
+__device__ __forceinline__ Edge<T> make_edge(double dx, double dy, double dz, double r2, double rc,
+                                             double rc2);
+
+template <>
+__device__ __forceinline__ Edge<float> make_edge<float>(double dx, double dy, double dz, double r2,
+                                                        double rc, double rc2) {
+  Edge<float> e;
+  const float r2f = static_cast<float>(r2);
+  e.rinv = rsqrtf(r2f);
+  e.r = r2f * e.rinv;
+  e.dx = static_cast<float>(dx);
+  e.dy = static_cast<float>(dy);
+  e.dz = static_cast<float>(dz);
+  e.ux = e.dx * e.rinv;
+  e.uy = e.dy * e.rinv;
+  e.uz = e.dz * e.rinv;
+  // (r - rc) without FP32 cancellation near the cutoff
+  e.dr = static_cast<float>(r2 - rc2) / (e.r + static_cast<float>(rc));
+  return e;
+}
+
+template <>
+__device__ __forceinline__ Edge<double> make_edge<double>(double dx, double dy, double dz, double r2,
+                                                          double rc, double rc2) {
+  Edge<double> e;
+  e.r = sqrt(r2);
+  e.rinv = 1.0 / e.r;
+  e.dx = dx;
+  e.dy = dy;
+  e.dz = dz;
+  e.ux = dx * e.rinv;
+  e.uy = dy * e.rinv;
+  e.uz = dz * e.rinv;
+  e.dr = (r2 - rc2) / (e.r + rc);
+  return e;
+}
+
+// R_mu for every mu; the pair table row holds KMU (scal, shift) pairs then
+// the LK pair scale.
+template <typename T, int KMU, int RB>
+__device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __restrict__ row,
+                                              const Edge<T>& e, T* R) {
+  const T f = row[2 * KMU] * e.dr * e.dr;
+  const bool rational = a.rs.rational != 0;
+  if (a.rs.shared_xi) {
+    T xi, dxi;
+    radial_map<T>(T(0.5) * row[0] * (e.r - row[1]), rational, xi, dxi);
+    T t[RB];
+    chebyshev<RB>(xi, t);
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      T s = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) s = fma(a.coef[mu * RB + n], t[n], s);
+      R[mu] = f * s;
+    }
+  } else {
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      T xi, dxi;
+      radial_map<T>(T(0.5) * row[2 * mu] * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+      T t[RB];
+      chebyshev<RB>(xi, t);
+      T s = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) s = fma(a.coef[mu * RB + n], t[n], s);
+      R[mu] = f * s;
+    }
+  }
+}
+
+template <typename T, int KMU, int RB>
+__device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T* __restrict__ row,
+                                                   const Edge<T>& e, T* R, T* dR) {
+  const T ps = row[2 * KMU];
+  const T f = ps * e.dr * e.dr;
+  const T df = T(2) * ps * e.dr;
+  const bool rational = a.rs.rational != 0;
+  if (a.rs.shared_xi) {
+    const T half_scal = T(0.5) * row[0];
+    T xi, dxi;
+    radial_map<T>(half_scal * (e.r - row[1]), rational, xi, dxi);
+    const T g = f * half_scal * dxi;  // f * d xi / dr
+    T t[RB], dt[RB];
+    chebyshev_d<RB>(xi, t, dt);
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      T s = T(0), sd = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) {
+        s = fma(a.coef[mu * RB + n], t[n], s);
+        sd = fma(a.coef[mu * RB + n], dt[n], sd);
+      }
+      R[mu] = f * s;
+      dR[mu] = df * s + g * sd;
+    }
+  } else {
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      const T half_scal = T(0.5) * row[2 * mu];
+      T xi, dxi;
+      radial_map<T>(half_scal * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+      T t[RB], dt[RB];
+      chebyshev_d<RB>(xi, t, dt);
+      T s = T(0), sd = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) {
+        s = fma(a.coef[mu * RB + n], t[n], s);
+        sd = fma(a.coef[mu * RB + n], dt[n], sd);
+      }
+      R[mu] = f * s;
+      dR[mu] = df * s + f * half_scal * dxi * sd;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void load_pair_table(const EdgeArgs<T>& a, T* s_tab) {
+  const int n = a.rs.species * a.rs.species * a.rs.pair_stride;
+  const T* src = reinterpret_cast<const T*>(a.pair_table);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) s_tab[t] = src[t];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// basic moments
+// ---------------------------------------------------------------------------
+template <typename T, int L, int K, int RB>
+__global__ void __launch_bounds__(kEdgeBlock) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_tab = reinterpret_cast<T*>(smem_raw);
+  load_pair_table(a, s_tab);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
+  T acc[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) acc[b] = T(0);
+  const double4 pi = a.pos4[i];
+  const int S = a.rs.species;
+  const int row_i = type_of(pi) * S;
+  const int cnt = min(a.ncount[i], a.cap);
+  const double rc = a.rs.rc, rc2 = rc * rc;
+  for (int n = 0; n < cnt; ++n) {
+    const int w = __ldg(a.nbr + static_cast<size_t>(n) * a.N + i);
+    const int j = w & 0xFFFFFF;
+    const int code = static_cast<unsigned>(w) >> 24;
+    const double4 pj = a.pos4[j];
+    const double dx = pj.x - pi.x + a.shift[code][0];
+    const double dy = pj.y - pi.y + a.shift[code][1];
+    const double dz = pj.z - pi.z + a.shift[code][2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 >= rc2) continue;
+    const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
+    const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
+    T R[KMU];
+    radial_values<T, KMU, RB>(a, row, e, R);
+    T Y[C];
+    sh_values<L>(e.ux, e.uy, e.uz, Y);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int l = 0; l <= L; ++l)
+#pragma unroll
+        for (int m = 0; m <= 2 * l; ++m)
+          acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], Y[l * l + m], acc[k * C + l * l + m]);
+  }
+#pragma unroll
+  for (int b = 0; b < NB; ++b) B[static_cast<size_t>(b) * a.N + i] = acc[b];
+}
+
+// ---------------------------------------------------------------------------
+// forces and virial
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Scatter;
+template <>
+struct Scatter<float> {
+  __device__ __forceinline__ static void add(void* buf, int j, float x, float y, float z) {
+    atomicAdd(reinterpret_cast<float4*>(buf) + j, make_float4(x, y, z, 0.0f));
+  }
+};
+template <>
+struct Scatter<double> {
+  __device__ __forceinline__ static void add(void* buf, int j, double x, double y, double z) {
+    double* p = reinterpret_cast<double*>(reinterpret_cast<double4*>(buf) + j);
+    atomicAdd(p, x);
+    atomicAdd(p + 1, y);
+    atomicAdd(p + 2, z);
+  }
+};
+
+template <typename T, int L, int K, int RB>
+__global__ void __launch_bounds__(kEdgeBlock)
+    k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
+            void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
+            double sign) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_tab = reinterpret_cast<T*>(smem_raw);
+  load_pair_table(a, s_tab);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
+  const T wscale = weight ? static_cast<T>(weight[i]) : T(1);
+  T g[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) g[b] = wscale * G[static_cast<size_t>(b) * a.N + i];
+  T fx = T(0), fy = T(0), fz = T(0);
+  T w[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) w[q] = T(0);
+  const double4 pi = a.pos4[i];
+  const int S = a.rs.species;
+  const int row_i = type_of(pi) * S;
+  const int cnt = min(a.ncount[i], a.cap);
+  const double rc = a.rs.rc, rc2 = rc * rc;
+  for (int n = 0; n < cnt; ++n) {
+    const int wd = __ldg(a.nbr + static_cast<size_t>(n) * a.N + i);
+    const int j = wd & 0xFFFFFF;
+    const int code = static_cast<unsigned>(wd) >> 24;
+    const double4 pj = a.pos4[j];
+    const double dx = pj.x - pi.x + a.shift[code][0];
+    const double dy = pj.y - pi.y + a.shift[code][1];
+    const double dz = pj.z - pi.z + a.shift[code][2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 >= rc2) continue;
+    const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
+    const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
+    T R[KMU], dR[KMU];
+    radial_values_ders<T, KMU, RB>(a, row, e, R, dR);
+    T Y[C];
+    sh_values<L>(e.ux, e.uy, e.uz, Y);
+    T Gy[C];
+    T s = T(0);
+#pragma unroll
+    for (int l = 0; l <= L; ++l)
+#pragma unroll
+      for (int m = 0; m <= 2 * l; ++m) {
+        T gv = T(0), hv = T(0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          gv = fma(g[k * C + l * l + m], R[k * (L + 1) + l], gv);
+          hv = fma(g[k * C + l * l + m], dR[k * (L + 1) + l], hv);
+        }
+        Gy[l * l + m] = gv;
+        s = fma(hv, Y[l * l + m], s);
+      }
+    T vx, vy, vz;
+    sh_grad_contract<L>(e.ux, e.uy, e.uz, Gy, vx, vy, vz);
+    const T uv = e.ux * vx + e.uy * vy + e.uz * vz;
+    const T dEx = s * e.ux + (vx - uv * e.ux) * e.rinv;
+    const T dEy = s * e.uy + (vy - uv * e.uy) * e.rinv;
+    const T dEz = s * e.uz + (vz - uv * e.uz) * e.rinv;
+    fx += dEx;
+    fy += dEy;
+    fz += dEz;
+    Scatter<T>::add(ftmp, j, -dEx, -dEy, -dEz);
+    w[0] -= e.dx * dEx;
+    w[1] -= e.dy * dEy;
+    w[2] -= e.dz * dEz;
+    w[3] -= e.dx * dEy;
+    w[4] -= e.dx * dEz;
+    w[5] -= e.dy * dEz;
+    w[6] -= e.dy * dEx;
+    w[7] -= e.dz * dEx;
+    w[8] -= e.dz * dEy;
+  }
+  force[i] += sign * static_cast<double>(fx);
+  force[i + a.N] += sign * static_cast<double>(fy);
+  force[i + 2 * a.N] += sign * static_cast<double>(fz);
+  if (virial) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) virial[static_cast<size_t>(q) * a.N + i] += static_cast<double>(w[q]);
+  }
+}
+
+template <typename T>
+__global__ void k_finalize(int N, const void* __restrict__ ftmp, double* __restrict__ force,
+                           double sign);
+template <>
+__global__ void k_finalize<float>(int N, const void* __restrict__ ftmp, double* __restrict__ force,
+                                  double sign) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float4 v = reinterpret_cast<const float4*>(ftmp)[i];
+  force[i] += sign * static_cast<double>(v.x);
+  force[i + N] += sign * static_cast<double>(v.y);
+  force[i + 2 * N] += sign * static_cast<double>(v.z);
+}
+template <>
+__global__ void k_finalize<double>(int N, const void* __restrict__ ftmp, double* __restrict__ force,
+                                   double sign) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double4 v = reinterpret_cast<const double4*>(ftmp)[i];
+  force[i] += sign * v.x;
+  force[i + N] += sign * v.y;
+  force[i + 2 * N] += sign * v.z;
+}
+
+// ---------------------------------------------------------------------------
+// CG product program (lane = atom).  Row header: kind(2) | nterms(14) | dst(16);
+// term word: a(16) | b(16).  Kinds:
+//   0 FWD   V[dst]  = sum c V[a] V[b]
+//   1 TERM  E += sum c V[a] V[b]; G[a] += c V[b]; G[b] += c V[a]
+//           (terminal scalar row, c premultiplied by its moment weight)
+//   2 SEED  E += c V[a]; G[a] += c              (non-terminal scalar)
+//   3 BACK  G[dst] += sum c G[a] V[b]           (a = consumer target slot)
+// G[v] lives at slot v + nvalue.
+// ---------------------------------------------------------------------------
+template <typename T, bool kShared>
+__global__ void __launch_bounds__(128)
+    k_product(int N, const ProgramDev p, const double4* __restrict__ pos4, const T* __restrict__ B,
+              T* __restrict__ G, T* __restrict__ scratch, const double* __restrict__ shift_coeffs,
+              const double* __restrict__ species_coeffs, double* __restrict__ pe, int pe_assign) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int atom = blockIdx.x * blockDim.x + threadIdx.x;
+  if (atom >= N) return;
+  T* S;
+  size_t stride;
+  if (kShared) {
+    S = reinterpret_cast<T*>(smem_raw) + threadIdx.x;
+    stride = blockDim.x;
+  } else {
+    S = scratch + atom;
+    stride = static_cast<size_t>(N);
+  }
+  const int gofs = p.nvalue;
+  for (int b = 0; b < p.nbasic; ++b)
+    S[b * stride] = B[static_cast<size_t>(__ldg(p.basic_canon + b)) * N + atom];
+  for (int v = 0; v < p.nvalue; ++v) S[(gofs + v) * stride] = T(0);
+  const uint32_t* __restrict__ code = p.code;
+  const T* __restrict__ cf = reinterpret_cast<const T*>(p.coef);
+  double E = 0.0;
+  for (int r = 0; r < p.nrows; ++r) {
+    const uint32_t h = __ldg(code++);
+    const int kind = h >> 30;
+    const int nt = (h >> 16) & 0x3FFF;
+    const int dst = h & 0xFFFF;
+    if (kind == 0) {
+      T acc = T(0);
+      for (int t = 0; t < nt; ++t) {
+        const uint32_t w = __ldg(code + t);
+        acc = fma(__ldg(cf + t) * S[(w & 0xFFFF) * stride], S[(w >> 16) * stride], acc);
+      }
+      S[dst * stride] = acc;
+    } else if (kind == 1) {
+      T acc = T(0);
+      for (int t = 0; t < nt; ++t) {
+        const uint32_t w = __ldg(code + t);
+        const int ia = w & 0xFFFF, ib = w >> 16;
+        const T c = __ldg(cf + t);
+        const T va = S[ia * stride], vb = S[ib * stride];
+        acc = fma(c * va, vb, acc);
+        S[(gofs + ia) * stride] += c * vb;
+        S[(gofs + ib) * stride] += c * va;
+      }
+      E += static_cast<double>(acc);
+    } else if (kind == 2) {
+      const uint32_t w = __ldg(code);
+      const int ia = w & 0xFFFF;
+      const T c = __ldg(cf);
+      E += static_cast<double>(c * S[ia * stride]);
+      S[(gofs + ia) * stride] += c;
+    } else {
+      T acc = T(0);
+      for (int t = 0; t < nt; ++t) {
+        const uint32_t w = __ldg(code + t);
+        acc = fma(__ldg(cf + t) * S[(gofs + (w & 0xFFFF)) * stride], S[(w >> 16) * stride], acc);
+      }
+      S[(gofs + dst) * stride] += acc;
+    }
+    code += nt;
+    cf += nt;
+  }
+  const int ti = type_of(pos4[atom]);
+  const double ct = species_coeffs[ti];
+  const double site = shift_coeffs[ti] + ct + ct * E;
+  if (pe) pe[atom] = pe_assign ? site : pe[atom] + site;
+  const T sc = static_cast<T>(ct);
+  for (int c = 0; c < p.ncanon; ++c) {
+    const int b = __ldg(p.canon_basic + c);
+    G[static_cast<size_t>(c) * N + atom] = b >= 0 ? sc * S[(gofs + b) * stride] : T(0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MD integrator (velocity Verlet); units A, fs, amu, eV.
+// ---------------------------------------------------------------------------
+constexpr double kAccel = 9.648533212331002e-3;  // (eV/A/amu) -> A/fs^2
+
+// Half kick + drift; the force (and optionally energy/virial) arrays are
+// zeroed after use so the next accumulating force call starts from zero.
+__global__ void k_kick_drift(int N, double dt, const double* __restrict__ inv_mass_type,
+                             const int* __restrict__ type, double* __restrict__ f,
+                             double* __restrict__ v, double* __restrict__ x,
+                             double* __restrict__ pe, double* __restrict__ vir) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double a = 0.5 * dt * kAccel * inv_mass_type[type[i]];
+  for (int d = 0; d < 3; ++d) {
+    const double vv = v[i + d * N] + a * f[i + d * N];
+    v[i + d * N] = vv;
+    x[i + d * N] += dt * vv;
+    f[i + d * N] = 0.0;
+  }
+  if (pe) pe[i] = 0.0;
+  if (vir)
+    for (int q = 0; q < 9; ++q) vir[static_cast<size_t>(q) * N + i] = 0.0;
+}
+
+__global__ void k_kick(int N, double dt, const double* __restrict__ inv_mass_type,
+                       const int* __restrict__ type, const double* __restrict__ f,
+                       double* __restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double a = 0.5 * dt * kAccel * inv_mass_type[type[i]];
+  for (int d = 0; d < 3; ++d) v[i + d * N] += a * f[i + d * N];
+}
+
+// Sum of per-atom energy (out[0]) and virial (out[1..9]); one FP64 atomic
+// per block and component.
+__global__ void k_reduce(int N, const double* __restrict__ pe, const double* __restrict__ vir,
+                         double* __restrict__ out) {
+  __shared__ double red[10][8];
+  double v[10];
+  for (int q = 0; q < 10; ++q) v[q] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    v[0] += pe[i];
+    if (vir)
+      for (int q = 0; q < 9; ++q) v[q + 1] += vir[static_cast<size_t>(q) * N + i];
+  }
+  for (int q = 0; q < 10; ++q) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 10) {
+    double x = 0.0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) x += red[threadIdx.x][w];
+    atomicAdd(out + threadIdx.x, x);
+  }
+}
+
+inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace
+
+void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial, double* out) {
+  cudaMemsetAsync(out, 0, 10 * sizeof(double), s);
+  int grid = blocks_for(N, 256);
+  if (grid > 592) grid = 592;
+  if (grid < 1) grid = 1;
+  k_reduce<<<grid, 256, 0, s>>>(N, pe, virial, out);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const double4* ref4,
+                 double4* pos4, const BoxGeom* geom_dev, int have_ref, Status* st) {
+  k_pack<<<blocks_for(N, 256), 256, 0, s>>>(N, x, type, ref4, pos4, geom_dev, have_ref, st);
+}
+
+void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
+                  const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
+                  int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
+                  int cap, int count_only, Status* st) {
+  (void)g;
+  k_decide<<<1, 1, 0, s>>>(st, force, half_skin2);
+  cudaMemsetAsync(cell_count, 0, sizeof(int) * (ncells + 1), s);
+  k_bin<<<blocks_for(N, 256), 256, 0, s>>>(N, st, geom_dev, pos4, ref4, cell_count, atom_cell, atom_rank);
+  k_scan<<<1, 1024, 0, s>>>(st, cell_count, cell_start, ncells);
+  k_scatter<<<blocks_for(N, 256), 256, 0, s>>>(N, st, cell_start, atom_cell, atom_rank, cell_atoms);
+  k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, cell_start, cell_atoms);
+  k_fill<<<blocks_for(N, 128), 128, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms,
+                                             atom_cell, nbr, ncount, pos4, cap, count_only);
+}
+
+// Compiled (L, K, RB) shapes of the edge kernels.
+#define SUS2_SHAPES(X) \
+  X(3, 3, 8)           \
+  X(3, 3, 10)          \
+  X(4, 4, 10)          \
+  X(4, 4, 8)           \
+  X(2, 2, 8)           \
+  X(1, 1, 4)
+
+bool shape_supported(int l_max, int k_max, int rb) {
+#define SUS2_CHECK(L, K, RB) \
+  if (l_max == L && k_max == K && rb == RB) return true;
+  SUS2_SHAPES(SUS2_CHECK)
+#undef SUS2_CHECK
+  return false;
+}
+
+template <typename T>
+static size_t pair_smem(const EdgeArgs<T>& a) {
+  return sizeof(T) * static_cast<size_t>(a.rs.species) * a.rs.species * a.rs.pair_stride;
+}
+
+template <typename T>
+int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B) {
+  const size_t sm = pair_smem(a);
+  const int grid = blocks_for(a.N, kEdgeBlock);
+#define SUS2_BASIC(L, K, RB)                                                 \
+  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) {                       \
+    k_basic<T, L, K, RB><<<grid, kEdgeBlock, sm, s>>>(a, B);                 \
+    return 0;                                                                \
+  }
+  SUS2_SHAPES(SUS2_BASIC)
+#undef SUS2_BASIC
+  return -1;
+}
+
+template <typename T>
+int launch_force(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight, void* ftmp,
+                 double* force, double* virial, double sign) {
+  const size_t sm = pair_smem(a);
+  const int grid = blocks_for(a.N, kEdgeBlock);
+#define SUS2_FORCE(L, K, RB)                                                          \
+  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) {                                \
+    k_force<T, L, K, RB><<<grid, kEdgeBlock, sm, s>>>(a, G, weight, ftmp, force, virial, sign); \
+    return 0;                                                                         \
+  }
+  SUS2_SHAPES(SUS2_FORCE)
+#undef SUS2_FORCE
+  return -1;
+}
+
+template <typename T>
+void launch_product(cudaStream_t s, int N, const ProgramDev& p, const double4* pos4, const T* B, T* G,
+                    T* scratch, size_t smem_tile_bytes, int tile, const double* shift_coeffs,
+                    const double* species_coeffs, double* pe, int pe_assign) {
+  if (scratch == nullptr) {
+    static bool configured[2] = {false, false};
+    const int which = sizeof(T) == 8;
+    if (!configured[which]) {
+      cudaFuncSetAttribute(k_product<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      configured[which] = true;
+    }
+    k_product<T, true><<<blocks_for(N, tile), tile, smem_tile_bytes, s>>>(
+        N, p, pos4, B, G, nullptr, shift_coeffs, species_coeffs, pe, pe_assign);
+  } else {
+    k_product<T, false><<<blocks_for(N, 128), 128, 0, s>>>(N, p, pos4, B, G, scratch, shift_coeffs,
+                                                           species_coeffs, pe, pe_assign);
+  }
+}
+
+template <typename T>
+void launch_finalize(cudaStream_t s, int N, const void* ftmp, double* force, double sign) {
+  k_finalize<T><<<blocks_for(N, 256), 256, 0, s>>>(N, ftmp, force, sign);
+}
+
+void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_mass_type, const int* type,
+                           double* force, double* vel, double* pos, double* pe, double* vir) {
+  k_kick_drift<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel, pos, pe, vir);
+}
+
+void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_type, const int* type,
+                     const double* force, double* vel) {
+  k_kick<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel);
+}
+
+template int launch_basic<float>(cudaStream_t, const EdgeArgs<float>&, float*);
+template int launch_basic<double>(cudaStream_t, const EdgeArgs<double>&, double*);
+template int launch_force<float>(cudaStream_t, const EdgeArgs<float>&, const float*, const double*, void*,
+                                 double*, double*, double);
+template int launch_force<double>(cudaStream_t, const EdgeArgs<double>&, const double*, const double*, void*,
+                                  double*, double*, double);
+template void launch_product<float>(cudaStream_t, int, const ProgramDev&, const double4*, const float*, float*,
+                                    float*, size_t, int, const double*, const double*, double*, int);
+template void launch_product<double>(cudaStream_t, int, const ProgramDev&, const double4*, const double*,
+                                     double*, double*, size_t, int, const double*, const double*, double*, int);
+template void launch_finalize<float>(cudaStream_t, int, const void*, double*, double);
+template void launch_finalize<double>(cudaStream_t, int, const void*, double*, double);
+
+}  // namespace sus2sh

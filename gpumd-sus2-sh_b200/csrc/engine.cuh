@@ -1,0 +1,110 @@
+// Device-side data layout and kernel launchers of the SUS2-SH engine.
+//
+// HBM layout (N atoms):
+//   pos4   double4[N]   unwrapped position (x,y,z) + species in .w (int bits)
+//   ref4   double4[N]   wrapped position at the last neighbour build
+//   nbr    int32[cap][N] neighbour j (bits 0-23) | image code (bits 24-31)
+//   ncount int32[N]
+//   B, G   T[K*C][N]    basic moments and their adjoints, canonical order
+//                        k*C + l*l + l + m, C = (L+1)^2
+//   ftmp   float4/double [N]  scatter target for F_j -= dE
+// Every launch goes to the caller's stream; no host synchronisation happens
+// in the steady state.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sus2sh {
+
+constexpr int kMaxPairTable = 8192;  // floats of per-pair radial table
+constexpr int kMaxCoef = 48 * 16;
+
+// Box and cell grid for one neighbour build (host computed).
+struct BoxGeom {
+  double h[9];      // column vectors a=(h0,h3,h6), b=(h1,h4,h7), c=(h2,h5,h8)
+  double hinv[9];
+  int pbc[3];
+  int ncell[3];     // cells per fractional direction
+  int reach[3];     // cell offsets scanned per direction
+  double shift[125][3];  // Cartesian image vectors of codes (base 5, -2..2)
+};
+
+struct Status {
+  unsigned int maxdisp2_bits;  // max |u - ref|^2 since last build (float bits)
+  int rebuilt;                 // a build happened in this call
+  int overflow;                // neighbour capacity exceeded (sticky)
+  int max_count;               // largest neighbour count seen at a build
+  int builds;                  // number of builds
+  int pad[3];
+};
+
+// Radial table: per pair p = t_i*S + t_j: [KMU] (scal, shift) pairs then the
+// pair scale; shared_xi means every mu of a pair uses the same (scal, shift).
+struct RadialSetup {
+  int species;
+  int kmu;
+  int rb;
+  int rational;
+  int shared_xi;
+  int pair_stride;  // floats per pair in the table
+  double rc;
+};
+
+template <typename T>
+struct EdgeArgs {
+  int N;
+  int cap;
+  int l_max, k_max;
+  RadialSetup rs;
+  const double4* pos4;
+  const int* nbr;
+  const int* ncount;
+  const void* pair_table;   // T[S*S][pair_stride]
+  const double (*shift)[3];  // device copy of BoxGeom::shift
+  T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
+};
+
+struct ProgramDev {
+  int nrows;
+  int nvalue;         // value slots; grad slot of v is v + nvalue
+  int nbasic;
+  int ncanon;         // K*C
+  const uint32_t* code;
+  const void* coef;   // T[]
+  const int* basic_canon;  // [nbasic] canonical index of model basic b
+  const int* canon_basic;  // [ncanon] model basic or -1
+};
+
+// ---- launchers (engine.cu) ----------------------------------------------
+void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const double4* ref4,
+                 double4* pos4, const BoxGeom* geom_dev, int have_ref, Status* st);
+void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
+                  const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
+                  int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
+                  int cap, int count_only, Status* st);
+
+template <typename T>
+int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B);
+template <typename T>
+int launch_force(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight,
+                 void* ftmp, double* force, double* virial, double sign);
+// Sums per-atom energy and virial into out[0] and out[1..9] (FP64 atomics).
+void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial, double* out);
+template <typename T>
+void launch_product(cudaStream_t s, int N, const ProgramDev& p, const double4* pos4, const T* B,
+                    T* G, T* scratch, size_t smem_tile_bytes, int tile, const double* shift_coeffs,
+                    const double* species_coeffs, double* pe, int pe_assign);
+template <typename T>
+void launch_finalize(cudaStream_t s, int N, const void* ftmp, double* force, double sign);
+
+// Integrator kernels for the benchmark MD driver.
+void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_mass_type,
+                           const int* type, double* force, double* vel, double* pos, double* pe,
+                           double* vir);
+void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_type,
+                     const int* type, const double* force, double* vel);
+
+bool shape_supported(int l_max, int k_max, int rb);
+
+}  // namespace sus2sh

@@ -1,0 +1,129 @@
+// SUS2-SH model description on the host: the .mtp reader, the real
+// Clebsch-Gordan standard graph builder and the run.in option parser.
+//
+// Reference interfaces restated here (hu-yanxiao/GPUMD-SUS2-SH):
+//   load_sh_model                     src/force/sus2_sh.cu:2105-2482
+//   SHStandardGraphBuilderHost        src/force/sus2_sh.cu:1227-1706
+//   standard_sh_graph_matches         src/force/sus2_sh.cu:1872-1911
+//   build_explicit_sh_graph_metadata  src/force/sus2_sh.cu:1913-2093
+//   parse_sh_float                    src/force/sus2_sh.cu:520-536
+// Input errors throw sus2sh::InputError; the C-ABI turns them into return
+// codes (the reference prints and calls exit(1), sus2_sh.cu:269-273).
+#pragma once
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace sus2sh {
+
+struct InputError : std::runtime_error {
+  explicit InputError(const std::string& m) : std::runtime_error(m) {}
+};
+
+struct Product {
+  int left = 0, right = 0, target = 0;
+  double coeff = 0.0;
+};
+
+enum class RadialMap { Tanh = 0, Rational = 1 };
+
+struct HostModel {
+  int species_count = 0;
+  int l_max = 0;
+  int k_max = 0;
+  int body_order = 0;
+  int rb_size = 0;
+  int radial_funcs = 0;     // K (L+1)
+  int moments = 0;          // alpha_moments_count
+  int basic_count = 0;      // alpha_index_basic_count
+  int scalar_count = 0;     // alpha_scalar_moments
+  double scaling = 1.0;
+  double rc = 0.0;          // max_dist
+  RadialMap radial_map = RadialMap::Tanh;
+  std::string radial_basis_type;
+  std::vector<int> body_l_max;          // indexed by body order, size 7
+  std::vector<double> shift_coeffs;     // [S] site energy shift
+  std::vector<double> scal_coeffs;      // [Kmu][2][S][S]: scal block then shift block
+  std::vector<double> species_coeffs;   // [S]
+  std::vector<double> moment_coeffs;    // [scalars]
+  std::vector<int> moment_mapping;      // [scalars] -> moment id
+  std::vector<int> basic_mu, basic_l, basic_m;  // [basics]
+  std::vector<Product> products;
+  std::vector<double> radial_coeffs;    // [Kmu][rb]
+  std::vector<double> radial_type_coeffs;  // [S]
+  bool standard_graph_matched = false;
+};
+
+// Parses a SUS2-SH v1.1.0 .mtp file with the reference reader's semantics.
+HostModel load_model(const std::string& path);
+// True when the file contains "potential_tag = SUS2-SH" (sus2_sh.cu:7771-7780).
+bool is_sus2_sh_file(const std::string& path);
+
+// ---- standard graph -------------------------------------------------------
+struct StandardGraph {
+  int node_count = 0;
+  int max_layer = 0;
+  std::vector<int> basic_k, basic_l, basic_m;
+  std::vector<Product> products;
+  std::vector<int> scalars;
+  int tensor_blocks = 0;
+  int cg_blocks = 0;
+  int cg_terms = 0;
+};
+
+// Body-order indexed l limits (size 7), default l_max everywhere.
+std::vector<int> default_body_l_max(int l_max);
+StandardGraph build_standard_graph(int l_max, int k_max, int body_order,
+                                   const std::vector<int>& body_l_max);
+double real_cg(int l1, int m1, int l2, int m2, int L, int M);
+
+// ---- explicit layered rows (build_explicit_sh_graph_metadata) -------------
+struct Row {
+  int layer = 0;
+  int target = 0;
+  std::vector<int> left, right;
+  std::vector<double> coeff;
+};
+struct Layered {
+  int max_layer = 0;
+  std::vector<Row> rows;            // sorted by (layer, target)
+  std::vector<int> node_layer;      // per moment
+  std::vector<char> terminal;       // scalar target consumed by no product
+  std::vector<int> scalar_of;       // moment -> scalar index (last wins), -1
+};
+Layered layer_products(const HostModel& m);
+
+// ---- run.in options ---------------------------------------------------------
+struct Options {
+  bool use_float = true;        // sus2_float / sus2_sh_float / SUS2_GPUMD_FLOAT
+  double skin = 1.0;            // sus2_sh_skin= (Angstrom)
+  int rebuild_interval = 0;     // sus2_sh_rebuild_interval= (0: displacement only)
+  bool reference_rounding = false;  // sus2_sh_reference_rounding=
+};
+// Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
+// the reference's tuning switches are accepted and ignored.
+Options parse_options(const HostModel& m, int nopts, const char** opts);
+
+// ---- synthetic model writer (seeded) -----------------------------------------
+struct SynthSpec {
+  int species = 2;
+  int l_max = 3;
+  int k_max = 3;
+  int body_order = 4;
+  int rb_size = 8;
+  double r_min = 2.0;
+  double rc = 5.0;
+  int rational = 0;
+  std::vector<int> body_l_max_list;      // empty: none written
+  std::vector<double> shift;             // [S] site energy shifts
+  double radial_sigma = 0.1;
+  double moment_sigma = 0.01;
+  double scal = 1.0;                     // radial tanh scale
+  double rshift = -1.0;                  // radial shift; <0 -> (r_min+rc)/2
+  double radial_type_coeff = 1.0;
+  unsigned long long seed = 0;
+};
+void write_synthetic_model(const std::string& path, const SynthSpec& spec);
+
+}  // namespace sus2sh

@@ -1,0 +1,216 @@
+// Per-edge math of the SUS2-SH descriptor, shared by the CUDA kernels and by
+// host-side unit tests (every function is __host__ __device__).
+//
+//  * Real spherical harmonics Y_lm(u), l <= 4, orthonormal, no Condon-Shortley
+//    phase, flat index l*l + l + m (same basis and ordering as the reference's
+//    eval_real_sh, src/force/sus2_sh.cu:3032-3169).  The polynomial forms are
+//    the standard real-harmonic table evaluated on the unit vector u = d/|d|.
+//  * Gradients use the tangential projection: for Y(d) = F(d/r),
+//        dY/dd = (grad F(u) - (u . grad F(u)) u) / r,
+//    with F the homogeneous Cartesian polynomial of each harmonic.  The force
+//    kernel contracts the adjoint first and projects once per edge.
+//  * Chebyshev-sss radial basis (sus2_sh.cu:3171-3220):
+//        xi = tanh(z) or z/sqrt(1+z^2) (rational map, README.md:45,55-56),
+//        z = scal (r - shift) / 2,
+//        R_mu = s_pair (r-rc)^2 sum_n c[mu][n] T_n(xi),
+//    T_0 = 1, T_1 = xi, T_n = 2 xi T_{n-1} - T_{n-2}; dT_n/dxi by the paired
+//    recurrence.  s_pair = scaling * rtc[t_i] * rtc[t_j] is the LK species
+//    scaling folded per pair (build_direct_radial_tables, sus2_sh.cu:2484-2517).
+#pragma once
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define SUS2_HD __host__ __device__ __forceinline__
+#else
+#define SUS2_HD inline
+#endif
+
+namespace sus2sh {
+
+// Normalisation constants of the real harmonics.
+struct YC {
+  static constexpr double c00 = 0.28209479177387814347;   // 1/2 sqrt(1/pi)
+  static constexpr double c1 = 0.48860251190291992159;    // 1/2 sqrt(3/pi)
+  static constexpr double c2a = 1.09254843059207907054;   // 1/2 sqrt(15/pi)
+  static constexpr double c20 = 0.31539156525252000603;   // 1/4 sqrt(5/pi)
+  static constexpr double c22 = 0.54627421529603953527;   // 1/4 sqrt(15/pi)
+  static constexpr double c33 = 0.59004358992664351035;   // 1/4 sqrt(35/(2pi))
+  static constexpr double c32 = 2.89061144264055405539;   // 1/2 sqrt(105/pi)
+  static constexpr double c31 = 0.45704579946446573616;   // 1/4 sqrt(21/(2pi))
+  static constexpr double c30 = 0.37317633259011539141;   // 1/4 sqrt(7/pi)
+  static constexpr double c3p2 = 1.44530572132027702770;  // 1/4 sqrt(105/pi)
+  static constexpr double c44m = 2.50334294179670453835;  // 3/4 sqrt(35/pi)
+  static constexpr double c43 = 1.77013076977993053104;   // 3/4 sqrt(35/(2pi))
+  static constexpr double c42m = 0.94617469575756001810;  // 3/4 sqrt(5/pi)
+  static constexpr double c41 = 0.66904654355728916795;   // 3/4 sqrt(5/(2pi))
+  static constexpr double c40 = 0.10578554691520430380;   // 3/16 sqrt(1/pi)
+  static constexpr double c42 = 0.47308734787878000905;   // 3/8 sqrt(5/pi)
+  static constexpr double c44 = 0.62583573544917613459;   // 3/16 sqrt(35/pi)
+};
+
+// Y[l*l+l+m] for l <= L at unit vector (x, y, z).
+template <int L, typename T>
+SUS2_HD void sh_values(T x, T y, T z, T* Y) {
+  Y[0] = T(YC::c00);
+  if (L < 1) return;
+  Y[1] = T(YC::c1) * y;
+  Y[2] = T(YC::c1) * z;
+  Y[3] = T(YC::c1) * x;
+  if (L < 2) return;
+  const T x2 = x * x, y2 = y * y, z2 = z * z;
+  Y[4] = T(YC::c2a) * x * y;
+  Y[5] = T(YC::c2a) * y * z;
+  Y[6] = T(YC::c20) * (T(2) * z2 - x2 - y2);
+  Y[7] = T(YC::c2a) * x * z;
+  Y[8] = T(YC::c22) * (x2 - y2);
+  if (L < 3) return;
+  const T a31 = T(4) * z2 - x2 - y2;
+  Y[9] = T(YC::c33) * y * (T(3) * x2 - y2);
+  Y[10] = T(YC::c32) * x * y * z;
+  Y[11] = T(YC::c31) * y * a31;
+  Y[12] = T(YC::c30) * z * (T(2) * z2 - T(3) * x2 - T(3) * y2);
+  Y[13] = T(YC::c31) * x * a31;
+  Y[14] = T(YC::c3p2) * z * (x2 - y2);
+  Y[15] = T(YC::c33) * x * (x2 - T(3) * y2);
+  if (L < 4) return;
+  const T r2 = x2 + y2;
+  Y[16] = T(YC::c44m) * x * y * (x2 - y2);
+  Y[17] = T(YC::c43) * y * z * (T(3) * x2 - y2);
+  Y[18] = T(YC::c42m) * x * y * (T(6) * z2 - r2);
+  Y[19] = T(YC::c41) * y * z * (T(4) * z2 - T(3) * r2);
+  Y[20] = T(YC::c40) * (T(8) * z2 * z2 - T(24) * z2 * r2 + T(3) * r2 * r2);
+  Y[21] = T(YC::c41) * x * z * (T(4) * z2 - T(3) * r2);
+  Y[22] = T(YC::c42) * (x2 - y2) * (T(6) * z2 - r2);
+  Y[23] = T(YC::c43) * x * z * (x2 - T(3) * y2);
+  Y[24] = T(YC::c44) * (x2 * x2 - T(6) * x2 * y2 + y2 * y2);
+}
+
+// V = sum_lm G[lm] * grad P_lm(u), P_lm the homogeneous polynomial of Y_lm.
+template <int L, typename T>
+SUS2_HD void sh_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
+  vx = T(0);
+  vy = T(0);
+  vz = T(0);
+  if (L < 1) return;
+  {
+    const T c = T(YC::c1);
+    vx += c * G[3];
+    vy += c * G[1];
+    vz += c * G[2];
+  }
+  if (L < 2) return;
+  const T x2 = x * x, y2 = y * y, z2 = z * z;
+  {
+    const T g4 = T(YC::c2a) * G[4], g5 = T(YC::c2a) * G[5], g6 = T(YC::c20) * G[6];
+    const T g7 = T(YC::c2a) * G[7], g8 = T(YC::c22) * G[8];
+    vx += g4 * y + g7 * z + T(2) * x * (g8 - g6);
+    vy += g4 * x + g5 * z - T(2) * y * (g6 + g8);
+    vz += g5 * y + g7 * x + T(4) * z * g6;
+  }
+  if (L < 3) return;
+  {
+    const T g9 = T(YC::c33) * G[9], g10 = T(YC::c32) * G[10], g11 = T(YC::c31) * G[11];
+    const T g12 = T(YC::c30) * G[12], g13 = T(YC::c31) * G[13], g14 = T(YC::c3p2) * G[14];
+    const T g15 = T(YC::c33) * G[15];
+    const T xy = x * y, xz = x * z, yz = y * z;
+    // Y3-3 = y(3x^2-y^2): (6xy, 3x^2-3y^2, 0)
+    // Y3-2 = xyz: (yz, xz, xy)
+    // Y3-1 = y(4z^2-x^2-y^2): (-2xy, 4z^2-x^2-3y^2, 8yz)
+    // Y30 = z(2z^2-3x^2-3y^2): (-6xz, -6yz, 6z^2-3x^2-3y^2)
+    // Y31 = x(4z^2-x^2-y^2): (4z^2-3x^2-y^2, -2xy, 8xz)
+    // Y32 = z(x^2-y^2): (2xz, -2yz, x^2-y^2)
+    // Y33 = x(x^2-3y^2): (3x^2-3y^2, -6xy, 0)
+    vx += T(6) * xy * g9 + yz * g10 - T(2) * xy * g11 - T(6) * xz * g12 +
+          (T(4) * z2 - T(3) * x2 - y2) * g13 + T(2) * xz * g14 + T(3) * (x2 - y2) * g15;
+    vy += T(3) * (x2 - y2) * g9 + xz * g10 + (T(4) * z2 - x2 - T(3) * y2) * g11 -
+          T(6) * yz * g12 - T(2) * xy * g13 - T(2) * yz * g14 - T(6) * xy * g15;
+    vz += xy * g10 + T(8) * yz * g11 + (T(6) * z2 - T(3) * x2 - T(3) * y2) * g12 +
+          T(8) * xz * g13 + (x2 - y2) * g14;
+  }
+  if (L < 4) return;
+  {
+    const T g16 = T(YC::c44m) * G[16], g17 = T(YC::c43) * G[17], g18 = T(YC::c42m) * G[18];
+    const T g19 = T(YC::c41) * G[19], g20 = T(YC::c40) * G[20], g21 = T(YC::c41) * G[21];
+    const T g22 = T(YC::c42) * G[22], g23 = T(YC::c43) * G[23], g24 = T(YC::c44) * G[24];
+    const T xy = x * y, xz = x * z, yz = y * z, xyz = x * y * z, r2 = x2 + y2;
+    // Y4-4 = x^3 y - x y^3
+    vx += g16 * (T(3) * x2 * y - y * y2);
+    vy += g16 * (x * x2 - T(3) * x * y2);
+    // Y4-3 = 3x^2 yz - y^3 z
+    vx += g17 * T(6) * xyz;
+    vy += g17 * (T(3) * x2 * z - T(3) * y2 * z);
+    vz += g17 * (T(3) * x2 * y - y * y2);
+    // Y4-2 = 6xyz^2 - x^3 y - x y^3
+    vx += g18 * (T(6) * y * z2 - T(3) * x2 * y - y * y2);
+    vy += g18 * (T(6) * x * z2 - x * x2 - T(3) * x * y2);
+    vz += g18 * T(12) * xyz;
+    // Y4-1 = 4yz^3 - 3x^2 yz - 3y^3 z
+    vx += g19 * (-T(6) * xyz);
+    vy += g19 * (T(4) * z * z2 - T(3) * x2 * z - T(9) * y2 * z);
+    vz += g19 * (T(12) * y * z2 - T(3) * x2 * y - T(3) * y * y2);
+    // Y40 = 8z^4 - 24 z^2 r2 + 3 r2^2, r2 = x^2 + y^2
+    const T a40 = T(12) * r2 - T(48) * z2;
+    vx += g20 * a40 * x;
+    vy += g20 * a40 * y;
+    vz += g20 * (T(32) * z * z2 - T(48) * z * r2);
+    // Y41 = 4xz^3 - 3x^3 z - 3x y^2 z
+    vx += g21 * (T(4) * z * z2 - T(9) * x2 * z - T(3) * y2 * z);
+    vy += g21 * (-T(6) * xyz);
+    vz += g21 * (T(12) * x * z2 - T(3) * x * x2 - T(3) * x * y2);
+    // Y42 = 6x^2 z^2 - 6y^2 z^2 - x^4 + y^4
+    vx += g22 * (T(12) * x * z2 - T(4) * x * x2);
+    vy += g22 * (T(4) * y * y2 - T(12) * y * z2);
+    vz += g22 * (T(12) * (x2 - y2) * z);
+    // Y43 = x^3 z - 3x y^2 z
+    vx += g23 * (T(3) * x2 * z - T(3) * y2 * z);
+    vy += g23 * (-T(6) * xyz);
+    vz += g23 * (x * x2 - T(3) * x * y2);
+    // Y44 = x^4 - 6x^2 y^2 + y^4
+    vx += g24 * (T(4) * x * x2 - T(12) * x * y2);
+    vy += g24 * (T(4) * y * y2 - T(12) * x2 * y);
+    (void)xy;
+    (void)xz;
+    (void)yz;
+  }
+}
+
+// Radial argument map xi(z) and d xi / dz.
+template <typename T>
+SUS2_HD void radial_map(T z, bool rational, T& xi, T& dxi_dz) {
+  if (rational) {
+    const T q = T(1) / sqrt(T(1) + z * z);
+    xi = z * q;
+    dxi_dz = q * q * q;
+  } else {
+    xi = tanh(z);
+    dxi_dz = T(1) - xi * xi;
+  }
+}
+
+// Chebyshev T_n(xi), n < RB.
+template <int RB, typename T>
+SUS2_HD void chebyshev(T xi, T* t) {
+  t[0] = T(1);
+  if (RB > 1) t[1] = xi;
+#pragma unroll
+  for (int n = 2; n < RB; ++n) t[n] = T(2) * xi * t[n - 1] - t[n - 2];
+}
+
+// T_n(xi) and dT_n/dxi, n < RB.
+template <int RB, typename T>
+SUS2_HD void chebyshev_d(T xi, T* t, T* dt) {
+  t[0] = T(1);
+  dt[0] = T(0);
+  if (RB > 1) {
+    t[1] = xi;
+    dt[1] = T(1);
+  }
+#pragma unroll
+  for (int n = 2; n < RB; ++n) {
+    t[n] = T(2) * xi * t[n - 1] - t[n - 2];
+    dt[n] = T(2) * (t[n - 1] + xi * dt[n - 1]) - dt[n - 2];
+  }
+}
+
+}  // namespace sus2sh

@@ -1,0 +1,51 @@
+"""Seeded synthetic SUS2-SH models of the benchmark workloads.
+
+The reference's trained Cu-Zr models are not shipped, so every workload uses a
+model written by ``sus2sh_write_synthetic_model`` (standard real-CG graph,
+random coefficients).  Choices not fixed by the workload description are
+recorded here: species_coeffs = 1, radial type coefficients = 1, every radial
+(scal, shift) = (1.0, (r_min + rc)/2), and the Al site shift -3.0 eV.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import _lib
+
+# name -> writer arguments
+PRESETS = {
+    # l3k3 Cu-Zr body-4 model: L=3, K=3, Chebyshev-sss rb=8, r_min 2.0, rc 5.0
+    "l3k3": dict(species=2, l_max=3, k_max=3, body_order=4, rb_size=8, r_min=2.0, rc=5.0,
+                 rational=0, shift=(-3.5, -5.0), radial_sigma=0.1, moment_sigma=0.01, seed=20260101),
+    # second seeded model of the same shape (targets of the loss workload)
+    "l3k3_target": dict(species=2, l_max=3, k_max=3, body_order=4, rb_size=8, r_min=2.0, rc=5.0,
+                        rational=0, shift=(-3.5, -5.0), radial_sigma=0.1, moment_sigma=0.01, seed=20260202),
+    # Cu-Zr-Al body-5 model: L=4, K=4, Chebyshev-sss-rational rb=10, rc 6.0
+    "l4k4": dict(species=3, l_max=4, k_max=4, body_order=5, rb_size=10, r_min=2.0, rc=6.0,
+                 rational=1, shift=(-3.5, -5.0, -3.0), radial_sigma=0.1, moment_sigma=0.01, seed=20260303),
+}
+
+
+def write_model(path: str, species=2, l_max=3, k_max=3, body_order=4, rb_size=8, r_min=2.0, rc=5.0,
+                rational=0, shift=(-3.5, -5.0), radial_sigma=0.1, moment_sigma=0.01, scal=1.0,
+                rshift=-1.0, seed=0, body_l_max=None) -> str:
+    lib = _lib.load()
+    sh = (ctypes.c_double * species)(*shift)
+    bl = (ctypes.c_int * len(body_l_max))(*body_l_max) if body_l_max else None
+    _lib.check(lib.sus2sh_write_synthetic_model(
+        path.encode(), species, l_max, k_max, body_order, ctypes.cast(bl, ctypes.c_void_p) if bl else None,
+        len(body_l_max) if body_l_max else 0, rb_size, r_min, rc, rational,
+        ctypes.cast(sh, ctypes.c_void_p), radial_sigma, moment_sigma, scal, rshift,
+        ctypes.c_ulonglong(seed)), "sus2sh_write_synthetic_model")
+    return path
+
+
+def preset_model(name: str, directory: str) -> str:
+    """Writes preset ``name`` into ``directory`` (once) and returns the path."""
+    os.makedirs(directory, exist_ok=True)
+    path = os.path.join(directory, f"{name}.mtp")
+    if not os.path.exists(path):
+        write_model(path + ".tmp", **PRESETS[name])
+        os.replace(path + ".tmp", path)
+    return path

@@ -1,0 +1,113 @@
+/*
+ * sus2sh.h - C ABI of the B200 SUS2-SH energy/force/virial engine.
+ *
+ * This is the drop-in boundary for GPUMD's potential dispatch.  Each entry
+ * point names the reference (hu-yanxiao/GPUMD-SUS2-SH) interface it replaces.
+ * All device arrays use GPUMD's layouts:
+ *   position  double[3N]  SoA  x0..x_{N-1}, y..., z...
+ *   type      int[N]      species index in [0, species_count)
+ *   potential double[N]   per-atom energy (eV)
+ *   force     double[3N]  SoA (eV/A)
+ *   virial    double[9N]  SoA, component order xx yy zz xy xz yz yx zx zy
+ *   box_h     double[9]   GPUMD Box::cpu_h: columns a=(h0,h3,h6), b=(h1,h4,h7), c=(h2,h5,h8)
+ *   pbc       int[3]      1 = periodic
+ * sus2sh_compute ACCUMULATES (+=) into potential/force/virial exactly like
+ * SUS2_SH::compute; the caller zeroes them (GPUMD's Force::compute does,
+ * src/force/force.cu:513-519).
+ *
+ * Return codes: 0 success, negative error (message via sus2sh_last_error()).
+ * A handle is not re-entrant; all work is enqueued on the stream passed in
+ * (cudaStream_t given as void*, NULL = legacy default stream).
+ */
+#ifndef SUS2SH_H
+#define SUS2SH_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sus2sh_handle sus2sh_handle;
+
+#define SUS2SH_OK 0
+#define SUS2SH_E_INPUT (-1)     /* malformed/unsupported model or options */
+#define SUS2SH_E_CUDA (-2)      /* CUDA runtime error */
+#define SUS2SH_E_ARG (-3)       /* invalid argument */
+#define SUS2SH_E_NEIGHBOR (-4)  /* neighbour capacity exceeded; recompute */
+
+/* status flags returned by sus2sh_sync */
+#define SUS2SH_STATUS_OVERFLOW 1
+
+/* Replaces is_sus2_sh_potential_file (src/force/sus2_sh.cu:7771-7780,
+ * declared src/force/sus2_sh.cuh:205): 1 if the file contains
+ * "potential_tag = SUS2-SH", else 0. */
+int sus2sh_is_sus2_sh_file(const char* path);
+
+/* Replaces SUS2_SH::SUS2_SH(const char* file_potential, int num_atoms,
+ * int num_potential_options, const char** potential_options)
+ * (src/force/sus2_sh.cuh:12-16, src/force/sus2_sh.cu:7782-9469).
+ * opts are the run.in tokens after the model file: the species symbols first,
+ * then key=value options (sus2_float=0|1; the reference's tuning switches are
+ * accepted and ignored; sus2_sh_skin=<A>, sus2_sh_rebuild_interval=<n>). */
+int sus2sh_create(const char* path, int num_atoms, int nopts, const char** opts,
+                  sus2sh_handle** out);
+
+/* Replaces SUS2_SH::compute(Box&, const GPU_Vector<int>& type,
+ * const GPU_Vector<double>& position, GPU_Vector<double>& potential,
+ * GPU_Vector<double>& force, GPU_Vector<double>& virial)
+ * (src/force/sus2_sh.cuh:19-25, src/force/sus2_sh.cu:9620-10675).
+ * Device pointers; accumulates into potential, force, virial. */
+int sus2sh_compute(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3],
+                   const int* type, const double* position, double* potential,
+                   double* force, double* virial, void* stream);
+
+/* Replaces SUS2_SH::~SUS2_SH (src/force/sus2_sh.cuh:17). */
+void sus2sh_destroy(sus2sh_handle* h);
+
+/* Replaces the Potential::rc member the reference sets from max_dist
+ * (src/force/sus2_sh.cu:7814). */
+double sus2sh_cutoff(const sus2sh_handle* h);
+
+/* Message of the last error on this thread (the reference prints it and
+ * exits, src/force/sus2_sh.cu:269-273). */
+const char* sus2sh_last_error(void);
+
+/* Waits for the handle's queued work and reports neighbour-list status
+ * (SUS2SH_STATUS_OVERFLOW when a list was truncated; the next call then
+ * rebuilds with a larger capacity).  The reference has no counterpart: its
+ * neighbour capacity is fixed at 512 (src/force/sus2_sh.cuh:68). */
+int sus2sh_sync(sus2sh_handle* h, int* status_flags);
+
+/* Forward/backward pair behind the force path (the explicit adjoint of
+ * SUS2_SH::compute's basic -> product -> force stages,
+ * src/force/sus2_sh.cu:10258-10469).
+ * forward:  potential[i] = E_i (assigned, not accumulated).
+ * backward: grad_position = sum_i w_i dE_i/dr (assigned; w = grad_potential,
+ *           NULL means all ones) and, if virial != NULL, the per-atom virial
+ *           of sum_i w_i E_i (assigned).  Uses the state of the last forward. */
+int sus2sh_forward(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3],
+                   const int* type, const double* position, double* potential, void* stream);
+int sus2sh_backward(sus2sh_handle* h, const double* grad_potential, double* grad_position,
+                    double* virial, void* stream);
+
+/* Host-buffer variant of sus2sh_compute for callers without device arrays:
+ * copies type/position in, evaluates, and copies per-atom energy, forces and
+ * the total virial (9 values, xx yy zz xy xz yz yx zx zy) out.  Outputs are
+ * assigned.  Pinned host buffers make the copies asynchronous-capable. */
+int sus2sh_compute_host(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3],
+                        const int* type, const double* position, double* potential,
+                        double* force, double* virial_total, void* stream);
+
+/* Model/graph statistics for logging (the reference prints them at
+ * construction, src/force/sus2_sh.cu:9339-9466).  Fills up to n ints:
+ * [0] species [1] l_max [2] k_max [3] body_order [4] rb_size [5] basics
+ * [6] moments [7] products [8] scalars [9] rows [10] layers
+ * [11] terminal scalar rows [12] program value slots [13] program rows
+ * [14] standard graph matched [15] use_float [16] neighbour capacity
+ * [17] neighbour builds so far.  Returns the number written. */
+int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUS2SH_H */

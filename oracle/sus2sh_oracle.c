@@ -1,0 +1,513 @@
+/*
+ * Oracle (test infrastructure only): FP64 CPU evaluation of SUS2-SH site
+ * energies, forces and per-atom virials.  Only tests/, __graft_entry__.smoke()
+ * and bench.py's CPU-baseline leg load this library; the product path never
+ * does.
+ *
+ * Restates the reference algorithm of hu-yanxiao/GPUMD-SUS2-SH
+ * (src/force/sus2_sh.cu) in its simplest correct form:
+ *   neighbours   every image j with |r_j - r_i + shift|^2 < rc^2 (strict),
+ *                i == j allowed for non-zero images      (:7668-7769)
+ *   radial       x = tanh(scal (r - s)/2) (or z/sqrt(1+z^2)),
+ *                R = s_pair (r - rc)^2 sum_n c_n T_n(x)   (:3171-3220, :2484-2517)
+ *                computed in FP64 throughout (no FP32 tables)
+ *   harmonics    Y_lm = c P_lm(x,y,z) / r^l, gradient by the quotient rule
+ *                (:2782-2808, :3032-3169)
+ *   basics       B_b = sum_j R_mu(b) Y_lm(b)               (:3486-3550)
+ *   products     flat, in file order, M[t] += c M[l] M[r]  (:4813-4821)
+ *   energy       E_i = shift_t + c_t + c_t sum_s w_s M[map_s]   (:4823-4832)
+ *   adjoint      g[map_s] += c_t w_s, then products reversed (:4830-4845)
+ *   forces       dE = sum_b g_b (R' d/r Y + R grad Y); F_i += dE, F_j -= dE,
+ *                W_i -= d (x) dE, order xx yy zz xy xz yz yx zx zy (:6388-6445)
+ * Outputs are assigned.  OpenMP over centre atoms.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+  int S, L, K, rb, kmu, M, nbasic, nscalar, nprod, rational;
+  double rc;
+  const double* radial;   /* [kmu][rb] */
+  const double* scal;     /* [S*S][kmu] */
+  const double* rshift;   /* [S*S][kmu] */
+  const double* pscale;   /* [S*S] */
+  const int* basic_mu;    /* [nbasic] */
+  const int* basic_y;     /* [nbasic] flat harmonic index l*l+l+m */
+  const int* prod_l;
+  const int* prod_r;
+  const int* prod_t;
+  const double* prod_c;   /* [nprod] */
+  const int* map;         /* [nscalar] */
+  const double* w;        /* [nscalar] */
+  const double* shift_e;  /* [S] */
+  const double* species;  /* [S] */
+} OracleModel;
+
+/* ---- real harmonics: value c*P/r^l and gradient ------------------------- */
+/* P and grad P for each (l, m), homogeneous Cartesian polynomials. */
+static void poly(int idx, double x, double y, double z, double* p, double* gx, double* gy, double* gz) {
+  const double x2 = x * x, y2 = y * y, z2 = z * z;
+  switch (idx) {
+    case 0: *p = 1; *gx = 0; *gy = 0; *gz = 0; return;
+    case 1: *p = y; *gx = 0; *gy = 1; *gz = 0; return;
+    case 2: *p = z; *gx = 0; *gy = 0; *gz = 1; return;
+    case 3: *p = x; *gx = 1; *gy = 0; *gz = 0; return;
+    case 4: *p = x * y; *gx = y; *gy = x; *gz = 0; return;
+    case 5: *p = y * z; *gx = 0; *gy = z; *gz = y; return;
+    case 6: *p = 2 * z2 - x2 - y2; *gx = -2 * x; *gy = -2 * y; *gz = 4 * z; return;
+    case 7: *p = x * z; *gx = z; *gy = 0; *gz = x; return;
+    case 8: *p = x2 - y2; *gx = 2 * x; *gy = -2 * y; *gz = 0; return;
+    case 9: *p = 3 * x2 * y - y * y2; *gx = 6 * x * y; *gy = 3 * x2 - 3 * y2; *gz = 0; return;
+    case 10: *p = x * y * z; *gx = y * z; *gy = x * z; *gz = x * y; return;
+    case 11: *p = 4 * y * z2 - x2 * y - y * y2; *gx = -2 * x * y; *gy = 4 * z2 - x2 - 3 * y2; *gz = 8 * y * z; return;
+    case 12: *p = 2 * z * z2 - 3 * x2 * z - 3 * y2 * z; *gx = -6 * x * z; *gy = -6 * y * z; *gz = 6 * z2 - 3 * x2 - 3 * y2; return;
+    case 13: *p = 4 * x * z2 - x * x2 - x * y2; *gx = 4 * z2 - 3 * x2 - y2; *gy = -2 * x * y; *gz = 8 * x * z; return;
+    case 14: *p = x2 * z - y2 * z; *gx = 2 * x * z; *gy = -2 * y * z; *gz = x2 - y2; return;
+    case 15: *p = x * x2 - 3 * x * y2; *gx = 3 * x2 - 3 * y2; *gy = -6 * x * y; *gz = 0; return;
+    case 16: *p = x * x2 * y - x * y * y2; *gx = 3 * x2 * y - y * y2; *gy = x * x2 - 3 * x * y2; *gz = 0; return;
+    case 17: *p = 3 * x2 * y * z - y * y2 * z; *gx = 6 * x * y * z; *gy = 3 * x2 * z - 3 * y2 * z; *gz = 3 * x2 * y - y * y2; return;
+    case 18: *p = 6 * x * y * z2 - x * x2 * y - x * y * y2;
+      *gx = 6 * y * z2 - 3 * x2 * y - y * y2; *gy = 6 * x * z2 - x * x2 - 3 * x * y2; *gz = 12 * x * y * z; return;
+    case 19: *p = 4 * y * z * z2 - 3 * x2 * y * z - 3 * y * y2 * z;
+      *gx = -6 * x * y * z; *gy = 4 * z * z2 - 3 * x2 * z - 9 * y2 * z; *gz = 12 * y * z2 - 3 * x2 * y - 3 * y * y2; return;
+    case 20: {
+      const double q = x2 + y2;
+      *p = 8 * z2 * z2 - 24 * z2 * q + 3 * q * q;
+      *gx = -48 * x * z2 + 12 * x * q; *gy = -48 * y * z2 + 12 * y * q; *gz = 32 * z * z2 - 48 * z * q; return;
+    }
+    case 21: *p = 4 * x * z * z2 - 3 * x * x2 * z - 3 * x * y2 * z;
+      *gx = 4 * z * z2 - 9 * x2 * z - 3 * y2 * z; *gy = -6 * x * y * z; *gz = 12 * x * z2 - 3 * x * x2 - 3 * x * y2; return;
+    case 22: *p = 6 * x2 * z2 - 6 * y2 * z2 - x2 * x2 + y2 * y2;
+      *gx = 12 * x * z2 - 4 * x * x2; *gy = -12 * y * z2 + 4 * y * y2; *gz = 12 * x2 * z - 12 * y2 * z; return;
+    case 23: *p = x * x2 * z - 3 * x * y2 * z; *gx = 3 * x2 * z - 3 * y2 * z; *gy = -6 * x * y * z; *gz = x * x2 - 3 * x * y2; return;
+    case 24: *p = x2 * x2 - 6 * x2 * y2 + y2 * y2; *gx = 4 * x * x2 - 12 * x * y2; *gy = -12 * x2 * y + 4 * y * y2; *gz = 0; return;
+    default: *p = 0; *gx = *gy = *gz = 0; return;
+  }
+}
+
+static double ycoef(int idx) {
+  const double pi = 3.14159265358979323846;
+  switch (idx) {
+    case 0: return 0.5 / sqrt(pi);
+    case 1: case 2: case 3: return 0.5 * sqrt(3.0 / pi);
+    case 4: case 5: case 7: return 0.5 * sqrt(15.0 / pi);
+    case 6: return 0.25 * sqrt(5.0 / pi);
+    case 8: return 0.25 * sqrt(15.0 / pi);
+    case 9: case 15: return 0.25 * sqrt(35.0 / (2.0 * pi));
+    case 10: return 0.5 * sqrt(105.0 / pi);
+    case 11: case 13: return 0.25 * sqrt(21.0 / (2.0 * pi));
+    case 12: return 0.25 * sqrt(7.0 / pi);
+    case 14: return 0.25 * sqrt(105.0 / pi);
+    case 16: return 0.75 * sqrt(35.0 / pi);
+    case 17: case 23: return 0.75 * sqrt(35.0 / (2.0 * pi));
+    case 18: return 0.75 * sqrt(5.0 / pi);
+    case 19: case 21: return 0.75 * sqrt(5.0 / (2.0 * pi));
+    case 20: return 0.1875 / sqrt(pi);
+    case 22: return 0.375 * sqrt(5.0 / pi);
+    case 24: return 0.1875 * sqrt(35.0 / pi);
+    default: return 0.0;
+  }
+}
+
+static int l_of(int idx) { return idx < 1 ? 0 : idx < 4 ? 1 : idx < 9 ? 2 : idx < 16 ? 3 : 4; }
+
+/* Y[idx] and dY[3*idx+a] at displacement d (not normalised). */
+void oracle_real_sh(int L, double x, double y, double z, double* Y, double* dY) {
+  const double r2 = x * x + y * y + z * z;
+  const double r = sqrt(r2);
+  const int C = (L + 1) * (L + 1);
+  for (int idx = 0; idx < C; ++idx) {
+    double p, gx, gy, gz;
+    poly(idx, x, y, z, &p, &gx, &gy, &gz);
+    const int l = l_of(idx);
+    const double c = ycoef(idx);
+    const double rl = pow(r, -l);
+    Y[idx] = c * p * rl;
+    if (dY) {
+      const double dr = -l * rl / r2;  /* d(r^-l)/dx_a = -l r^(-l-2) x_a */
+      dY[3 * idx + 0] = c * (gx * rl + p * dr * x);
+      dY[3 * idx + 1] = c * (gy * rl + p * dr * y);
+      dY[3 * idx + 2] = c * (gz * rl + p * dr * z);
+    }
+  }
+}
+
+/* R_mu and dR_mu/dr for one pair (FP64). */
+void oracle_radial(const OracleModel* m, int pair, double r, double* R, double* dR) {
+  const double dr = r - m->rc;
+  const double f = m->pscale[pair] * dr * dr;
+  const double df = 2.0 * m->pscale[pair] * dr;
+  double t[32], dt[32];
+  for (int mu = 0; mu < m->kmu; ++mu) {
+    const double sc = m->scal[pair * m->kmu + mu];
+    const double z = 0.5 * sc * (r - m->rshift[pair * m->kmu + mu]);
+    double xi, dxdr;
+    if (m->rational) {
+      const double q = 1.0 / sqrt(1.0 + z * z);
+      xi = z * q;
+      dxdr = 0.5 * sc * q * q * q;
+    } else {
+      xi = tanh(z);
+      dxdr = 0.5 * sc * (1.0 - xi * xi);
+    }
+    t[0] = 1.0;
+    dt[0] = 0.0;
+    if (m->rb > 1) {
+      t[1] = xi;
+      dt[1] = 1.0;
+    }
+    for (int n = 2; n < m->rb; ++n) {
+      t[n] = 2.0 * xi * t[n - 1] - t[n - 2];
+      dt[n] = 2.0 * t[n - 1] + 2.0 * xi * dt[n - 1] - dt[n - 2];
+    }
+    double s = 0.0, sd = 0.0;
+    for (int n = 0; n < m->rb; ++n) {
+      s += m->radial[mu * m->rb + n] * t[n];
+      sd += m->radial[mu * m->rb + n] * dt[n];
+    }
+    R[mu] = f * s;
+    if (dR) dR[mu] = df * s + f * sd * dxdr;
+  }
+}
+
+/* ---- neighbours ---------------------------------------------------------- */
+typedef struct {
+  int j;
+  double d[3];
+} Edge;
+
+typedef struct {
+  double h[9], hinv[9];
+  int pbc[3];
+  int n[3];       /* cells */
+  int reach[3];   /* image range for brute force */
+  int use_cells;
+} Geo;
+
+static void inv3(const double* h, double* o) {
+  const double det = h[0] * (h[4] * h[8] - h[5] * h[7]) - h[1] * (h[3] * h[8] - h[5] * h[6]) +
+                     h[2] * (h[3] * h[7] - h[4] * h[6]);
+  const double id = 1.0 / det;
+  o[0] = (h[4] * h[8] - h[5] * h[7]) * id;
+  o[1] = (h[2] * h[7] - h[1] * h[8]) * id;
+  o[2] = (h[1] * h[5] - h[2] * h[4]) * id;
+  o[3] = (h[5] * h[6] - h[3] * h[8]) * id;
+  o[4] = (h[0] * h[8] - h[2] * h[6]) * id;
+  o[5] = (h[2] * h[3] - h[0] * h[5]) * id;
+  o[6] = (h[3] * h[7] - h[4] * h[6]) * id;
+  o[7] = (h[1] * h[6] - h[0] * h[7]) * id;
+  o[8] = (h[0] * h[4] - h[1] * h[3]) * id;
+}
+
+static void geo_init(Geo* g, const double* h, const int* pbc, double rc) {
+  memcpy(g->h, h, sizeof(g->h));
+  inv3(h, g->hinv);
+  const double a[3] = {h[0], h[3], h[6]}, b[3] = {h[1], h[4], h[7]}, c[3] = {h[2], h[5], h[8]};
+  const double* v[3][2] = {{b, c}, {c, a}, {a, b}};
+  const double vol = fabs(a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) +
+                          a[2] * (b[0] * c[1] - b[1] * c[0]));
+  g->use_cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    const double* u = v[d][0];
+    const double* w = v[d][1];
+    const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+    const double thick = vol / sqrt(cx * cx + cy * cy + cz * cz);
+    g->pbc[d] = pbc[d] ? 1 : 0;
+    g->reach[d] = g->pbc[d] ? (int)ceil(rc / thick) : 0;
+    if (g->reach[d] < 1 && g->pbc[d]) g->reach[d] = 1;
+    int n = (int)floor(thick / rc);
+    if (n < 1) n = 1;
+    if (n > 512) n = 512;
+    g->n[d] = n;
+    if (g->pbc[d] && n < 3) g->use_cells = 0;
+  }
+}
+
+/* Collects the neighbours of every atom; returns per-atom arrays. */
+typedef struct {
+  int* start;  /* [N+1] */
+  Edge* e;
+} NList;
+
+static void frac(const Geo* g, const double* p, double* s) {
+  for (int a = 0; a < 3; ++a) s[a] = g->hinv[3 * a] * p[0] + g->hinv[3 * a + 1] * p[1] + g->hinv[3 * a + 2] * p[2];
+}
+
+static int build_nlist(const Geo* g, int N, const double* pos, double rc, NList* out) {
+  const double rc2 = rc * rc;
+  int* cnt = (int*)calloc((size_t)N + 1, sizeof(int));
+  Edge** per = (Edge**)calloc((size_t)N, sizeof(Edge*));
+  int* capv = (int*)calloc((size_t)N, sizeof(int));
+  if (!cnt || !per || !capv) return -1;
+  int ncell = 1, *cstart = NULL, *catoms = NULL, *cell_of = NULL;
+  if (g->use_cells) {
+    ncell = g->n[0] * g->n[1] * g->n[2];
+    cstart = (int*)calloc((size_t)ncell + 1, sizeof(int));
+    catoms = (int*)malloc(sizeof(int) * (size_t)N);
+    cell_of = (int*)malloc(sizeof(int) * (size_t)N);
+    for (int i = 0; i < N; ++i) {
+      double p[3] = {pos[i], pos[i + N], pos[i + 2 * N]}, s[3];
+      frac(g, p, s);
+      int c[3];
+      for (int a = 0; a < 3; ++a) {
+        if (g->pbc[a]) s[a] -= floor(s[a]);
+        c[a] = (int)floor(s[a] * g->n[a]);
+        if (c[a] < 0) c[a] = 0;
+        if (c[a] >= g->n[a]) c[a] = g->n[a] - 1;
+      }
+      cell_of[i] = (c[2] * g->n[1] + c[1]) * g->n[0] + c[0];
+      cstart[cell_of[i] + 1]++;
+    }
+    for (int c = 0; c < ncell; ++c) cstart[c + 1] += cstart[c];
+    int* fillp = (int*)malloc(sizeof(int) * (size_t)ncell);
+    memcpy(fillp, cstart, sizeof(int) * (size_t)ncell);
+    for (int i = 0; i < N; ++i) catoms[fillp[cell_of[i]]++] = i;
+    free(fillp);
+  }
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < N; ++i) {
+    const double pi[3] = {pos[i], pos[i + N], pos[i + 2 * N]};
+    int k = 0, cap = 64;
+    Edge* e = (Edge*)malloc(sizeof(Edge) * cap);
+    if (g->use_cells) {
+      /* wrapped fractional coordinate of i decides its cell; neighbours are
+       * searched through the 27 surrounding cells with explicit images */
+      double s[3];
+      frac(g, pi, s);
+      int ci[3];
+      double wi[3];
+      for (int a = 0; a < 3; ++a) {
+        wi[a] = g->pbc[a] ? floor(s[a]) : 0.0;
+        double t = s[a] - wi[a];
+        ci[a] = (int)floor(t * g->n[a]);
+        if (ci[a] < 0) ci[a] = 0;
+        if (ci[a] >= g->n[a]) ci[a] = g->n[a] - 1;
+      }
+      for (int oz = -1; oz <= 1; ++oz)
+        for (int oy = -1; oy <= 1; ++oy)
+          for (int ox = -1; ox <= 1; ++ox) {
+            int o[3] = {ox, oy, oz}, cc[3], sh[3];
+            int skip = 0;
+            for (int a = 0; a < 3; ++a) {
+              int v = ci[a] + o[a];
+              sh[a] = 0;
+              if (g->pbc[a]) {
+                if (v < 0) { v += g->n[a]; sh[a] = -1; }
+                else if (v >= g->n[a]) { v -= g->n[a]; sh[a] = 1; }
+              } else if (v < 0 || v >= g->n[a]) {
+                skip = 1;
+              }
+              cc[a] = v;
+            }
+            if (skip) continue;
+            const int c = (cc[2] * g->n[1] + cc[1]) * g->n[0] + cc[0];
+            for (int q = cstart[c]; q < cstart[c + 1]; ++q) {
+              const int j = catoms[q];
+              const double pj[3] = {pos[j], pos[j + N], pos[j + 2 * N]};
+              double sj[3];
+              frac(g, pj, sj);
+              double t[3];
+              for (int a = 0; a < 3; ++a) {
+                const double wj = g->pbc[a] ? floor(sj[a]) : 0.0;
+                /* image of j: wrapped j shifted by the cell-wrap, relative to wrapped i */
+                t[a] = (double)sh[a] - wj + wi[a];
+              }
+              double d[3];
+              for (int a = 0; a < 3; ++a)
+                d[a] = pj[a] - pi[a] + g->h[3 * a] * t[0] + g->h[3 * a + 1] * t[1] + g->h[3 * a + 2] * t[2];
+              if (j == i && t[0] == 0 && t[1] == 0 && t[2] == 0) continue;
+              const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+              if (r2 < rc2) {
+                if (k == cap) { cap *= 2; e = (Edge*)realloc(e, sizeof(Edge) * cap); }
+                e[k].j = j;
+                e[k].d[0] = d[0]; e[k].d[1] = d[1]; e[k].d[2] = d[2];
+                ++k;
+              }
+            }
+          }
+    } else {
+      for (int j = 0; j < N; ++j) {
+        const double d0[3] = {pos[j] - pi[0], pos[j + N] - pi[1], pos[j + 2 * N] - pi[2]};
+        for (int tx = -g->reach[0]; tx <= g->reach[0]; ++tx)
+          for (int ty = -g->reach[1]; ty <= g->reach[1]; ++ty)
+            for (int tz = -g->reach[2]; tz <= g->reach[2]; ++tz) {
+              if (j == i && tx == 0 && ty == 0 && tz == 0) continue;
+              double d[3];
+              for (int a = 0; a < 3; ++a)
+                d[a] = d0[a] + g->h[3 * a] * tx + g->h[3 * a + 1] * ty + g->h[3 * a + 2] * tz;
+              const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+              if (r2 < rc2) {
+                if (k == cap) { cap *= 2; e = (Edge*)realloc(e, sizeof(Edge) * cap); }
+                e[k].j = j;
+                e[k].d[0] = d[0]; e[k].d[1] = d[1]; e[k].d[2] = d[2];
+                ++k;
+              }
+            }
+      }
+    }
+    per[i] = e;
+    capv[i] = k;
+  }
+  out->start = (int*)malloc(sizeof(int) * ((size_t)N + 1));
+  out->start[0] = 0;
+  for (int i = 0; i < N; ++i) out->start[i + 1] = out->start[i] + capv[i];
+  out->e = (Edge*)malloc(sizeof(Edge) * ((size_t)out->start[N] + 1));
+  for (int i = 0; i < N; ++i) {
+    memcpy(out->e + out->start[i], per[i], sizeof(Edge) * (size_t)capv[i]);
+    free(per[i]);
+  }
+  free(per);
+  free(capv);
+  free(cnt);
+  free(cstart);
+  free(catoms);
+  free(cell_of);
+  return 0;
+}
+
+/* ---- energy / forces / virial -------------------------------------------- */
+int oracle_efs(const OracleModel* m, int N, const double* h, const int* pbc, const int* type,
+               const double* pos, double* pe, double* f, double* vir, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int nt = omp_get_max_threads();
+#else
+  (void)nthreads;
+  const int nt = 1;
+#endif
+  Geo g;
+  geo_init(&g, h, pbc, m->rc);
+  NList nl;
+  if (build_nlist(&g, N, pos, m->rc, &nl) != 0) return -1;
+  double* fbuf = (double*)calloc((size_t)nt * 3 * N, sizeof(double));
+  if (!fbuf) return -1;
+  const int C = (m->L + 1) * (m->L + 1);
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num();
+#else
+    const int tid = 0;
+#endif
+    double* fl = fbuf + (size_t)tid * 3 * N;
+    double* Mv = (double*)malloc(sizeof(double) * m->M);
+    double* gv = (double*)malloc(sizeof(double) * m->M);
+    double R[64], dR[64], Y[32], dY[96];
+#pragma omp for schedule(dynamic, 32)
+    for (int i = 0; i < N; ++i) {
+      const int ti = type[i];
+      memset(Mv, 0, sizeof(double) * m->M);
+      for (int q = nl.start[i]; q < nl.start[i + 1]; ++q) {
+        const Edge* e = nl.e + q;
+        const double r = sqrt(e->d[0] * e->d[0] + e->d[1] * e->d[1] + e->d[2] * e->d[2]);
+        oracle_radial(m, ti * m->S + type[e->j], r, R, NULL);
+        oracle_real_sh(m->L, e->d[0], e->d[1], e->d[2], Y, NULL);
+        for (int b = 0; b < m->nbasic; ++b) Mv[b] += R[m->basic_mu[b]] * Y[m->basic_y[b]];
+      }
+      for (int p = 0; p < m->nprod; ++p) Mv[m->prod_t[p]] += m->prod_c[p] * Mv[m->prod_l[p]] * Mv[m->prod_r[p]];
+      const double ct = m->species[ti];
+      double E = m->shift_e[ti] + ct;
+      memset(gv, 0, sizeof(double) * m->M);
+      for (int s = 0; s < m->nscalar; ++s) {
+        E += ct * m->w[s] * Mv[m->map[s]];
+        gv[m->map[s]] += ct * m->w[s];
+      }
+      pe[i] = E;
+      for (int p = m->nprod - 1; p >= 0; --p) {
+        const double gt = gv[m->prod_t[p]] * m->prod_c[p];
+        gv[m->prod_l[p]] += gt * Mv[m->prod_r[p]];
+        gv[m->prod_r[p]] += gt * Mv[m->prod_l[p]];
+      }
+      double w9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int q = nl.start[i]; q < nl.start[i + 1]; ++q) {
+        const Edge* e = nl.e + q;
+        const double dx = e->d[0], dy = e->d[1], dz = e->d[2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        oracle_radial(m, ti * m->S + type[e->j], r, R, dR);
+        oracle_real_sh(m->L, dx, dy, dz, Y, dY);
+        double ex = 0, ey = 0, ez = 0;
+        for (int b = 0; b < m->nbasic; ++b) {
+          const double a = gv[b];
+          if (a == 0.0) continue;
+          const int mu = m->basic_mu[b], y = m->basic_y[b];
+          ex += a * (dR[mu] * dx / r * Y[y] + R[mu] * dY[3 * y + 0]);
+          ey += a * (dR[mu] * dy / r * Y[y] + R[mu] * dY[3 * y + 1]);
+          ez += a * (dR[mu] * dz / r * Y[y] + R[mu] * dY[3 * y + 2]);
+        }
+        fl[i] += ex;
+        fl[i + N] += ey;
+        fl[i + 2 * N] += ez;
+        fl[e->j] -= ex;
+        fl[e->j + N] -= ey;
+        fl[e->j + 2 * N] -= ez;
+        w9[0] -= dx * ex;
+        w9[1] -= dy * ey;
+        w9[2] -= dz * ez;
+        w9[3] -= dx * ey;
+        w9[4] -= dx * ez;
+        w9[5] -= dy * ez;
+        w9[6] -= dy * ex;
+        w9[7] -= dz * ex;
+        w9[8] -= dz * ey;
+      }
+      for (int k = 0; k < 9; ++k) vir[(size_t)k * N + i] = w9[k];
+    }
+    free(Mv);
+    free(gv);
+  }
+  for (int a = 0; a < 3 * N; ++a) {
+    double s = 0.0;
+    for (int t = 0; t < nt; ++t) s += fbuf[(size_t)t * 3 * N + a];
+    f[a] = s;
+  }
+  (void)C;
+  free(fbuf);
+  free(nl.start);
+  free(nl.e);
+  return 0;
+}
+
+/* Basic moments only (for kernel-level parity checks): B[b*N+i]. */
+int oracle_basics(const OracleModel* m, int N, const double* h, const int* pbc, const int* type,
+                  const double* pos, double* B, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  Geo g;
+  geo_init(&g, h, pbc, m->rc);
+  NList nl;
+  if (build_nlist(&g, N, pos, m->rc, &nl) != 0) return -1;
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int i = 0; i < N; ++i) {
+    double R[64], Y[32];
+    for (int b = 0; b < m->nbasic; ++b) B[(size_t)b * N + i] = 0.0;
+    for (int q = nl.start[i]; q < nl.start[i + 1]; ++q) {
+      const Edge* e = nl.e + q;
+      const double r = sqrt(e->d[0] * e->d[0] + e->d[1] * e->d[1] + e->d[2] * e->d[2]);
+      oracle_radial(m, type[i] * m->S + type[e->j], r, R, NULL);
+      oracle_real_sh(m->L, e->d[0], e->d[1], e->d[2], Y, NULL);
+      for (int b = 0; b < m->nbasic; ++b) B[(size_t)b * N + i] += R[m->basic_mu[b]] * Y[m->basic_y[b]];
+    }
+  }
+  free(nl.start);
+  free(nl.e);
+  return 0;
+}
+
+/* Neighbour count per atom within rc (for neighbour-list parity). */
+int oracle_neighbor_counts(int N, const double* h, const int* pbc, const double* pos, double rc, int* counts) {
+  Geo g;
+  geo_init(&g, h, pbc, rc);
+  NList nl;
+  if (build_nlist(&g, N, pos, rc, &nl) != 0) return -1;
+  for (int i = 0; i < N; ++i) counts[i] = nl.start[i + 1] - nl.start[i];
+  free(nl.start);
+  free(nl.e);
+  return 0;
+}

@@ -1,0 +1,221 @@
+"""Parity of the CUDA engine (through the C-ABI) with the FP64 oracle.
+
+Bars: FP32 engine within 1e-6 eV/atom energy and
+1e-5 eV/A force RMS of the FP64 oracle; the FP64 engine within 1e-9.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+import sus2sh_oracle as O  # noqa: E402
+from sus2sh import SUS2_SH, Box, structures  # noqa: E402
+
+E_TOL32 = 1e-6      # eV/atom
+F_RMS32 = 1e-5      # eV/A
+W_RMS32 = 5e-5      # eV per atom virial component
+TOL64 = 1e-9
+
+
+def engine_efs(path, box, types, pos, opts=(), species=("Cu", "Zr")):
+    N = types.size
+    pot = SUS2_SH(path, N, [*species, *opts])
+    dev = torch.device("cuda")
+    t = torch.as_tensor(types.astype(np.int32), device=dev)
+    x = torch.as_tensor(np.ascontiguousarray(pos).reshape(-1), device=dev)
+    pe = torch.zeros(N, dtype=torch.float64, device=dev)
+    f = torch.zeros(3 * N, dtype=torch.float64, device=dev)
+    w = torch.zeros(9 * N, dtype=torch.float64, device=dev)
+    pot.compute(box, t, x, pe, f, w)
+    torch.cuda.synchronize()
+    assert pot.sync() == 0
+    out = pe.cpu().numpy(), f.cpu().numpy().reshape(3, N), w.cpu().numpy().reshape(9, N)
+    pot.close()
+    return out
+
+
+def compare(path, box, types, pos, opts=(), species=("Cu", "Zr"), fp64=False):
+    orc = O.Oracle(path)
+    pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types, pos)
+    pe, f, w = engine_efs(path, box, types, pos, opts=opts + (("sus2_float=0",) if fp64 else ()),
+                          species=species)
+    de = np.abs(pe - pe0).max()
+    frms = np.sqrt(((f - f0) ** 2).mean())
+    wrms = np.sqrt(((w - w0) ** 2).mean())
+    if fp64:
+        assert de < TOL64 and np.abs(f - f0).max() < TOL64 * 10 and np.abs(w - w0).max() < TOL64 * 100, (de, frms, wrms)
+    else:
+        assert de < E_TOL32, de
+        assert frms < F_RMS32, frms
+        assert wrms < W_RMS32, wrms
+    return de, frms, wrms
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_config0_fcc_2048(l3k3_path, fp64):
+    box, types, pos = structures.fcc(8, 8, 8, 3.8, (0.5, 0.5), 0.05, seed=1)
+    compare(l3k3_path, box, types, pos, fp64=fp64)
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_small_periodic_cell_images(l3k3_path, fp64):
+    # 3x3x3 FCC (11.4 A < 2 (rc + skin)): every neighbour image is explicit
+    box, types, pos = structures.fcc(3, 3, 3, 3.8, (0.5, 0.5), 0.1, seed=2)
+    compare(l3k3_path, box, types, pos, fp64=fp64)
+
+
+def test_tiny_random_cell(l3k3_path):
+    # 16 atoms at 0.06 A^-3 (edge about 6.4 A): images up to two boxes away
+    box, types, pos = structures.random_insertion(16, 0.06, 2.1, (0.8, 1.0, 1.25), seed=3)
+    compare(l3k3_path, box, types, pos)
+    compare(l3k3_path, box, types, pos, fp64=True)
+
+
+def test_triclinic_box(l3k3_path):
+    box, types, pos = structures.fcc(5, 5, 5, 3.8, (0.5, 0.5), 0.05, seed=4)
+    L = 19.0
+    h = np.array([[L, 1.7, -0.9], [0.0, L, 2.3], [0.0, 0.0, L]])
+    frac = np.linalg.solve(box.cpu_h.reshape(3, 3), pos)
+    tbox = Box(h.ravel())
+    compare(l3k3_path, tbox, types, h @ frac)
+
+
+def test_open_boundaries(l3k3_path):
+    box, types, pos = structures.fcc(3, 3, 3, 3.8, (0.5, 0.5), 0.1, seed=5)
+    obox = Box.orthorhombic(60.0, 60.0, 60.0, pbc=(0, 0, 0))
+    compare(l3k3_path, obox, types, pos + 20.0)
+    mixed = Box.orthorhombic(11.4, 60.0, 11.4, pbc=(1, 0, 1))
+    compare(l3k3_path, mixed, types, pos + np.array([[0.0], [20.0], [0.0]]))
+
+
+def test_large_model_rational_three_species(l4k4_path):
+    # body-5 L=4 K=4 graph: product slots live in HBM scratch
+    box, types, pos = structures.random_insertion(600, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=6)
+    compare(l4k4_path, box, types, pos, species=("Cu", "Zr", "Al"))
+    compare(l4k4_path, box, types, pos, species=("Cu", "Zr", "Al"), fp64=True)
+
+
+def test_reference_rounding_option(l3k3_path):
+    box, types, pos = structures.fcc(4, 4, 4, 3.8, (0.5, 0.5), 0.05, seed=7)
+    orc = O.Oracle(l3k3_path, reference_rounding=True)
+    pe0, f0, _ = orc.efs(box.cpu_h, box.pbc, types, pos)
+    pe, f, _ = engine_efs(l3k3_path, box, types, pos, opts=("sus2_float=0", "sus2_sh_reference_rounding=1"))
+    assert np.abs(pe - pe0).max() < 1e-9 and np.abs(f - f0).max() < 1e-8
+
+
+def test_accumulates_into_outputs(l3k3_path):
+    box, types, pos = structures.fcc(4, 4, 4, 3.8, (0.5, 0.5), 0.05, seed=8)
+    N = types.size
+    pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr"])
+    dev = torch.device("cuda")
+    t = torch.as_tensor(types, device=dev)
+    x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
+    pe = torch.full((N,), 1.5, dtype=torch.float64, device=dev)
+    f = torch.full((3 * N,), -0.25, dtype=torch.float64, device=dev)
+    w = torch.full((9 * N,), 2.0, dtype=torch.float64, device=dev)
+    pot.compute(box, t, x, pe, f, w)
+    torch.cuda.synchronize()
+    pe1, f1, w1 = engine_efs(l3k3_path, box, types, pos)
+    assert np.allclose(pe.cpu().numpy() - 1.5, pe1, atol=1e-12)
+    assert np.allclose(f.cpu().numpy() + 0.25, f1.ravel(), atol=1e-12)
+    assert np.allclose(w.cpu().numpy() - 2.0, w1.ravel(), atol=1e-12)
+
+
+def test_deterministic_energy(l3k3_path):
+    box, types, pos = structures.fcc(6, 6, 6, 3.8, (0.5, 0.5), 0.05, seed=9)
+    a = engine_efs(l3k3_path, box, types, pos)
+    b = engine_efs(l3k3_path, box, types, pos)
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[2], b[2])
+    assert np.abs(a[1] - b[1]).max() < 1e-6
+
+
+def test_md_steps_with_skin_rebuilds(l3k3_path):
+    from sus2sh.md import NVE
+    box, types, pos = structures.fcc(6, 6, 6, 3.8, (0.64, 0.36), 0.05, seed=10)
+    masses = [structures.AMU["Cu"], structures.AMU["Zr"]]
+    vel = structures.maxwell_boltzmann(types, masses, 2000.0, seed=11)  # hot: forces rebuilds
+    pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr", "sus2_sh_rebuild_interval=10"])
+    md = NVE(pot, box, types, pos, vel, masses, dt_fs=2.0)
+    md.initial_force()
+    for _ in range(40):
+        md.step()
+    torch.cuda.synchronize()
+    assert pot.sync() == 0
+    assert pot.info()["neighbor_builds"] >= 4
+    # the engine's forces at the final positions match the oracle there
+    xf = md.pos.view(3, -1).cpu().numpy()
+    orc = O.Oracle(l3k3_path)
+    pe0, f0, _ = orc.efs(box.cpu_h, box.pbc, types, xf)
+    assert np.abs(md.pe.cpu().numpy() - pe0).max() < E_TOL32
+    assert np.sqrt(((md.force.view(3, -1).cpu().numpy() - f0) ** 2).mean()) < F_RMS32
+
+
+def test_neighbor_overflow_is_reported_and_recovered(l3k3_path):
+    # dilute first frame sizes the list; a compressed cluster then overflows it
+    rng = np.random.default_rng(12)
+    N = 200
+    box = Box.orthorhombic(40.0, 40.0, 40.0)
+    pos = rng.uniform(0, 40.0, size=(3, N))
+    types = rng.integers(0, 2, N).astype(np.int32)
+    pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr"])
+    dev = torch.device("cuda")
+    t = torch.as_tensor(types, device=dev)
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)
+    pot.compute(box, t, torch.as_tensor(pos.reshape(-1).copy(), device=dev), z(N), z(3 * N), z(9 * N))
+    torch.cuda.synchronize()
+    assert pot.sync() == 0
+    dense = 15.0 + rng.uniform(0, 9.0, size=(3, N))  # ~0.27 A^-3 cluster
+    x = torch.as_tensor(dense.reshape(-1).copy(), device=dev)
+    pot.compute(box, t, x, z(N), z(3 * N), z(9 * N))
+    assert pot.sync() & 1  # overflow flagged, capacity grown
+    pe, f, w = z(N), z(3 * N), z(9 * N)
+    pot.compute(box, t, x, pe, f, w)
+    assert pot.sync() == 0
+    orc = O.Oracle(l3k3_path)
+    pe0, f0, _ = orc.efs(box.cpu_h, box.pbc, types, dense)
+    assert np.abs(pe.cpu().numpy() - pe0).max() < 1e-4 * max(1.0, np.abs(pe0).max())
+
+
+def test_autograd_backward_matches_forces_and_fd(l3k3_path):
+    from sus2sh.autograd import site_energy
+    box, types, pos = structures.fcc(3, 3, 3, 3.8, (0.5, 0.5), 0.1, seed=13)
+    N = types.size
+    dev = torch.device("cuda")
+    t = torch.as_tensor(types, device=dev)
+    orc = O.Oracle(l3k3_path)
+    pe0, f0, _ = orc.efs(box.cpu_h, box.pbc, types, pos)
+    for fp64 in (False, True):
+        pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr"] + (["sus2_float=0"] if fp64 else []))
+        x = torch.as_tensor(pos.reshape(-1).copy(), device=dev).requires_grad_(True)
+        e = site_energy(pot, box, t, x)
+        (g,) = torch.autograd.grad(e.sum(), x)
+        assert np.abs(e.detach().cpu().numpy() - pe0).max() < (1e-10 if fp64 else E_TOL32)
+        assert np.abs(g.cpu().numpy().reshape(3, N) + f0).max() < (1e-9 if fp64 else 1e-4)
+        # weighted energies: gradient vs central differences of the oracle
+        wts = np.random.default_rng(14).normal(size=N)
+        e = site_energy(pot, box, t, x)
+        (g,) = torch.autograd.grad((e * torch.as_tensor(wts, device=dev)).sum(), x)
+        g = g.cpu().numpy().reshape(3, N)
+        h = 1e-5
+        for i in (0, 7, 33):
+            for a in range(3):
+                p1 = pos.copy(); p1[a, i] += h
+                p2 = pos.copy(); p2[a, i] -= h
+                fd = (wts @ orc.efs(box.cpu_h, box.pbc, types, p1)[0]
+                      - wts @ orc.efs(box.cpu_h, box.pbc, types, p2)[0]) / (2 * h)
+                assert abs(fd - g[a, i]) < (1e-7 if fp64 else 1e-4)
+        pot.close()
+
+
+def test_host_buffer_entry_point(l3k3_path):
+    box, types, pos = structures.fcc(4, 4, 4, 3.8, (0.5, 0.5), 0.05, seed=15)
+    pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr"])
+    pe, f, vt = pot.compute_host(box, types, pos)
+    orc = O.Oracle(l3k3_path)
+    pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types, pos)
+    assert np.abs(pe - pe0).max() < E_TOL32
+    assert np.sqrt(((f - f0) ** 2).mean()) < F_RMS32
+    assert np.abs(vt - w0.sum(axis=1)).max() < 1e-3
