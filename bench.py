@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the SUS2-SH engine on the 1,024,000-atom Cu-Zr l3k3 NVE workload.
+
+Workload (seeded synthetic stand-in for the reference's unshipped model.xyz and
+p.mtp): FCC 80x80x40 cells, a = 3.8 A (1,024,000 atoms, box 304x304x152 A),
+64/36 Cu/Zr random species, Maxwell-Boltzmann velocities at 200 K, NVE with
+dt = 0.5 fs, Verlet skin 1.0 A and a forced neighbour rebuild every 10 steps.
+Model: SUS2-SH l3k3 body 4 (L=3, K=3, Chebyshev-sss rb 8, rc 5.0 A, 248
+moments, 806 CG products), random coefficients (radial ~N(0,0.1), moment
+weights ~N(0,0.01)).
+
+A step is one velocity-Verlet MD step (kick+drift, one energy/force/virial
+evaluation through the C-ABI, kick) over all atoms of this rank.  The FP32
+engine (sus2_float=1) is the headline; the plain FP64 engine (sus2_float=0)
+runs the same workload for the FP32/FP64 ratio.  Multi-GPU runs are
+independent replicas (weak scaling, no collective on the data path); timing is
+the max over ranks.
+
+--impl reference times the reference-semantics CPU evaluation (the FP64 oracle
+port; the reference itself cannot be built without an upstream GPUMD tree) on
+this host's cores, one force evaluation of a 6,912-atom sample of the same
+crystal and model per step.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "gpumd-sus2-sh_b200")
+ORACLE = os.path.join(REPO, "oracle")
+sys.path.insert(0, PKG)
+
+METRIC = "atom-step/s, 1.024M-atom l3k3: FP32 vs FP64 path; force RMS err vs FP64 oracle"
+CELLS = (80, 80, 40)
+A = 3.8
+DT = 0.5
+TEMP = 200.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
+    ap.add_argument("--fp64-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def edges_within(box, pos, rc):
+    """In-cutoff (directed) neighbour pairs of the structure, for the
+    algorithmic flop count."""
+    from scipy.spatial import cKDTree
+    L = box.lengths()
+    tree = cKDTree((pos.T % L), boxsize=L)
+    counts = tree.query_ball_point(pos.T % L, r=rc * (1 - 1e-12), return_length=True)
+    return int(counts.sum()) - pos.shape[1]  # minus self
+
+
+def flops_model(kmu, rb, C, Bb, P):
+    """Counting rule for algorithmic work (FMA = 2 flops)."""
+    per_edge_basic = kmu * (2 * rb + 4) + 6 * C + 2 * Bb
+    per_edge_force = kmu * (4 * rb + 6) + 20 * C + 8 * Bb + 24
+    per_atom_product = 9 * P
+    return per_edge_basic, per_edge_force, per_atom_product
+
+
+def fma_peak(lib):
+    v32, v64 = ctypes.c_double(0), ctypes.c_double(0)
+    lib.sus2sh_measure_fma_peak(0, ctypes.byref(v32))
+    lib.sus2sh_measure_fma_peak(1, ctypes.byref(v64))
+    return v32.value, v64.value
+
+
+def make_workload(model_dir, rank):
+    from sus2sh import models, structures
+    path = models.preset_model("l3k3", model_dir)
+    box, types, pos = structures.fcc(*CELLS_RUN, A, (0.64, 0.36), 0.0, seed=1000 + rank)
+    masses = [structures.AMU["Cu"], structures.AMU["Zr"]]
+    vel = structures.maxwell_boltzmann(types, masses, TEMP, seed=2000 + rank)
+    return path, box, types, pos, vel, masses
+
+
+def run_md(torch, path, box, types, pos, vel, masses, steps, warmup, fp64, world, clocks=None):
+    from sus2sh import SUS2_SH
+    from sus2sh.md import NVE
+    opts = ["Cu", "Zr", "sus2_sh_skin=1.0", "sus2_sh_rebuild_interval=10"] + (["sus2_float=0"] if fp64 else [])
+    pot = SUS2_SH(path, types.size, opts)
+    md = NVE(pot, box, types, pos, vel, masses, dt_fs=DT)
+    md.initial_force()
+    for _ in range(warmup):
+        md.step()
+    torch.cuda.synchronize()
+    if pot.sync() != 0:
+        raise RuntimeError("neighbour list overflow during warm-up")
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    pot.profile(True)
+    l0 = pot.info()["launches"]
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if clocks:
+        clocks.start()
+    s.record()
+    for _ in range(steps):
+        md.step()
+    e.record()
+    torch.cuda.synchronize()
+    if clocks:
+        clk = clocks.stop()
+    else:
+        clk = None
+    if world > 1:
+        torch.distributed.barrier()
+    ms = s.elapsed_time(e)
+    prof = pot.profile_read()
+    info = pot.info()
+    launches = info["launches"] - l0 + 2 * steps  # + kick_drift and kick
+    flags = pot.sync()
+    if flags:
+        raise RuntimeError(f"neighbour list status {flags} during timed steps")
+    return pot, md, ms, prof, launches, clk
+
+
+def force_error_vs_fp64(torch, path, box, types, x_dev):
+    """FP32 and FP64 engines on the same frame: force RMS and max |dE|/atom."""
+    from sus2sh import SUS2_SH
+    N = types.size
+    dev = x_dev.device
+    t = torch.as_tensor(types, device=dev)
+    out = []
+    for opt in ([], ["sus2_float=0"]):
+        pot = SUS2_SH(path, N, ["Cu", "Zr"] + opt)
+        pe = torch.zeros(N, dtype=torch.float64, device=dev)
+        f = torch.zeros(3 * N, dtype=torch.float64, device=dev)
+        w = torch.zeros(9 * N, dtype=torch.float64, device=dev)
+        pot.compute(box, t, x_dev, pe, f, w)
+        torch.cuda.synchronize()
+        pot.sync()
+        out.append((pe, f))
+        pot.close()
+    frms = float(torch.sqrt(((out[0][1] - out[1][1]) ** 2).mean()))
+    de = float((out[0][0] - out[1][0]).abs().max())
+    return frms, de
+
+
+def e2e_run(torch, pot, box, types, x_dev, steps):
+    """Host-buffer path: pinned host positions in, energies/forces out, every step."""
+    N = types.size
+    pin = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True)
+    h_pos = pin(3 * N, torch.float64)
+    h_pos.copy_(x_dev.cpu())
+    h_type = pin(N, torch.int32)
+    h_type.copy_(torch.as_tensor(types))
+    h_pe = pin(N, torch.float64)
+    h_f = pin(3 * N, torch.float64)
+    h_vt = pin(9, torch.float64)
+    for _ in range(2):
+        pot.compute_host_ptrs(box, N, h_type.data_ptr(), h_pos.data_ptr(), h_pe.data_ptr(), h_f.data_ptr(),
+                              h_vt.data_ptr())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pot.compute_host_ptrs(box, N, h_type.data_ptr(), h_pos.data_ptr(), h_pe.data_ptr(), h_f.data_ptr(),
+                              h_vt.data_ptr())
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return N * steps / dt, 28 * N, 32 * N + 72
+
+
+def cpu_baseline_sample(path, cells=20, reps=3):
+    sys.path.insert(0, ORACLE)
+    import sus2sh_oracle
+    from sus2sh import structures
+    box, types, pos = structures.fcc(cells, cells, cells, A, (0.64, 0.36), 0.0, seed=7)
+    orc = sus2sh_oracle.Oracle(path)
+    threads = os.cpu_count() or 1
+    orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": types.size * reps / dt, "unit": "atom-step/s", "cores": threads, "kind": "port",
+            "sample": f"{reps} FP64 oracle force evaluations of a {types.size}-atom {cells}^3-cell slice of "
+                      f"the same FCC Cu-Zr crystal and model (same per-atom work), OpenMP {threads} threads"}
+
+
+def reference_arm(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, ORACLE)
+    import sus2sh_oracle
+    from sus2sh import models, structures
+    with tempfile.TemporaryDirectory() as d:
+        path = models.preset_model("l3k3", d)
+        box, types, pos = structures.fcc(12, 12, 12, A, (0.64, 0.36), 0.0, seed=7)
+        orc = sus2sh_oracle.Oracle(path)
+        threads = os.cpu_count() or 1
+        for _ in range(args.warmup):
+            orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+        dt = time.perf_counter() - t0
+    value = types.size * args.steps / dt
+    sample = (f"one FP64 force evaluation per step of a {types.size}-atom 12^3-cell slice of the 1.024M-atom "
+              f"FCC Cu-Zr crystal, same l3k3 model; reference-semantics C port (the reference needs an "
+              f"upstream GPUMD tree that is not available), OpenMP {threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "atom-step/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded FCC Cu-Zr, seeded random l3k3 model)",
+            "config": {"workload": "1.024M-atom l3k3 Cu-Zr NVE (CPU arm: bounded per-step sample)",
+                       "sample_atoms": int(types.size)},
+            "cpu_baseline": {"value": value, "unit": "atom-step/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "atom-step/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    global CELLS_RUN
+    CELLS_RUN = tuple(args.cells)
+    import numpy as np
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    from sus2sh import _lib
+    lib = _lib.load()
+    with tempfile.TemporaryDirectory() as d:
+        path, box, types, pos, vel, masses = make_workload(d, rank)
+        N = types.size
+        clocks = ClockSampler(local)
+        pot, md, ms, prof, launches, clk = run_md(torch, path, box, types, pos, vel, masses, args.steps,
+                                                  args.warmup, False, world, clocks)
+        # FP64 engine on the same workload
+        pot64 = md64 = None
+        ms64 = None
+        if args.fp64_steps > 0:
+            pot64, md64, ms64, prof64, _, _ = run_md(torch, path, box, types, pos, vel, masses, args.fp64_steps,
+                                                     min(args.warmup, 3), True, world)
+        frms, de = force_error_vs_fp64(torch, path, box, types, md.pos)
+        e2e_val, h2d, d2h = e2e_run(torch, pot, box, types, md.pos, args.e2e_steps)
+        times = torch.tensor([ms, ms64 or 0.0, 1.0 / max(e2e_val, 1e-30)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+        ms_max, ms64_max, inv_e2e = times.tolist()
+        if rank == 0:
+            total_atoms = N * world
+            value = total_atoms * args.steps / (ms_max * 1e-3)
+            info = pot.info()
+            kmu = info["k_max"] * (info["l_max"] + 1)
+            C = (info["l_max"] + 1) ** 2
+            fb, ff, fp = flops_model(kmu, info["rb_size"], C, info["basics"], info["products"])
+            edges = edges_within(box, pos, pot.rc)
+            force_ms_launch = prof["force_ms"] / max(prof["calls"], 1)
+            force_flops = edges * ff
+            fp32_peak, fp64_peak = fma_peak(lib)
+            achieved = force_flops / (force_ms_launch * 1e-3) / 1e12
+            step_flops = edges * (fb + ff) + N * fp
+            line = {
+                "metric": METRIC, "value": value, "unit": "atom-step/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded 80x80x40 FCC Cu-Zr 64/36, MB velocities 200 K; seeded random l3k3 model)",
+                "config": {"workload": "1.024M-atom l3k3 Cu-Zr NVE MD, FP32 engine", "atoms_per_gpu": N,
+                           "dt_fs": DT, "skin_A": 1.0, "rebuild_every": 10, "rc_A": pot.rc,
+                           "model": "SUS2-SH L3 K3 body4 rb8 (248 moments, 806 products)",
+                           "l2": "inputs larger than L2 (positions+neighbour list+moments > 126 MB)",
+                           "parallelism": f"replicas x{world}"},
+                "fp64": {"value": N * world * args.fp64_steps / (ms64_max * 1e-3) if ms64_max else None,
+                         "ms_per_step": ms64_max / args.fp64_steps if ms64_max else None,
+                         "steps": args.fp64_steps},
+                "fp32_over_fp64": (value / (N * world * args.fp64_steps / (ms64_max * 1e-3))) if ms64_max else None,
+                "accuracy": {"force_rms_fp32_vs_fp64_eV_per_A": frms, "max_abs_dE_per_atom_eV": de},
+                "stage_ms_per_step": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"},
+                "roofline": {"kernel": "k_force (adjoint force/virial)", "bound": "fp32",
+                             "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                             "frac": achieved / fp32_peak if fp32_peak > 0 else None, "traffic": None,
+                             "peak_source": "measured FP32 FMA-chain microbenchmark on this GPU (burst)",
+                             "flops_per_edge": ff, "edges_per_launch": edges,
+                             "launch_ms": force_ms_launch,
+                             "step_tflops": step_flops * args.steps / (ms_max * 1e-3) / 1e12 / world,
+                             "fp64_peak_tflops": fp64_peak},
+                "e2e": {"value": 1.0 / inv_e2e * world, "unit": "atom-step/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h,
+                        "path": "sus2sh_compute_host: pinned host positions -> device -> energies/forces/virial "
+                                "-> pinned host, every step"},
+                "gpu_launches": launches,
+                "clocks": clk,
+            }
+            if world == 1 and not args.no_cpu_baseline:
+                line["cpu_baseline"] = cpu_baseline_sample(path)
+            print(json.dumps(line), flush=True)
+        pot.close()
+        if pot64:
+            pot64.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

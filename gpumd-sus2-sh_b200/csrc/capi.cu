@@ -296,10 +296,54 @@ struct Engine {
   DevBuf<int> io_type;
   // forward state
   int fwd_N = 0;
+  // stage profiler (CUDA events on the caller's stream; the reference's
+  // sus2_sh_profile stages neighbor/basic/product/force/accumulate,
+  // sus2_sh.cu:67-80, timed there with device syncs)
+  bool profile = false;
+  struct EvSet {
+    cudaEvent_t e[6];
+  };
+  std::vector<EvSet> ev_used, ev_free;
+  double prof_ms[5] = {0, 0, 0, 0, 0};
+  long long prof_calls = 0;
+  long long launches = 0;  // kernels launched by this handle
 
   ~Engine() {
     if (h_geom) cudaFreeHost(h_geom);
     if (h_status) cudaFreeHost(h_status);
+    for (auto& v : {&ev_used, &ev_free})
+      for (EvSet& es : *v)
+        for (cudaEvent_t e : es.e) cudaEventDestroy(e);
+  }
+
+  EvSet* ev_begin(cudaStream_t s) {
+    if (!profile) return nullptr;
+    if (ev_free.empty()) {
+      EvSet es;
+      for (cudaEvent_t& e : es.e) ck(cudaEventCreate(&e), "cudaEventCreate");
+      ev_free.push_back(es);
+    }
+    ev_used.push_back(ev_free.back());
+    ev_free.pop_back();
+    ck(cudaEventRecord(ev_used.back().e[0], s), "cudaEventRecord");
+    return &ev_used.back();
+  }
+  void mark(EvSet* ev, int k, cudaStream_t s) {
+    if (ev) ck(cudaEventRecord(ev->e[k], s), "cudaEventRecord");
+  }
+  // Waits for recorded calls and folds their stage times into prof_ms.
+  void profile_collect() {
+    for (EvSet& es : ev_used) {
+      ck(cudaEventSynchronize(es.e[5]), "cudaEventSynchronize");
+      for (int k = 0; k < 5; ++k) {
+        float ms = 0.0f;
+        ck(cudaEventElapsedTime(&ms, es.e[k], es.e[k + 1]), "cudaEventElapsedTime");
+        prof_ms[k] += ms;
+      }
+      ++prof_calls;
+      ev_free.push_back(es);
+    }
+    ev_used.clear();
   }
 
   size_t elem() const { return use_float ? sizeof(float) : sizeof(double); }
@@ -308,6 +352,7 @@ struct Engine {
     model = load_model(path);
     opt = parse_options(model, nopts, opts);
     use_float = opt.use_float;
+    profile = opt.profile;
     lay = layer_products(model);
     prog = compile_program(model, lay);
     if (!shape_supported(model.l_max, model.k_max, model.rb_size)) {
@@ -463,7 +508,8 @@ struct Engine {
     bool force = force_next;
     if (opt.rebuild_interval > 0 && calls_since_build + 1 >= opt.rebuild_interval) force = true;
     ck(cudaMemsetAsync(&d_status.p->maxdisp2_bits, 0, sizeof(unsigned int), s), "memset");
-    launch_pack(s, N, x, type, ref4.p, pos4.p, d_geom.p, have_ref ? 1 : 0, d_status.p);
+    launch_pack(s, N, x, type, ref4.p, pos4.p, d_geom.p, have_ref ? 1 : 0, model.species_count, d_status.p);
+    launches += 1;
     const float half_skin2 = static_cast<float>(0.25 * opt.skin * opt.skin);
     const double cutoff2 = cutoff * cutoff;
     if (cap == 0) {
@@ -471,6 +517,7 @@ struct Engine {
       ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
       launch_build(s, N, 1, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p, cell_start.p,
                    cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nullptr, ncount.p, 0, 1, d_status.p);
+      launches += 6;
       Status st{};
       ck(cudaMemcpyAsync(&st, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
       ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
@@ -480,6 +527,7 @@ struct Engine {
     launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
                  cell_start.p, cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
                  d_status.p);
+    launches += 6;
     ck(cudaGetLastError(), "neighbour build launch");
     have_ref = true;
     force_next = false;
@@ -495,23 +543,31 @@ struct Engine {
   }
 
   template <typename T>
-  void forward_impl(cudaStream_t s, double* pe, int pe_assign) {
+  void forward_impl(cudaStream_t s, double* pe, int pe_assign, EvSet* ev = nullptr) {
     const EdgeArgs<T> a = edge_args<T>();
+    mark(ev, 1, s);
     if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p)) != 0)
       throw InputError("SUS2_SH basic kernel shape not compiled.");
+    mark(ev, 2, s);
     launch_product<T>(s, N, program_dev(), pos4.p, reinterpret_cast<const T*>(Bbuf.p),
                       reinterpret_cast<T*>(Gbuf.p),
                       prod_global ? reinterpret_cast<T*>(scratch.p) : nullptr, prod_smem, prod_tile,
                       d_shift.p, d_species.p, pe, pe_assign);
+    launches += 2;
   }
 
   template <typename T>
-  void backward_impl(cudaStream_t s, const double* weight, double* force, double* virial, double sign) {
+  void backward_impl(cudaStream_t s, const double* weight, double* force, double* virial, double sign,
+                     EvSet* ev = nullptr) {
     const EdgeArgs<T> a = edge_args<T>();
     ck(cudaMemsetAsync(ftmp.p, 0, ftmp.n, s), "memset");
+    mark(ev, 3, s);
     if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign) != 0)
       throw InputError("SUS2_SH force kernel shape not compiled.");
+    mark(ev, 4, s);
     launch_finalize<T>(s, N, ftmp.p, force, sign);
+    mark(ev, 5, s);
+    launches += 2;
   }
 
   void finish(cudaStream_t s) {
@@ -521,13 +577,14 @@ struct Engine {
 
   void compute(cudaStream_t s, int n, const double* h, const int* pbc, const int* type, const double* x,
                double* pe, double* f, double* vir) {
+    EvSet* ev = ev_begin(s);
     prepare(s, n, h, pbc, type, x);
     if (use_float) {
-      forward_impl<float>(s, pe, 0);
-      backward_impl<float>(s, nullptr, f, vir, 1.0);
+      forward_impl<float>(s, pe, 0, ev);
+      backward_impl<float>(s, nullptr, f, vir, 1.0, ev);
     } else {
-      forward_impl<double>(s, pe, 0);
-      backward_impl<double>(s, nullptr, f, vir, 1.0);
+      forward_impl<double>(s, pe, 0, ev);
+      backward_impl<double>(s, nullptr, f, vir, 1.0, ev);
     }
     finish(s);
   }
@@ -544,7 +601,17 @@ struct Engine {
       h_status->overflow = 0;
       force_next = true;
     }
+    if (h_status->bad_type) {
+      f |= SUS2SH_STATUS_BAD_TYPE;
+      const int zero = 0;
+      ck(cudaMemcpy(&d_status.p->bad_type, &zero, sizeof(int), cudaMemcpyHostToDevice), "status reset");
+      h_status->bad_type = 0;
+    }
     if (flags) *flags = f;
+    if (f & SUS2SH_STATUS_BAD_TYPE) {
+      g_last_error = "species index outside [0, species_count) (treated as species 0)";
+      return SUS2SH_E_ARG;
+    }
     return (f & SUS2SH_STATUS_OVERFLOW) ? SUS2SH_E_NEIGHBOR : SUS2SH_OK;
   }
 };
@@ -674,6 +741,7 @@ int sus2sh_compute_host(sus2sh_handle* h, int N, const double box_h[9], const in
     ck(cudaMemsetAsync(e.io_vir.p, 0, sizeof(double) * 9 * N, s), "memset");
     e.compute(s, N, box_h, pbc, e.io_type.p, e.io_pos.p, e.io_pe.p, e.io_f.p, e.io_vir.p);
     sus2sh::launch_reduce(s, N, e.io_pe.p, e.io_vir.p, e.io_red.p);
+    e.launches += 1;
     ck(cudaMemcpyAsync(potential, e.io_pe.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s), "D2H");
     ck(cudaMemcpyAsync(force, e.io_f.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s), "D2H");
     if (virial_total) {
@@ -707,15 +775,36 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[18] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[21] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
                      e.prog.nvalue, e.prog.nrows, e.model.standard_graph_matched ? 1 : 0,
-                     e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0};
-  const int k = std::min(n, 18);
+                     e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0,
+                     static_cast<int>(e.launches & 0x7fffffff), e.rs.shared_xi, e.prod_global ? 1 : 0};
+  const int k = std::min(n, 21);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
+}
+
+int sus2sh_profile(sus2sh_handle* h, int enable) {
+  if (!h) return SUS2SH_E_ARG;
+  return guarded([&] {
+    h->e.profile_collect();
+    h->e.profile = enable != 0;
+    for (double& v : h->e.prof_ms) v = 0.0;
+    h->e.prof_calls = 0;
+  });
+}
+
+int sus2sh_profile_read(sus2sh_handle* h, double* out, int n) {
+  if (!h || !out) return SUS2SH_E_ARG;
+  int rc = guarded([&] { h->e.profile_collect(); });
+  if (rc != SUS2SH_OK) return rc;
+  const double v[6] = {h->e.prof_ms[0], h->e.prof_ms[1], h->e.prof_ms[2], h->e.prof_ms[3], h->e.prof_ms[4],
+                       static_cast<double>(h->e.prof_calls)};
+  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+  return SUS2SH_OK;
 }
 
 // ---- tools -----------------------------------------------------------------
@@ -781,6 +870,12 @@ int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* typ
 int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream) {
   sus2sh::launch_reduce(static_cast<cudaStream_t>(stream), N, potential, virial, out);
   return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
+}
+
+int sus2sh_measure_fma_peak(int fp64, double* tflops) {
+  if (!tflops) return SUS2SH_E_ARG;
+  *tflops = sus2sh::measure_fma_tflops(fp64 != 0);
+  return *tflops > 0 ? SUS2SH_OK : SUS2SH_E_CUDA;
 }
 
 int sus2sh_random_insertion(int N, double lx, double ly, double lz, double dmin, unsigned long long seed,

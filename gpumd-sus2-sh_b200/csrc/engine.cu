@@ -35,7 +35,7 @@ __device__ __forceinline__ int type_of(const double4& p) {
 // ---------------------------------------------------------------------------
 __global__ void k_pack(int N, const double* __restrict__ x, const int* __restrict__ type,
                        const double4* __restrict__ ref4, double4* __restrict__ pos4,
-                       const BoxGeom* __restrict__ g, int have_ref, Status* st) {
+                       const BoxGeom* __restrict__ g, int have_ref, int species, Status* st) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.0f;
   if (i < N) {
@@ -55,7 +55,12 @@ __global__ void k_pack(int N, const double* __restrict__ x, const int* __restric
       const double ex = px - r.x, ey = py - r.y, ez = pz - r.z;
       d2 = static_cast<float>(ex * ex + ey * ey + ez * ez);
     }
-    pos4[i] = make_double4(px, py, pz, __longlong_as_double(static_cast<long long>(type[i])));
+    int t = type[i];
+    if (t < 0 || t >= species) {  // keep every table lookup in bounds
+      st->bad_type = 1;
+      t = 0;
+    }
+    pos4[i] = make_double4(px, py, pz, __longlong_as_double(static_cast<long long>(t)));
   }
   // block max of the displacement, one atomic per block
   __shared__ float red[32];
@@ -682,9 +687,55 @@ __global__ void k_reduce(int N, const double* __restrict__ pe, const double* __r
   }
 }
 
+// FMA throughput probe: 8 independent dependency chains per thread, each
+// thread writes only its own output slot.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_peak(int iters, T seed, T* __restrict__ out) {
+  T a0 = seed + threadIdx.x, a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3);
+  T a4 = a0 + T(4), a5 = a0 + T(5), a6 = a0 + T(6), a7 = a0 + T(7);
+  const T m = T(0.9999), c = T(1e-4);
+  for (int k = 0; k < iters; ++k) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+}
+
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
+
+double measure_fma_tflops(bool fp64) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = sms * 8, threads = 256, iters = fp64 ? 512 : 2048;
+  void* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double) * blocks * threads) != cudaSuccess) return -1.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 6; ++rep) {
+    cudaEventRecord(e0);
+    if (fp64) k_fma_peak<double><<<blocks, threads>>>(iters, 1.0, static_cast<double*>(out));
+    else k_fma_peak<float><<<blocks, threads>>>(iters, 1.0f, static_cast<float*>(out));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  const double flops = 2.0 * 8.0 * 16.0 * iters * static_cast<double>(blocks) * threads;
+  return flops / (best * 1e-3) / 1e12;
+}
 
 void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial, double* out) {
   cudaMemsetAsync(out, 0, 10 * sizeof(double), s);
@@ -698,8 +749,8 @@ void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial
 // launchers
 // ---------------------------------------------------------------------------
 void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const double4* ref4,
-                 double4* pos4, const BoxGeom* geom_dev, int have_ref, Status* st) {
-  k_pack<<<blocks_for(N, 256), 256, 0, s>>>(N, x, type, ref4, pos4, geom_dev, have_ref, st);
+                 double4* pos4, const BoxGeom* geom_dev, int have_ref, int species, Status* st) {
+  k_pack<<<blocks_for(N, 256), 256, 0, s>>>(N, x, type, ref4, pos4, geom_dev, have_ref, species, st);
 }
 
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,

@@ -36,7 +36,8 @@ struct Status {
   int overflow;                // neighbour capacity exceeded (sticky)
   int max_count;               // largest neighbour count seen at a build
   int builds;                  // number of builds
-  int pad[3];
+  int bad_type;                // a species index outside [0, species_count) was seen (sticky)
+  int pad[2];
 };
 
 // Radial table: per pair p = t_i*S + t_j: [KMU] (scal, shift) pairs then the
@@ -78,7 +79,7 @@ struct ProgramDev {
 
 // ---- launchers (engine.cu) ----------------------------------------------
 void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const double4* ref4,
-                 double4* pos4, const BoxGeom* geom_dev, int have_ref, Status* st);
+                 double4* pos4, const BoxGeom* geom_dev, int have_ref, int species, Status* st);
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
                   const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
                   int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
@@ -106,5 +107,9 @@ void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_ty
                      const int* type, const double* force, double* vel);
 
 bool shape_supported(int l_max, int k_max, int rb);
+
+// Measured FMA throughput of the current device (TFLOP/s, 2 flops per FMA),
+// best of five launches; -1 on error.
+double measure_fma_tflops(bool fp64);
 
 }  // namespace sus2sh

@@ -134,10 +134,6 @@ std::vector<T> numbers(const std::string& text) {
   return v;
 }
 
-bool starts_with(const std::string& s, const std::string& p) {
-  return s.size() >= p.size() && s.compare(0, p.size(), p) == 0;
-}
-
 bool parse_bool(const std::string& v, const std::string& name) {
   if (v == "1" || v == "true" || v == "TRUE" || v == "yes" || v == "on") return true;
   if (v == "0" || v == "false" || v == "FALSE" || v == "no" || v == "off") return false;
@@ -739,6 +735,11 @@ Layered layer_products(const HostModel& m) {
 Options parse_options(const HostModel& m, int nopts, const char** opts) {
   Options o;
   if (const char* env = std::getenv("SUS2_GPUMD_FLOAT")) o.use_float = parse_bool(env, "SUS2_GPUMD_FLOAT");
+  {
+    const char* env = std::getenv("SUS2_SH_GPUMD_PROFILE");
+    if (!env) env = std::getenv("SUS2_GPUMD_PROFILE");
+    if (env) o.profile = parse_bool(env, "SUS2_SH_GPUMD_PROFILE");
+  }
   const int begin = std::min(nopts, m.species_count);
   for (int i = begin; i < nopts; ++i) {
     const std::string s = opts[i] ? opts[i] : "";
@@ -752,6 +753,8 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       if (!(o.skin >= 0.0)) throw InputError("sus2_sh_skin must be >= 0.");
     } else if (key == "sus2_sh_rebuild_interval") {
       o.rebuild_interval = std::atoi(val.c_str());
+    } else if (key == "sus2_sh_profile" || key == "sus2_profile") {
+      o.profile = parse_bool(val, key);
     } else if (key == "sus2_sh_reference_rounding") {
       o.reference_rounding = parse_bool(val, key);
     } else if (key == "sus2_radial_direct" || key == "sus2_sh_radial_direct" || key == "radial_direct") {

@@ -100,6 +100,7 @@ struct Options {
   double skin = 1.0;            // sus2_sh_skin= (Angstrom)
   int rebuild_interval = 0;     // sus2_sh_rebuild_interval= (0: displacement only)
   bool reference_rounding = false;  // sus2_sh_reference_rounding=
+  bool profile = false;             // sus2_sh_profile / sus2_profile / SUS2_SH_GPUMD_PROFILE
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

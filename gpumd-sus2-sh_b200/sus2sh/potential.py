@@ -20,7 +20,8 @@ from . import _lib
 MODEL_INFO_FIELDS = (
     "species", "l_max", "k_max", "body_order", "rb_size", "basics", "moments", "products",
     "scalars", "rows", "layers", "terminal_rows", "value_slots", "program_rows",
-    "standard_graph_matched", "use_float", "neighbor_capacity", "neighbor_builds",
+    "standard_graph_matched", "use_float", "neighbor_capacity", "neighbor_builds", "launches",
+    "shared_xi", "product_slots_in_hbm",
 )
 
 
@@ -131,6 +132,15 @@ class SUS2_SH:
             self._h, N, box.cpu_h.ctypes.data_as(ctypes.c_void_p), box.pbc.ctypes.data_as(ctypes.c_void_p),
             ctypes.c_void_p(type_ptr), ctypes.c_void_p(pos_ptr), ctypes.c_void_p(pe_ptr),
             ctypes.c_void_p(f_ptr), ctypes.c_void_p(vt_ptr), _stream_ptr(stream)), "sus2sh_compute_host")
+
+    def profile(self, enable: bool = True):
+        _lib.check(self._lib.sus2sh_profile(self._h, 1 if enable else 0), "sus2sh_profile")
+
+    def profile_read(self) -> dict:
+        out = (ctypes.c_double * 6)()
+        _lib.check(self._lib.sus2sh_profile_read(self._h, out, 6), "sus2sh_profile_read")
+        keys = ("neighbor_ms", "basic_ms", "product_ms", "force_ms", "accumulate_ms", "calls")
+        return {k: out[i] for i, k in enumerate(keys)}
 
     def sync(self) -> int:
         flags = ctypes.c_int(0)

@@ -36,6 +36,7 @@ typedef struct sus2sh_handle sus2sh_handle;
 
 /* status flags returned by sus2sh_sync */
 #define SUS2SH_STATUS_OVERFLOW 1
+#define SUS2SH_STATUS_BAD_TYPE 2  /* a type was outside [0, species_count) */
 
 /* Replaces is_sus2_sh_potential_file (src/force/sus2_sh.cu:7771-7780,
  * declared src/force/sus2_sh.cuh:205): 1 if the file contains
@@ -97,13 +98,26 @@ int sus2sh_compute_host(sus2sh_handle* h, int N, const double box_h[9], const in
                         const int* type, const double* position, double* potential,
                         double* force, double* virial_total, void* stream);
 
+/* Stage profiler (the reference's sus2_sh_profile=1 stage times,
+ * src/force/sus2_sh.cu:9631-9645,10638-10674, measured here with CUDA events
+ * on the caller's stream instead of device-wide syncs).  sus2sh_profile turns
+ * it on/off and clears it; sus2sh_profile_read waits for the recorded calls
+ * and returns up to n values: total ms of [0] neighbour (pack + conditional
+ * build) [1] basic [2] product [3] force [4] accumulate, and [5] the number
+ * of profiled calls.  The option token sus2_sh_profile=1 enables it at
+ * creation. */
+int sus2sh_profile(sus2sh_handle* h, int enable);
+int sus2sh_profile_read(sus2sh_handle* h, double* out, int n);
+
 /* Model/graph statistics for logging (the reference prints them at
  * construction, src/force/sus2_sh.cu:9339-9466).  Fills up to n ints:
  * [0] species [1] l_max [2] k_max [3] body_order [4] rb_size [5] basics
  * [6] moments [7] products [8] scalars [9] rows [10] layers
  * [11] terminal scalar rows [12] program value slots [13] program rows
  * [14] standard graph matched [15] use_float [16] neighbour capacity
- * [17] neighbour builds so far.  Returns the number written. */
+ * [17] neighbour builds so far (valid after sus2sh_sync) [18] kernels
+ * launched by this handle [19] shared radial argument [20] product slots in
+ * HBM.  Returns the number written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

@@ -44,6 +44,11 @@ int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* typ
  * out is a device array of 10 doubles; virial may be NULL. */
 int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream);
 
+/* FMA-chain microbenchmark of the current device: measured FP32 (fp64 = 0)
+ * or FP64 (fp64 = 1) CUDA-core throughput in TFLOP/s (2 flops per FMA).  It is
+ * the roofline denominator of the SIMT kernels. */
+int sus2sh_measure_fma_peak(int fp64, double* tflops);
+
 /* Random sequential insertion of N points with minimum distance dmin in the
  * orthorhombic box lx*ly*lz (periodic), seeded; writes SoA positions (3N).
  * Returns 0, or a negative value when the insertion budget runs out. */
