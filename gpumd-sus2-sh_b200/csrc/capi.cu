@@ -622,6 +622,19 @@ struct sus2sh_handle {
   sus2sh::Engine e;
 };
 
+namespace sus2sh {
+bool cg_view(const sus2sh_handle* h, CgView* out) {
+  if (!h || !out) return false;
+  out->prog = h->e.program_dev();
+  out->shift = h->e.d_shift.p;
+  out->species = h->e.d_species.p;
+  out->species_count = h->e.model.species_count;
+  out->use_float = h->e.use_float ? 1 : 0;
+  return true;
+}
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace sus2sh
+
 using sus2sh::CudaError;
 using sus2sh::InputError;
 

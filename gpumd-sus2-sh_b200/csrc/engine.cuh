@@ -77,6 +77,15 @@ struct ProgramDev {
   const int* canon_basic;  // [ncanon] model basic or -1
 };
 
+// Program tables of a handle, for kernels outside the handle's own path.
+struct CgView {
+  ProgramDev prog;
+  const double* shift;
+  const double* species;
+  int species_count;
+  int use_float;
+};
+
 // ---- launchers (engine.cu) ----------------------------------------------
 void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const double4* ref4,
                  double4* pos4, const BoxGeom* geom_dev, int have_ref, int species, Status* st);

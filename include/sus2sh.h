@@ -109,6 +109,27 @@ int sus2sh_compute_host(sus2sh_handle* h, int N, const double box_h[9], const in
 int sus2sh_profile(sus2sh_handle* h, int enable);
 int sus2sh_profile_read(sus2sh_handle* h, double* out, int n);
 
+/* No counterpart in the reference.  The CG product stage alone (forward
+ * contraction, site energy E_i and adjoints dE_i/dB_b(i)) on basic moments the
+ * caller provides, for callers that cannot allocate device memory at call
+ * time: code inside a CUDA stream capture, MD codes that reserve all device
+ * memory up front and forbid allocations during a run, and real-time loops
+ * that cannot take an allocation's implicit synchronisation.  It calls no
+ * cudaMalloc, cudaFree or allocating library routine.
+ *   basics        [alpha_index_basic_count][N], the model's basic order,
+ *                 float for an FP32 handle (sus2_float=1), double otherwise
+ *   potential     [N] double, assigned
+ *   basic_adjoint [alpha_index_basic_count][N], same type as basics, assigned
+ * Its work area is one fixed 16 MiB device array inside the library (held by
+ * every GPU that loads the library until the process exits), so
+ * N * 2 * (program value slots) * sizeof(element) must be at most 16 MiB;
+ * larger N is rejected with SUS2SH_E_ARG and a message giving the limit.  The
+ * first call on each device resolves that array's device address with the
+ * device current; make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race, so serialise them. */
+int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, const void* basics,
+                             double* potential, void* basic_adjoint, void* stream);
+
 /* Model/graph statistics for logging (the reference prints them at
  * construction, src/force/sus2_sh.cu:9339-9466).  Fills up to n ints:
  * [0] species [1] l_max [2] k_max [3] body_order [4] rb_size [5] basics

@@ -511,3 +511,40 @@ int oracle_neighbor_counts(int N, const double* h, const int* pbc, const double*
   free(nl.e);
   return 0;
 }
+
+/* Site energies and basic-moment adjoints dE_i/dB_b(i) from given basics
+ * B[b*N+i] (flat products, sus2_sh.cu:4813-4845); G[b*N+i] assigned. */
+int oracle_cg_energy(const OracleModel* m, int N, const int* type, const double* B, double* pe, double* G) {
+  int fail = 0;
+#pragma omp parallel
+  {
+    double* Mv = (double*)malloc(sizeof(double) * m->M);
+    double* gv = (double*)malloc(sizeof(double) * m->M);
+    if (!Mv || !gv) fail = 1;
+#pragma omp for schedule(static)
+    for (int i = 0; i < N; ++i) {
+      if (!Mv || !gv) continue;
+      memset(Mv, 0, sizeof(double) * m->M);
+      memset(gv, 0, sizeof(double) * m->M);
+      for (int b = 0; b < m->nbasic; ++b) Mv[b] = B[(size_t)b * N + i];
+      for (int p = 0; p < m->nprod; ++p) Mv[m->prod_t[p]] += m->prod_c[p] * Mv[m->prod_l[p]] * Mv[m->prod_r[p]];
+      const int ti = type[i];
+      const double ct = m->species[ti];
+      double E = m->shift_e[ti] + ct;
+      for (int s = 0; s < m->nscalar; ++s) {
+        E += ct * m->w[s] * Mv[m->map[s]];
+        gv[m->map[s]] += ct * m->w[s];
+      }
+      for (int p = m->nprod - 1; p >= 0; --p) {
+        const double gt = gv[m->prod_t[p]] * m->prod_c[p];
+        gv[m->prod_l[p]] += gt * Mv[m->prod_r[p]];
+        gv[m->prod_r[p]] += gt * Mv[m->prod_l[p]];
+      }
+      pe[i] = E;
+      for (int b = 0; b < m->nbasic; ++b) G[(size_t)b * N + i] = gv[b];
+    }
+    free(Mv);
+    free(gv);
+  }
+  return fail ? -1 : 0;
+}

@@ -148,6 +148,19 @@ class Oracle:
         return B
 
 
+    def cg_energy(self, types, B):
+        """Site energies and dE_i/dB_b(i) from basic moments B (model order, (Bb, N))."""
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        N = B.shape[1]
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        pe = np.zeros(N)
+        G = np.zeros_like(B)
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        if self.lib.oracle_cg_energy(ctypes.byref(self._c), N, ptr(types), ptr(B), ptr(pe), ptr(G)) != 0:
+            raise RuntimeError("oracle_cg_energy failed")
+        return pe, G
+
+
 def neighbor_counts(h, pbc, pos, rc):
     lib = ctypes.CDLL(build_oracle())
     pos = np.ascontiguousarray(pos, dtype=np.float64)
