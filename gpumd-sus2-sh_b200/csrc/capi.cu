@@ -2,10 +2,12 @@
 // sus2sh_tools.h.
 #include "../../include/sus2sh.h"
 #include "../../include/sus2sh_tools.h"
+#include "cg_codegen.h"
 #include "engine.cuh"
 #include "mtp_model.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +21,10 @@ namespace sus2sh {
 namespace {
 
 thread_local std::string g_last_error;
+
+// Graphs up to this many saved products get a straight-line CG kernel; larger
+// ones (body-5 L=4 graphs have ~3e4) run the row interpreter.
+constexpr long long kCgJitMaxProducts = 12000;
 
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& m) : std::runtime_error(m) {}
@@ -307,6 +313,11 @@ struct Engine {
   double prof_ms[5] = {0, 0, 0, 0, 0};
   long long prof_calls = 0;
   long long launches = 0;  // kernels launched by this handle
+  // model-specialised CG kernel (NVRTC); empty cubin -> interpreter
+  CgSource cg_src;
+  CgBinary cg_bin;
+  CgModule cg_mod;
+  double cg_compile_ms = 0.0;
 
   ~Engine() {
     if (h_geom) cudaFreeHost(h_geom);
@@ -427,6 +438,18 @@ struct Engine {
     prod_global = best_tile == 0;
     prod_tile = best_tile ? best_tile : 128;
     prod_smem = per_atom * prod_tile;
+    // straight-line CG kernel for graphs of moderate size
+    if (opt.cg_jit) {
+      long long terms = 0;
+      for (const Row& r : lay.rows) terms += static_cast<long long>(r.left.size());
+      if (terms <= kCgJitMaxProducts) {
+        const auto t0 = std::chrono::steady_clock::now();
+        cg_src = generate_cg_source(model, lay, use_float, prog.basic_canon, prog.ncanon);
+        cg_bin = compile_cg_source(cg_src);
+        cg_compile_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      }
+    }
     if (num_atoms > 0) ensure_size(num_atoms);
   }
 
@@ -549,10 +572,17 @@ struct Engine {
     if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p)) != 0)
       throw InputError("SUS2_SH basic kernel shape not compiled.");
     mark(ev, 2, s);
-    launch_product<T>(s, N, program_dev(), pos4.p, reinterpret_cast<const T*>(Bbuf.p),
-                      reinterpret_cast<T*>(Gbuf.p),
-                      prod_global ? reinterpret_cast<T*>(scratch.p) : nullptr, prod_smem, prod_tile,
-                      d_shift.p, d_species.p, pe, pe_assign);
+    if (!cg_bin.cubin.empty()) {
+      std::string err;
+      if (!cg_mod.load(cg_bin, cg_src.kernel_name, &err) ||
+          !cg_mod.launch(s, N, pos4.p, Bbuf.p, Gbuf.p, d_shift.p, d_species.p, pe, pe_assign, &err))
+        throw CudaError(err);
+    } else {
+      launch_product<T>(s, N, program_dev(), pos4.p, reinterpret_cast<const T*>(Bbuf.p),
+                        reinterpret_cast<T*>(Gbuf.p),
+                        prod_global ? reinterpret_cast<T*>(scratch.p) : nullptr, prod_smem, prod_tile,
+                        d_shift.p, d_species.p, pe, pe_assign);
+    }
     launches += 2;
   }
 
@@ -788,14 +818,15 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[21] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[24] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
                      e.prog.nvalue, e.prog.nrows, e.model.standard_graph_matched ? 1 : 0,
                      e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0,
-                     static_cast<int>(e.launches & 0x7fffffff), e.rs.shared_xi, e.prod_global ? 1 : 0};
-  const int k = std::min(n, 21);
+                     static_cast<int>(e.launches & 0x7fffffff), e.rs.shared_xi, e.prod_global ? 1 : 0,
+                     e.cg_bin.cubin.empty() ? 0 : 1, e.cg_bin.registers, static_cast<int>(e.cg_compile_ms)};
+  const int k = std::min(n, 24);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -883,6 +914,41 @@ int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* typ
 int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream) {
   sus2sh::launch_reduce(static_cast<cudaStream_t>(stream), N, potential, virial, out);
   return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
+}
+
+int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text, size_t text_size) {
+  if (!path || !info) return SUS2SH_E_ARG;
+  return guarded([&] {
+    const sus2sh::HostModel m = sus2sh::load_model(path);
+    const sus2sh::Layered lay = sus2sh::layer_products(m);
+    const sus2sh::ProgramHost prog = sus2sh::compile_program(m, lay);
+    if (static_cast<long long>(m.products.size()) > sus2sh::kCgJitMaxProducts)
+      throw InputError("graph has more products than the straight-line CG kernel limit (" +
+                       std::to_string(sus2sh::kCgJitMaxProducts) + "); the row interpreter runs it");
+    const auto t0 = std::chrono::steady_clock::now();
+    const sus2sh::CgSource src = sus2sh::generate_cg_source(m, lay, use_float != 0, prog.basic_canon, prog.ncanon);
+    const sus2sh::CgBinary bin = sus2sh::compile_cg_source(src);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    int spill = 0;
+    const size_t p = bin.log.find("bytes spill stores");
+    if (p != std::string::npos) {
+      size_t q = p;
+      while (q > 0 && bin.log[q - 1] == ' ') --q;
+      while (q > 0 && std::isdigit(static_cast<unsigned char>(bin.log[q - 1]))) --q;
+      spill = std::atoi(bin.log.c_str() + q);
+    }
+    info[0] = bin.registers;
+    info[1] = spill;
+    info[2] = static_cast<int>(src.fp_terms);
+    info[3] = static_cast<int>(ms);
+    info[4] = static_cast<int>(bin.cubin.size());
+    if (text && text_size) {
+      const std::string& t = use_float < 0 ? src.code : bin.log;
+      const size_t k = std::min(text_size - 1, t.size());
+      std::memcpy(text, t.data(), k);
+      text[k] = 0;
+    }
+  });
 }
 
 int sus2sh_measure_fma_peak(int fp64, double* tflops) {

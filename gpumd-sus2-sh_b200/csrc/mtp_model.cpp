@@ -755,6 +755,8 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       o.rebuild_interval = std::atoi(val.c_str());
     } else if (key == "sus2_sh_profile" || key == "sus2_profile") {
       o.profile = parse_bool(val, key);
+    } else if (key == "sus2_sh_cg_jit") {
+      o.cg_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_reference_rounding") {
       o.reference_rounding = parse_bool(val, key);
     } else if (key == "sus2_radial_direct" || key == "sus2_sh_radial_direct" || key == "radial_direct") {

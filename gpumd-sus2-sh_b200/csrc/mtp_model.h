@@ -101,6 +101,7 @@ struct Options {
   int rebuild_interval = 0;     // sus2_sh_rebuild_interval= (0: displacement only)
   bool reference_rounding = false;  // sus2_sh_reference_rounding=
   bool profile = false;             // sus2_sh_profile / sus2_profile / SUS2_SH_GPUMD_PROFILE
+  bool cg_jit = true;               // sus2_sh_cg_jit=0 runs the CG row interpreter instead
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

@@ -17,6 +17,7 @@ EXPORTS = (
     "sus2sh_cg_energy_noalloc",
     "sus2sh_write_synthetic_model", "sus2sh_standard_graph_counts", "sus2sh_md_kick_drift",
     "sus2sh_md_kick", "sus2sh_reduce", "sus2sh_random_insertion", "sus2sh_measure_fma_peak",
+    "sus2sh_cg_kernel_info",
 )
 
 _lib = None
@@ -51,6 +52,7 @@ def load() -> ctypes.CDLL:
         "sus2sh_cg_energy_noalloc": (I, [P, I, P, P, P, P, P]),
         "sus2sh_profile_read": (I, [P, P, I]),
         "sus2sh_measure_fma_peak": (I, [I, P]),
+        "sus2sh_cg_kernel_info": (I, [S, I, P, P, ctypes.c_size_t]),
         "sus2sh_write_synthetic_model": (I, [S, I, I, I, I, P, I, I, D, D, I, P, D, D, D, D,
                                              ctypes.c_ulonglong]),
         "sus2sh_standard_graph_counts": (I, [I, I, I, P, I, P]),

@@ -21,7 +21,7 @@ MODEL_INFO_FIELDS = (
     "species", "l_max", "k_max", "body_order", "rb_size", "basics", "moments", "products",
     "scalars", "rows", "layers", "terminal_rows", "value_slots", "program_rows",
     "standard_graph_matched", "use_float", "neighbor_capacity", "neighbor_builds", "launches",
-    "shared_xi", "product_slots_in_hbm",
+    "shared_xi", "product_slots_in_hbm", "cg_jit", "cg_jit_registers", "cg_jit_compile_ms",
 )
 
 

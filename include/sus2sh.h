@@ -138,7 +138,8 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * [14] standard graph matched [15] use_float [16] neighbour capacity
  * [17] neighbour builds so far (valid after sus2sh_sync) [18] kernels
  * launched by this handle [19] shared radial argument [20] product slots in
- * HBM.  Returns the number written. */
+ * HBM [21] model-specialised CG kernel in use [22] its registers per thread
+ * [23] its NVRTC compile time (ms).  Returns the number written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

@@ -44,6 +44,13 @@ int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* typ
  * out is a device array of 10 doubles; virial may be NULL. */
 int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream);
 
+/* Generates and NVRTC-compiles (sm_100a, no GPU needed) the model-specialised
+ * CG product kernel of a model file: info[0] registers per thread, [1] spill
+ * store bytes, [2] emitted multiply-add terms, [3] generate+compile ms,
+ * [4] cubin bytes.  text (if not NULL) receives the ptxas report.  Graphs
+ * above the straight-line limit (12000 products) return SUS2SH_E_INPUT. */
+int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text, size_t text_size);
+
 /* FMA-chain microbenchmark of the current device: measured FP32 (fp64 = 0)
  * or FP64 (fp64 = 1) CUDA-core throughput in TFLOP/s (2 flops per FMA).  It is
  * the roofline denominator of the SIMT kernels. */

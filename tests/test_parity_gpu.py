@@ -68,6 +68,13 @@ def test_config0_fcc_2048(l3k3_path, fp64):
 
 
 @pytest.mark.parametrize("fp64", [False, True])
+def test_config0_row_interpreter(l3k3_path, fp64):
+    # the generic CG row interpreter (used for large graphs) on the same case
+    box, types, pos = structures.fcc(8, 8, 8, 3.8, (0.5, 0.5), 0.05, seed=1)
+    compare(l3k3_path, box, types, pos, opts=("sus2_sh_cg_jit=0",), fp64=fp64)
+
+
+@pytest.mark.parametrize("fp64", [False, True])
 def test_small_periodic_cell_images(l3k3_path, fp64):
     # 3x3x3 FCC (11.4 A < 2 (rc + skin)): every neighbour image is explicit
     box, types, pos = structures.fcc(3, 3, 3, 3.8, (0.5, 0.5), 0.1, seed=2)
