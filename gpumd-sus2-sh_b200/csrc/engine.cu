@@ -24,6 +24,16 @@ namespace sus2sh {
 namespace {
 
 constexpr int kEdgeBlock = 128;
+// Minimum resident CTAs per SM of the FP32 edge kernels (register caps).
+// Measured on the 1.024M-atom l3k3 workload: k_force at 4 CTAs (128 registers,
+// 8 B spill) runs 1.55 ms vs 1.87 ms at its natural 167 registers; capping
+// k_basic below its natural 126 registers (5 CTAs) spills and loses.
+#ifndef SUS2_BASIC_MIN_BLOCKS
+#define SUS2_BASIC_MIN_BLOCKS 1
+#endif
+#ifndef SUS2_FORCE_MIN_BLOCKS
+#define SUS2_FORCE_MIN_BLOCKS 4
+#endif
 constexpr int kCenterCode = 62;  // image (0,0,0) in base-5 codes
 
 __device__ __forceinline__ int type_of(const double4& p) {
@@ -366,11 +376,50 @@ __device__ __forceinline__ void load_pair_table(const EdgeArgs<T>& a, T* s_tab) 
   __syncthreads();
 }
 
+// Software-pipelined neighbour stream of one centre atom: the neighbour word
+// is fetched two edges ahead and the neighbour's position one edge ahead, so
+// the dependent gathers overlap the previous edge's arithmetic.
+struct NeighborStream {
+  const int* __restrict__ nbr;
+  const double4* __restrict__ pos4;
+  size_t stride;
+  int cnt;
+  int w_next, w_next2;
+  double4 p_next;
+
+  __device__ __forceinline__ NeighborStream(const int* nb, const double4* p4, int N, int i, int count)
+      : nbr(nb + i), pos4(p4), stride(static_cast<size_t>(N)), cnt(count) {
+    w_next = cnt > 0 ? __ldg(nbr) : 0;
+    w_next2 = cnt > 1 ? __ldg(nbr + stride) : 0;
+    p_next = cnt > 0 ? pos4[w_next & 0xFFFFFF] : make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  // Returns edge n's word and position and issues the loads for n+1 / n+2.
+  __device__ __forceinline__ void next(int n, int& w, double4& pj) {
+    w = w_next;
+    pj = p_next;
+    w_next = w_next2;
+    if (n + 1 < cnt) p_next = pos4[w_next & 0xFFFFFF];
+    if (n + 2 < cnt) w_next2 = __ldg(nbr + static_cast<size_t>(n + 2) * stride);
+  }
+};
+
+// Image shift of a neighbour word (zero for the home image, which is most).
+__device__ __forceinline__ void image_shift(const double (*shift)[3], int code, double& sx, double& sy,
+                                            double& sz) {
+  if (code == kCenterCode) {
+    sx = sy = sz = 0.0;
+  } else {
+    sx = shift[code][0];
+    sy = shift[code][1];
+    sz = shift[code][2];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // basic moments
 // ---------------------------------------------------------------------------
 template <typename T, int L, int K, int RB>
-__global__ void __launch_bounds__(kEdgeBlock) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
+__global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_BASIC_MIN_BLOCKS : 1) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_tab = reinterpret_cast<T*>(smem_raw);
   load_pair_table(a, s_tab);
@@ -385,14 +434,16 @@ __global__ void __launch_bounds__(kEdgeBlock) k_basic(const EdgeArgs<T> a, T* __
   const int row_i = type_of(pi) * S;
   const int cnt = min(a.ncount[i], a.cap);
   const double rc = a.rs.rc, rc2 = rc * rc;
+  NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
   for (int n = 0; n < cnt; ++n) {
-    const int w = __ldg(a.nbr + static_cast<size_t>(n) * a.N + i);
-    const int j = w & 0xFFFFFF;
-    const int code = static_cast<unsigned>(w) >> 24;
-    const double4 pj = a.pos4[j];
-    const double dx = pj.x - pi.x + a.shift[code][0];
-    const double dy = pj.y - pi.y + a.shift[code][1];
-    const double dz = pj.z - pi.z + a.shift[code][2];
+    int w;
+    double4 pj;
+    ns.next(n, w, pj);
+    double sx, sy, sz;
+    image_shift(a.shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
+    const double dx = pj.x - pi.x + sx;
+    const double dy = pj.y - pi.y + sy;
+    const double dz = pj.z - pi.z + sz;
     const double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 >= rc2) continue;
     const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
@@ -435,7 +486,7 @@ struct Scatter<double> {
 };
 
 template <typename T, int L, int K, int RB>
-__global__ void __launch_bounds__(kEdgeBlock)
+__global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_FORCE_MIN_BLOCKS : 1)
     k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
             void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
             double sign) {
@@ -458,14 +509,17 @@ __global__ void __launch_bounds__(kEdgeBlock)
   const int row_i = type_of(pi) * S;
   const int cnt = min(a.ncount[i], a.cap);
   const double rc = a.rs.rc, rc2 = rc * rc;
+  NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
   for (int n = 0; n < cnt; ++n) {
-    const int wd = __ldg(a.nbr + static_cast<size_t>(n) * a.N + i);
+    int wd;
+    double4 pj;
+    ns.next(n, wd, pj);
     const int j = wd & 0xFFFFFF;
-    const int code = static_cast<unsigned>(wd) >> 24;
-    const double4 pj = a.pos4[j];
-    const double dx = pj.x - pi.x + a.shift[code][0];
-    const double dy = pj.y - pi.y + a.shift[code][1];
-    const double dz = pj.z - pi.z + a.shift[code][2];
+    double sx, sy, sz;
+    image_shift(a.shift, static_cast<unsigned>(wd) >> 24, sx, sy, sz);
+    const double dx = pj.x - pi.x + sx;
+    const double dy = pj.y - pi.y + sy;
+    const double dz = pj.z - pi.z + sz;
     const double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 >= rc2) continue;
     const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
