@@ -208,7 +208,8 @@ def force_error_vs_fp64(torch, path, box, types, x_dev):
         pot.close()
     frms = float(torch.sqrt(((out[0][1] - out[1][1]) ** 2).mean()))
     de = float((out[0][0] - out[1][0]).abs().max())
-    return frms, de
+    de_total = float((out[0][0].sum() - out[1][0].sum()).abs()) / N
+    return frms, de, de_total
 
 
 def e2e_run(torch, pot, box, types, x_dev, steps):
@@ -315,7 +316,7 @@ def main():
         if args.fp64_steps > 0:
             pot64, md64, ms64, prof64, _, _ = run_md(torch, path, box, types, pos, vel, masses, args.fp64_steps,
                                                      min(args.warmup, 3), True, world)
-        frms, de = force_error_vs_fp64(torch, path, box, types, md.pos)
+        frms, de, de_total = force_error_vs_fp64(torch, path, box, types, md.pos)
         e2e_val, h2d, d2h = e2e_run(torch, pot, box, types, md.pos, args.e2e_steps)
         times = torch.tensor([ms, ms64 or 0.0, 1.0 / max(e2e_val, 1e-30)], dtype=torch.float64, device="cuda")
         if world > 1:
@@ -348,7 +349,8 @@ def main():
                          "ms_per_step": ms64_max / args.fp64_steps if ms64_max else None,
                          "steps": args.fp64_steps},
                 "fp32_over_fp64": (value / (N * world * args.fp64_steps / (ms64_max * 1e-3))) if ms64_max else None,
-                "accuracy": {"force_rms_fp32_vs_fp64_eV_per_A": frms, "max_abs_dE_per_atom_eV": de},
+                "accuracy": {"force_rms_fp32_vs_fp64_eV_per_A": frms, "max_abs_dE_per_atom_eV": de,
+                             "abs_dE_total_per_atom_eV": de_total},
                 "stage_ms_per_step": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"},
                 "roofline": {"kernel": "k_force (adjoint force/virial)", "bound": "fp32",
                              "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",

@@ -313,6 +313,10 @@ struct Engine {
   double prof_ms[5] = {0, 0, 0, 0, 0};
   long long prof_calls = 0;
   long long launches = 0;  // kernels launched by this handle
+  // flat products + scalars (parameter gradients)
+  DevBuf<int> d_fl, d_fr, d_ft, d_smap;
+  DevBuf<double> d_fc, d_sw;
+  DevBuf<unsigned char> pg_buf;
   // model-specialised CG kernel (NVRTC); empty cubin -> interpreter
   CgSource cg_src;
   CgBinary cg_bin;
@@ -416,6 +420,22 @@ struct Engine {
     d_canon_basic.upload(prog.canon_basic);
     d_shift.upload(model.shift_coeffs);
     d_species.upload(model.species_coeffs);
+    {
+      std::vector<int> l, r, t;
+      std::vector<double> c;
+      for (const Product& p : model.products) {
+        l.push_back(p.left);
+        r.push_back(p.right);
+        t.push_back(p.target);
+        c.push_back(p.coeff);
+      }
+      d_fl.upload(l);
+      d_fr.upload(r);
+      d_ft.upload(t);
+      d_fc.upload(c);
+      d_smap.upload(model.moment_mapping);
+      d_sw.upload(model.moment_coeffs);
+    }
     ck(cudaMallocHost(&h_geom, sizeof(BoxGeom)), "cudaMallocHost");
     ck(cudaMallocHost(&h_status, sizeof(Status)), "cudaMallocHost");
     std::memset(h_status, 0, sizeof(Status));
@@ -600,6 +620,31 @@ struct Engine {
     launches += 2;
   }
 
+  // dL/dw and dL/dc of a loss with upstream weights ew = dL/dE_i, fw = dL/dF_i.
+  template <typename T>
+  void param_grad_impl(cudaStream_t s, const double* ew, const double* fw, double* grad_w, double* grad_c) {
+    const size_t nb = static_cast<size_t>(prog.ncanon) * N;
+    const size_t work = 4ull * model.moments * N;
+    pg_buf.resize((4 * nb + work) * sizeof(T));
+    T* base = reinterpret_cast<T*>(pg_buf.p);
+    FlatProgram fp{};
+    fp.nprod = static_cast<int>(model.products.size());
+    fp.nbasic = prog.nbasic;
+    fp.ncanon = prog.ncanon;
+    fp.nscalar = model.scalar_count;
+    fp.left = d_fl.p;
+    fp.right = d_fr.p;
+    fp.target = d_ft.p;
+    fp.coeff = d_fc.p;
+    fp.basic_canon = d_basic_canon.p;
+    fp.scalar_map = d_smap.p;
+    fp.scalar_w = d_sw.p;
+    if (launch_param_grad<T>(s, edge_args<T>(), fp, model.moments, d_species.p, ew, fw, base, base + nb,
+                             base + 4 * nb, base + 2 * nb, base + 3 * nb, grad_w, grad_c) != 0)
+      throw InputError("SUS2_SH parameter-gradient kernel shape not compiled.");
+    launches += 3;
+  }
+
   void finish(cudaStream_t s) {
     ck(cudaMemcpyAsync(h_status, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
     ck(cudaGetLastError(), "kernel launch");
@@ -755,6 +800,25 @@ int sus2sh_backward(sus2sh_handle* h, const double* grad_potential, double* grad
     if (virial) sus2sh::ck(cudaMemsetAsync(virial, 0, sizeof(double) * 9 * N, s), "memset");
     if (h->e.use_float) h->e.backward_impl<float>(s, grad_potential, grad_position, virial, -1.0);
     else h->e.backward_impl<double>(s, grad_potential, grad_position, virial, -1.0);
+    h->e.finish(s);
+  });
+}
+
+int sus2sh_param_grad(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3], const int* type,
+                      const double* position, const double* energy_weight, const double* force_weight,
+                      double* grad_moment_coeffs, double* grad_radial_coeffs, void* stream) {
+  if (!h || !type || !position || !grad_moment_coeffs || !grad_radial_coeffs || N <= 0) {
+    sus2sh::g_last_error = "sus2sh_param_grad: invalid argument";
+    return SUS2SH_E_ARG;
+  }
+  if (!check_box(box_h, pbc)) return SUS2SH_E_ARG;
+  return guarded([&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->e.prepare(s, N, box_h, pbc, type, position);
+    if (h->e.use_float)
+      h->e.param_grad_impl<float>(s, energy_weight, force_weight, grad_moment_coeffs, grad_radial_coeffs);
+    else
+      h->e.param_grad_impl<double>(s, energy_weight, force_weight, grad_moment_coeffs, grad_radial_coeffs);
     h->e.finish(s);
   });
 }

@@ -1,0 +1,192 @@
+// Per-edge device helpers shared by the engine's kernels: species bits,
+// neighbour stream, image shifts, FP64-to-working-precision edge geometry and
+// the radial basis (values, and values + derivatives).
+#pragma once
+
+#include "engine.cuh"
+#include "sh_math.cuh"
+
+namespace sus2sh {
+namespace edge {
+
+constexpr int kCenterCode = 62;  // image (0,0,0) in base-5 codes
+
+__device__ __forceinline__ int type_of(const double4& p) {
+  return static_cast<int>(__double_as_longlong(p.w));
+}
+
+// ---------------------------------------------------------------------------
+// per-edge geometry and radial basis
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Edge {
+  T r, rinv, ux, uy, uz, dr;  // dr = r - rc (computed from r^2 - rc^2 in FP64)
+  T dx, dy, dz;
+};
+
+template <typename T>
+__device__ __forceinline__ Edge<T> make_edge(double dx, double dy, double dz, double r2, double rc,
+                                             double rc2);
+
+template <>
+__device__ __forceinline__ Edge<float> make_edge<float>(double dx, double dy, double dz, double r2,
+                                                        double rc, double rc2) {
+  Edge<float> e;
+  const float r2f = static_cast<float>(r2);
+  e.rinv = rsqrtf(r2f);
+  e.r = r2f * e.rinv;
+  e.dx = static_cast<float>(dx);
+  e.dy = static_cast<float>(dy);
+  e.dz = static_cast<float>(dz);
+  e.ux = e.dx * e.rinv;
+  e.uy = e.dy * e.rinv;
+  e.uz = e.dz * e.rinv;
+  // (r - rc) without FP32 cancellation near the cutoff
+  e.dr = static_cast<float>(r2 - rc2) / (e.r + static_cast<float>(rc));
+  return e;
+}
+
+template <>
+__device__ __forceinline__ Edge<double> make_edge<double>(double dx, double dy, double dz, double r2,
+                                                          double rc, double rc2) {
+  Edge<double> e;
+  e.r = sqrt(r2);
+  e.rinv = 1.0 / e.r;
+  e.dx = dx;
+  e.dy = dy;
+  e.dz = dz;
+  e.ux = dx * e.rinv;
+  e.uy = dy * e.rinv;
+  e.uz = dz * e.rinv;
+  e.dr = (r2 - rc2) / (e.r + rc);
+  return e;
+}
+
+// R_mu for every mu; the pair table row holds KMU (scal, shift) pairs then
+// the LK pair scale.
+template <typename T, int KMU, int RB>
+__device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __restrict__ row,
+                                              const Edge<T>& e, T* R) {
+  const T f = row[2 * KMU] * e.dr * e.dr;
+  const bool rational = a.rs.rational != 0;
+  if (a.rs.shared_xi) {
+    T xi, dxi;
+    radial_map<T>(T(0.5) * row[0] * (e.r - row[1]), rational, xi, dxi);
+    T t[RB];
+    chebyshev<RB>(xi, t);
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      T s = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) s = fma(a.coef[mu * RB + n], t[n], s);
+      R[mu] = f * s;
+    }
+  } else {
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      T xi, dxi;
+      radial_map<T>(T(0.5) * row[2 * mu] * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+      T t[RB];
+      chebyshev<RB>(xi, t);
+      T s = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) s = fma(a.coef[mu * RB + n], t[n], s);
+      R[mu] = f * s;
+    }
+  }
+}
+
+template <typename T, int KMU, int RB>
+__device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T* __restrict__ row,
+                                                   const Edge<T>& e, T* R, T* dR) {
+  const T ps = row[2 * KMU];
+  const T f = ps * e.dr * e.dr;
+  const T df = T(2) * ps * e.dr;
+  const bool rational = a.rs.rational != 0;
+  if (a.rs.shared_xi) {
+    const T half_scal = T(0.5) * row[0];
+    T xi, dxi;
+    radial_map<T>(half_scal * (e.r - row[1]), rational, xi, dxi);
+    const T g = f * half_scal * dxi;  // f * d xi / dr
+    T t[RB], dt[RB];
+    chebyshev_d<RB>(xi, t, dt);
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      T s = T(0), sd = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) {
+        s = fma(a.coef[mu * RB + n], t[n], s);
+        sd = fma(a.coef[mu * RB + n], dt[n], sd);
+      }
+      R[mu] = f * s;
+      dR[mu] = df * s + g * sd;
+    }
+  } else {
+#pragma unroll
+    for (int mu = 0; mu < KMU; ++mu) {
+      const T half_scal = T(0.5) * row[2 * mu];
+      T xi, dxi;
+      radial_map<T>(half_scal * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+      T t[RB], dt[RB];
+      chebyshev_d<RB>(xi, t, dt);
+      T s = T(0), sd = T(0);
+#pragma unroll
+      for (int n = 0; n < RB; ++n) {
+        s = fma(a.coef[mu * RB + n], t[n], s);
+        sd = fma(a.coef[mu * RB + n], dt[n], sd);
+      }
+      R[mu] = f * s;
+      dR[mu] = df * s + f * half_scal * dxi * sd;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void load_pair_table(const EdgeArgs<T>& a, T* s_tab) {
+  const int n = a.rs.species * a.rs.species * a.rs.pair_stride;
+  const T* src = reinterpret_cast<const T*>(a.pair_table);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) s_tab[t] = src[t];
+  __syncthreads();
+}
+
+// Software-pipelined neighbour stream of one centre atom: the neighbour word
+// is fetched two edges ahead and the neighbour's position one edge ahead, so
+// the dependent gathers overlap the previous edge's arithmetic.
+struct NeighborStream {
+  const int* __restrict__ nbr;
+  const double4* __restrict__ pos4;
+  size_t stride;
+  int cnt;
+  int w_next, w_next2;
+  double4 p_next;
+
+  __device__ __forceinline__ NeighborStream(const int* nb, const double4* p4, int N, int i, int count)
+      : nbr(nb + i), pos4(p4), stride(static_cast<size_t>(N)), cnt(count) {
+    w_next = cnt > 0 ? __ldg(nbr) : 0;
+    w_next2 = cnt > 1 ? __ldg(nbr + stride) : 0;
+    p_next = cnt > 0 ? pos4[w_next & 0xFFFFFF] : make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  // Returns edge n's word and position and issues the loads for n+1 / n+2.
+  __device__ __forceinline__ void next(int n, int& w, double4& pj) {
+    w = w_next;
+    pj = p_next;
+    w_next = w_next2;
+    if (n + 1 < cnt) p_next = pos4[w_next & 0xFFFFFF];
+    if (n + 2 < cnt) w_next2 = __ldg(nbr + static_cast<size_t>(n + 2) * stride);
+  }
+};
+
+// Image shift of a neighbour word (zero for the home image, which is most).
+__device__ __forceinline__ void image_shift(const double (*shift)[3], int code, double& sx, double& sy,
+                                            double& sz) {
+  if (code == kCenterCode) {
+    sx = sy = sz = 0.0;
+  } else {
+    sx = shift[code][0];
+    sy = shift[code][1];
+    sz = shift[code][2];
+  }
+}
+
+}  // namespace edge
+}  // namespace sus2sh

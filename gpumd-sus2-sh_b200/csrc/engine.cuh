@@ -77,6 +77,27 @@ struct ProgramDev {
   const int* canon_basic;  // [ncanon] model basic or -1
 };
 
+// The saved products in file order (flat form) and the scalar weights, for
+// the parameter-gradient pass.
+struct FlatProgram {
+  int nprod, nbasic, ncanon, nscalar;
+  const int* left;
+  const int* right;
+  const int* target;
+  const double* coeff;
+  const int* basic_canon;
+  const int* scalar_map;
+  const double* scalar_w;
+};
+
+// Parameter gradients (param_grad.cu): weights ew = dL/dE_i (N, may be NULL)
+// and fw = dL/dF_i (3N SoA, may be NULL); grad_w [nscalar] and grad_c
+// [kmu*rb] are assigned.  B, Bd, Galpha, Gbeta: [K*C][N]; work: [4 M][N].
+template <typename T>
+int launch_param_grad(cudaStream_t s, const EdgeArgs<T>& a, const FlatProgram& p, int M,
+                      const double* species_coeffs, const double* ew, const double* fw, T* B, T* Bd, T* work,
+                      T* Galpha, T* Gbeta, double* grad_w, double* grad_c);
+
 // Program tables of a handle, for kernels outside the handle's own path.
 struct CgView {
   ProgramDev prog;

@@ -90,6 +90,20 @@ int sus2sh_forward(sus2sh_handle* h, int N, const double box_h[9], const int pbc
 int sus2sh_backward(sus2sh_handle* h, const double* grad_potential, double* grad_position,
                     double* virial, void* stream);
 
+/* Gradient of a loss L(E_i, F_i) with respect to the model's linear weights
+ * (moment_coeffs, [alpha_scalar_moments]) and radial coefficients
+ * (radial_coeffs without the species columns, [radial_funcs_count][rb], the
+ * .mtp order).  The caller passes the upstream weights energy_weight[i] =
+ * dL/dE_i ([N], NULL = 0) and force_weight = dL/dF_i ([3N] SoA, NULL = 0);
+ * the force part is the forward-over-reverse derivative of dE/dtheta along
+ * force_weight (moments recomputed, nothing stored per pair).  Outputs are
+ * device arrays, assigned.  The reference has no counterpart (its trainer
+ * lives in a separate project); this is the gradient path of the engine. */
+int sus2sh_param_grad(sus2sh_handle* h, int N, const double box_h[9], const int pbc[3],
+                      const int* type, const double* position, const double* energy_weight,
+                      const double* force_weight, double* grad_moment_coeffs,
+                      double* grad_radial_coeffs, void* stream);
+
 /* Host-buffer variant of sus2sh_compute for callers without device arrays:
  * copies type/position in, evaluates, and copies per-atom energy, forces and
  * the total virial (9 values, xx yy zz xy xz yz yx zx zy) out.  Outputs are
