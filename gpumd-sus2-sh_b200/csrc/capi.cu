@@ -313,6 +313,11 @@ struct Engine {
   double prof_ms[5] = {0, 0, 0, 0, 0};
   long long prof_calls = 0;
   long long launches = 0;  // kernels launched by this handle
+  // batches of cells
+  bool batch_active = false;
+  int batch_ncells = 0;
+  DevBuf<double> d_cell_hinv, d_cell_shift;
+  DevBuf<int> d_cell_reach, d_batch_cell;
   // flat products + scalars (parameter gradients)
   DevBuf<int> d_fl, d_fr, d_ft, d_smap;
   DevBuf<double> d_fc, d_sw;
@@ -507,7 +512,13 @@ struct Engine {
     a.nbr = nbr.p;
     a.ncount = ncount.p;
     a.pair_table = use_float ? static_cast<const void*>(d_pair_f.p) : static_cast<const void*>(d_pair_d.p);
-    a.shift = d_geom.p->shift;
+    if (batch_active) {
+      a.shift = reinterpret_cast<const double(*)[3]>(d_cell_shift.p);
+      a.atom_cell = d_batch_cell.p;
+    } else {
+      a.shift = d_geom.p->shift;
+      a.atom_cell = nullptr;
+    }
     for (size_t k = 0; k < coef.size(); ++k) a.coef[k] = static_cast<T>(coef[k]);
     return a;
   }
@@ -525,10 +536,54 @@ struct Engine {
     return p;
   }
 
+  // Batch of independent cells: geometry tables, packing and a fresh
+  // neighbour list (cutoff rc, no skin) on every call.  After the first call
+  // with a given (N, ncells) nothing synchronises or allocates, so the call
+  // can be captured in a CUDA graph.
+  void prepare_batch(cudaStream_t s, int n, int ncells, const int* off, const double* cell_h, const int* cell_pbc,
+                     const int* type, const double* x) {
+    if (ncells <= 0) throw InputError("sus2sh batch: ncells must be positive.");
+    ensure_size(n);
+    last_stream = s;
+    if (ncells != batch_ncells) {
+      d_cell_hinv.resize(9ull * ncells);
+      d_cell_reach.resize(3ull * ncells);
+      d_cell_shift.resize(375ull * ncells);
+      batch_ncells = ncells;
+      cap = 0;
+    }
+    d_batch_cell.resize(N);
+    batch_active = true;
+    have_ref = false;  // the single-box list is no longer current
+    force_next = true;
+    launch_batch_geometry(s, ncells, cell_h, cell_pbc, model.rc, d_cell_hinv.p, d_cell_reach.p,
+                          reinterpret_cast<double(*)[3]>(d_cell_shift.p), &d_status.p->thin_cell);
+    launch_batch_pack(s, N, ncells, off, x, type, cell_h, d_cell_hinv.p, cell_pbc, model.species_count,
+                      d_batch_cell.p, pos4.p, d_status.p);
+    launches += 2;
+    const double cutoff2 = model.rc * model.rc;
+    if (cap == 0) {
+      ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
+      launch_batch_fill(s, N, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nullptr, ncount.p, 0, 1,
+                        d_status.p);
+      Status st{};
+      ck(cudaMemcpyAsync(&st, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
+      ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+      if (st.thin_cell) throw InputError("sus2sh batch: a periodic cell is thinner than half the cutoff.");
+      grow_capacity(st.max_count);
+      launches += 1;
+    }
+    launch_batch_fill(s, N, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nbr.p, ncount.p, cap, 0,
+                      d_status.p);
+    launches += 1;
+    ck(cudaGetLastError(), "batch neighbour build launch");
+  }
+
   // Positions -> pos4, conditional neighbour build.
   void prepare(cudaStream_t s, int n, const double* h, const int* pbc, const int* type, const double* x) {
     ensure_size(n);
     last_stream = s;
+    batch_active = false;
     bool box_changed = false;
     for (int k = 0; k < 9; ++k) box_changed |= h[k] != last_h[k];
     for (int k = 0; k < 3; ++k) box_changed |= (pbc[k] ? 1 : 0) != last_pbc[k];
@@ -676,6 +731,7 @@ struct Engine {
       h_status->overflow = 0;
       force_next = true;
     }
+    if (h_status->thin_cell) f |= SUS2SH_STATUS_THIN_CELL;
     if (h_status->bad_type) {
       f |= SUS2SH_STATUS_BAD_TYPE;
       const int zero = 0;
@@ -815,6 +871,54 @@ int sus2sh_param_grad(sus2sh_handle* h, int N, const double box_h[9], const int 
   return guarded([&] {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     h->e.prepare(s, N, box_h, pbc, type, position);
+    if (h->e.use_float)
+      h->e.param_grad_impl<float>(s, energy_weight, force_weight, grad_moment_coeffs, grad_radial_coeffs);
+    else
+      h->e.param_grad_impl<double>(s, energy_weight, force_weight, grad_moment_coeffs, grad_radial_coeffs);
+    h->e.finish(s);
+  });
+}
+
+int sus2sh_compute_batch(sus2sh_handle* h, int N, int ncells, const int* cell_offset, const double* cell_h,
+                         const int* cell_pbc, const int* type, const double* position, double* potential,
+                         double* force, double* virial, double* cell_energy, double* cell_virial, void* stream) {
+  if (!h || !cell_offset || !cell_h || !type || !position || !potential || !force || !virial || N <= 0 ||
+      ncells <= 0) {
+    sus2sh::g_last_error = "sus2sh_compute_batch: invalid argument";
+    return SUS2SH_E_ARG;
+  }
+  return guarded([&] {
+    sus2sh::Engine& e = h->e;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    e.prepare_batch(s, N, ncells, cell_offset, cell_h, cell_pbc, type, position);
+    if (e.use_float) {
+      e.forward_impl<float>(s, potential, 0);
+      e.backward_impl<float>(s, nullptr, force, virial, 1.0);
+    } else {
+      e.forward_impl<double>(s, potential, 0);
+      e.backward_impl<double>(s, nullptr, force, virial, 1.0);
+    }
+    if (cell_energy || cell_virial) {
+      sus2sh::launch_cell_reduce(s, ncells, N, cell_offset, potential, cell_virial ? virial : nullptr, cell_energy,
+                                 cell_virial);
+      e.launches += 1;
+    }
+    e.finish(s);
+  });
+}
+
+int sus2sh_param_grad_batch(sus2sh_handle* h, int N, int ncells, const int* cell_offset, const double* cell_h,
+                            const int* cell_pbc, const int* type, const double* position, const double* energy_weight,
+                            const double* force_weight, double* grad_moment_coeffs, double* grad_radial_coeffs,
+                            void* stream) {
+  if (!h || !cell_offset || !cell_h || !type || !position || !grad_moment_coeffs || !grad_radial_coeffs ||
+      N <= 0 || ncells <= 0) {
+    sus2sh::g_last_error = "sus2sh_param_grad_batch: invalid argument";
+    return SUS2SH_E_ARG;
+  }
+  return guarded([&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    h->e.prepare_batch(s, N, ncells, cell_offset, cell_h, cell_pbc, type, position);
     if (h->e.use_float)
       h->e.param_grad_impl<float>(s, energy_weight, force_weight, grad_moment_coeffs, grad_radial_coeffs);
     else

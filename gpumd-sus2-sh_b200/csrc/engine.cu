@@ -253,6 +253,7 @@ __global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_BASIC_MIN_BL
 #pragma unroll
   for (int b = 0; b < NB; ++b) acc[b] = T(0);
   const double4 pi = a.pos4[i];
+  const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
   const int S = a.rs.species;
   const int row_i = type_of(pi) * S;
   const int cnt = min(a.ncount[i], a.cap);
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_BASIC_MIN_BL
     double4 pj;
     ns.next(n, w, pj);
     double sx, sy, sz;
-    image_shift(a.shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
+    image_shift(cell_shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
     const double dx = pj.x - pi.x + sx;
     const double dy = pj.y - pi.y + sy;
     const double dz = pj.z - pi.z + sz;
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_FORCE_MIN_BL
 #pragma unroll
   for (int q = 0; q < 9; ++q) w[q] = T(0);
   const double4 pi = a.pos4[i];
+  const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
   const int S = a.rs.species;
   const int row_i = type_of(pi) * S;
   const int cnt = min(a.ncount[i], a.cap);
@@ -339,7 +341,7 @@ __global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_FORCE_MIN_BL
     ns.next(n, wd, pj);
     const int j = wd & 0xFFFFFF;
     double sx, sy, sz;
-    image_shift(a.shift, static_cast<unsigned>(wd) >> 24, sx, sy, sz);
+    image_shift(cell_shift, static_cast<unsigned>(wd) >> 24, sx, sy, sz);
     const double dx = pj.x - pi.x + sx;
     const double dy = pj.y - pi.y + sy;
     const double dz = pj.z - pi.z + sz;

@@ -37,7 +37,8 @@ struct Status {
   int max_count;               // largest neighbour count seen at a build
   int builds;                  // number of builds
   int bad_type;                // a species index outside [0, species_count) was seen (sticky)
-  int pad[2];
+  int thin_cell;               // a batch cell thinner than half the cutoff (sticky)
+  int pad;
 };
 
 // Radial table: per pair p = t_i*S + t_j: [KMU] (scal, shift) pairs then the
@@ -62,7 +63,8 @@ struct EdgeArgs {
   const int* nbr;
   const int* ncount;
   const void* pair_table;   // T[S*S][pair_stride]
-  const double (*shift)[3];  // device copy of BoxGeom::shift
+  const double (*shift)[3];  // image vectors [cells][125][3] (one box: BoxGeom::shift)
+  const int* atom_cell;      // cell of each atom in a batch of boxes, NULL for one box
   T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
 };
 
@@ -128,6 +130,20 @@ void launch_product(cudaStream_t s, int N, const ProgramDev& p, const double4* p
                     const double* species_coeffs, double* pe, int pe_assign);
 template <typename T>
 void launch_finalize(cudaStream_t s, int N, const void* ftmp, double* force, double sign);
+
+// Batches of independent periodic boxes (cells) evaluated in one pass.
+// Cell c holds atoms [off[c], off[c+1]); box columns cell_h[9c..9c+8].
+void launch_batch_geometry(cudaStream_t s, int ncells, const double* cell_h, const int* cell_pbc,
+                           double cutoff, double* cell_hinv, int* cell_reach, double (*cell_shift)[3],
+                           int* status_error);
+void launch_batch_pack(cudaStream_t s, int N, int ncells, const int* off, const double* x, const int* type,
+                       const double* cell_h, const double* cell_hinv, const int* cell_pbc, int species,
+                       int* atom_cell, double4* pos4, Status* st);
+void launch_batch_fill(cudaStream_t s, int N, const int* off, const int* atom_cell, const double4* pos4,
+                       const double* cell_h, const int* cell_reach, double cutoff2, int* nbr, int* ncount,
+                       int cap, int count_only, Status* st);
+void launch_cell_reduce(cudaStream_t s, int ncells, int N, const int* off, const double* pe, const double* virial,
+                        double* cell_energy, double* cell_virial);
 
 // Integrator kernels for the benchmark MD driver.
 void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_mass_type,

@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
   for (int b = 0; b < NB; ++b) acc[b] = accd[b] = T(0);
   const double4 pi = a.pos4[i];
+  const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
   const double bix = fw ? fw[i] : 0.0, biy = fw ? fw[i + a.N] : 0.0, biz = fw ? fw[i + 2 * a.N] : 0.0;
   const int row_i = type_of(pi) * a.rs.species;
   const int cnt = min(a.ncount[i], a.cap);
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(128)
     const int j = w & 0xFFFFFF;
     const double4 pj = a.pos4[j];
     double sx, sy, sz;
-    image_shift(a.shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
+    image_shift(cell_shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
     const double dx = pj.x - pi.x + sx, dy = pj.y - pi.y + sy, dz = pj.z - pi.z + sz;
     const double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 >= rc2) continue;
@@ -204,6 +205,7 @@ __global__ void __launch_bounds__(128)
       be[b] = Gbeta[static_cast<size_t>(b) * a.N + i];
     }
     const double4 pi = a.pos4[i];
+    const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
     const double bix = fw ? fw[i] : 0.0, biy = fw ? fw[i + a.N] : 0.0, biz = fw ? fw[i + 2 * a.N] : 0.0;
     const int row_i = type_of(pi) * a.rs.species;
     const int cnt = min(a.ncount[i], a.cap);
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(128)
       const int j = w & 0xFFFFFF;
       const double4 pj = a.pos4[j];
       double sx, sy, sz;
-      image_shift(a.shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
+      image_shift(cell_shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
       const double dx = pj.x - pi.x + sx, dy = pj.y - pi.y + sy, dz = pj.z - pi.z + sz;
       const double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 >= rc2) continue;

@@ -14,7 +14,7 @@ EXPORTS = (
     "sus2sh_is_sus2_sh_file", "sus2sh_create", "sus2sh_compute", "sus2sh_destroy",
     "sus2sh_cutoff", "sus2sh_last_error", "sus2sh_sync", "sus2sh_forward", "sus2sh_backward",
     "sus2sh_compute_host", "sus2sh_model_info", "sus2sh_profile", "sus2sh_profile_read",
-    "sus2sh_cg_energy_noalloc", "sus2sh_param_grad",
+    "sus2sh_cg_energy_noalloc", "sus2sh_param_grad", "sus2sh_compute_batch", "sus2sh_param_grad_batch",
     "sus2sh_write_synthetic_model", "sus2sh_standard_graph_counts", "sus2sh_md_kick_drift",
     "sus2sh_md_kick", "sus2sh_reduce", "sus2sh_random_insertion", "sus2sh_measure_fma_peak",
     "sus2sh_cg_kernel_info",
@@ -51,6 +51,8 @@ def load() -> ctypes.CDLL:
         "sus2sh_profile": (I, [P, I]),
         "sus2sh_cg_energy_noalloc": (I, [P, I, P, P, P, P, P]),
         "sus2sh_param_grad": (I, [P, I, P, P, P, P, P, P, P, P, P]),
+        "sus2sh_compute_batch": (I, [P, I, I, P, P, P, P, P, P, P, P, P, P, P]),
+        "sus2sh_param_grad_batch": (I, [P, I, I, P, P, P, P, P, P, P, P, P, P]),
         "sus2sh_profile_read": (I, [P, P, I]),
         "sus2sh_measure_fma_peak": (I, [I, P]),
         "sus2sh_cg_kernel_info": (I, [S, I, P, P, ctypes.c_size_t]),

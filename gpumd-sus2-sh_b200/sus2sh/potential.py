@@ -133,6 +133,25 @@ class SUS2_SH:
             ctypes.c_void_p(type_ptr), ctypes.c_void_p(pos_ptr), ctypes.c_void_p(pe_ptr),
             ctypes.c_void_p(f_ptr), ctypes.c_void_p(vt_ptr), _stream_ptr(stream)), "sus2sh_compute_host")
 
+    def compute_batch(self, cell_offset, cell_h, type_, position, potential, force, virial, cell_pbc=None,
+                      cell_energy=None, cell_virial=None, stream=None):
+        """Batch of independent cells (device tensors; see sus2sh_compute_batch)."""
+        N = type_.numel()
+        ncells = cell_offset.numel() - 1
+        _lib.check(self._lib.sus2sh_compute_batch(
+            self._h, N, ncells, _ptr(cell_offset), _ptr(cell_h), _ptr(cell_pbc), _ptr(type_), _ptr(position),
+            _ptr(potential), _ptr(force), _ptr(virial), _ptr(cell_energy), _ptr(cell_virial),
+            _stream_ptr(stream)), "sus2sh_compute_batch")
+
+    def param_grad_batch(self, cell_offset, cell_h, type_, position, energy_weight, force_weight, grad_w, grad_c,
+                         cell_pbc=None, stream=None):
+        N = type_.numel()
+        ncells = cell_offset.numel() - 1
+        _lib.check(self._lib.sus2sh_param_grad_batch(
+            self._h, N, ncells, _ptr(cell_offset), _ptr(cell_h), _ptr(cell_pbc), _ptr(type_), _ptr(position),
+            _ptr(energy_weight), _ptr(force_weight), _ptr(grad_w), _ptr(grad_c), _stream_ptr(stream)),
+            "sus2sh_param_grad_batch")
+
     def profile(self, enable: bool = True):
         _lib.check(self._lib.sus2sh_profile(self._h, 1 if enable else 0), "sus2sh_profile")
 

@@ -76,3 +76,26 @@ def maxwell_boltzmann(types: np.ndarray, masses, temperature: float, seed: int =
     if t_now > 0:
         v *= np.sqrt(temperature / t_now)
     return np.ascontiguousarray(v)
+
+
+def cell_batch(n_cells: int, n_min: int = 16, n_max: int = 512, density: float = 0.06, dmin: float = 2.1,
+               ratio_range=(0.8, 1.25), fractions=(0.5, 0.5), seed: int = 0):
+    """Batch of independent periodic random-insertion cells with atom counts
+    uniform in [n_min, n_max] and orthorhombic edge ratios uniform in
+    ratio_range.  Returns (offsets[n_cells+1], cell_h[n_cells, 9], boxes,
+    types[N], positions[3, N]) with the cells concatenated."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(n_min, n_max + 1, size=n_cells)
+    offsets = np.zeros(n_cells + 1, dtype=np.int32)
+    offsets[1:] = np.cumsum(counts)
+    hs, boxes, ts, ps = [], [], [], []
+    for c in range(n_cells):
+        ratios = rng.uniform(ratio_range[0], ratio_range[1], size=3)
+        box, types, pos = random_insertion(int(counts[c]), density, dmin, ratios, fractions,
+                                           seed=int(rng.integers(1 << 31)))
+        hs.append(box.cpu_h)
+        boxes.append(box)
+        ts.append(types)
+        ps.append(pos)
+    return (offsets, np.stack(hs), boxes, np.concatenate(ts).astype(np.int32),
+            np.ascontiguousarray(np.concatenate(ps, axis=1)))

@@ -37,6 +37,7 @@ typedef struct sus2sh_handle sus2sh_handle;
 /* status flags returned by sus2sh_sync */
 #define SUS2SH_STATUS_OVERFLOW 1
 #define SUS2SH_STATUS_BAD_TYPE 2  /* a type was outside [0, species_count) */
+#define SUS2SH_STATUS_THIN_CELL 4 /* a batch cell is thinner than half the cutoff */
 
 /* Replaces is_sus2_sh_potential_file (src/force/sus2_sh.cu:7771-7780,
  * declared src/force/sus2_sh.cuh:205): 1 if the file contains
@@ -103,6 +104,30 @@ int sus2sh_param_grad(sus2sh_handle* h, int N, const double box_h[9], const int 
                       const int* type, const double* position, const double* energy_weight,
                       const double* force_weight, double* grad_moment_coeffs,
                       double* grad_radial_coeffs, void* stream);
+
+/* Batch of independent periodic cells in one call (many small training or
+ * screening structures).  All arrays are device arrays: cell c holds atoms
+ * [cell_offset[c], cell_offset[c+1]) of the concatenated SoA position/type
+ * arrays (N = cell_offset[ncells]); cell_h[9c..9c+8] is its box in the
+ * box_h layout; cell_pbc[3c..3c+2] its periodicity (NULL = periodic).  Each
+ * cell may be as thin as half of rc (images are explicit).  Outputs accumulate
+ * like sus2sh_compute; cell_energy [ncells] and cell_virial [9 ncells] (NULL
+ * to skip) are assigned.  After the first call with a given (N, ncells) the
+ * call neither allocates nor synchronises, so it can be captured in a CUDA
+ * graph and replayed.  The reference evaluates one box per call
+ * (SUS2_SH::compute, src/force/sus2_sh.cu:9620). */
+int sus2sh_compute_batch(sus2sh_handle* h, int N, int ncells, const int* cell_offset,
+                         const double* cell_h, const int* cell_pbc, const int* type,
+                         const double* position, double* potential, double* force, double* virial,
+                         double* cell_energy, double* cell_virial, void* stream);
+
+/* sus2sh_param_grad over a batch of cells (arguments as in
+ * sus2sh_compute_batch and sus2sh_param_grad). */
+int sus2sh_param_grad_batch(sus2sh_handle* h, int N, int ncells, const int* cell_offset,
+                            const double* cell_h, const int* cell_pbc, const int* type,
+                            const double* position, const double* energy_weight,
+                            const double* force_weight, double* grad_moment_coeffs,
+                            double* grad_radial_coeffs, void* stream);
 
 /* Host-buffer variant of sus2sh_compute for callers without device arrays:
  * copies type/position in, evaluates, and copies per-atom energy, forces and

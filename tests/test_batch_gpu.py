@@ -1,0 +1,139 @@
+"""Batches of small periodic cells of uneven size in one pass
+(sus2sh_compute_batch / sus2sh_param_grad_batch), against the FP64 oracle
+cell by cell, and captured in a CUDA graph."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+import sus2sh_oracle as O  # noqa: E402
+from sus2sh import SUS2_SH, structures  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def batch():
+    return structures.cell_batch(24, 16, 512, seed=41)
+
+
+def _run(pot, off, H, types, pos, dev, cell=True):
+    N = types.size
+    ncells = off.size - 1
+    t = torch.as_tensor(types, device=dev)
+    x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
+    o = torch.as_tensor(off, device=dev)
+    h = torch.as_tensor(H.reshape(-1).copy(), device=dev)
+    pe = torch.zeros(N, dtype=torch.float64, device=dev)
+    f = torch.zeros(3 * N, dtype=torch.float64, device=dev)
+    w = torch.zeros(9 * N, dtype=torch.float64, device=dev)
+    ce = torch.zeros(ncells, dtype=torch.float64, device=dev)
+    cw = torch.zeros(9 * ncells, dtype=torch.float64, device=dev)
+    pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce, cell_virial=cw)
+    torch.cuda.synchronize()
+    assert pot.sync() == 0
+    return pe.cpu().numpy(), f.view(3, N).cpu().numpy(), w.view(9, N).cpu().numpy(), ce.cpu().numpy(), \
+        cw.view(ncells, 9).cpu().numpy()
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_batch_matches_oracle_cell_by_cell(l3k3_path, batch, fp64):
+    off, H, boxes, types, pos = batch
+    dev = torch.device("cuda")
+    pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr"] + (["sus2_float=0"] if fp64 else []))
+    pe, f, w, ce, cw = _run(pot, off, H, types, pos, dev)
+    orc = O.Oracle(l3k3_path)
+    etol, frms_tol = (1e-9, 1e-9) if fp64 else (1e-6, 1e-5)
+    for c, box in enumerate(boxes):
+        a, b = off[c], off[c + 1]
+        pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types[a:b], pos[:, a:b])
+        assert np.abs(pe[a:b] - pe0).max() < etol
+        assert np.sqrt(((f[:, a:b] - f0) ** 2).mean()) < frms_tol
+        assert np.sqrt(((w[:, a:b] - w0) ** 2).mean()) < frms_tol
+        assert abs(ce[c] - pe0.sum()) < etol * (b - a)
+        assert np.abs(cw[c] - w0.sum(axis=1)).max() < frms_tol * (b - a)
+    pot.close()
+
+
+def test_batch_in_a_cuda_graph(l3k3_path, batch):
+    off, H, boxes, types, pos = batch
+    dev = torch.device("cuda")
+    N, ncells = types.size, off.size - 1
+    pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr"])
+    ref = _run(pot, off, H, types, pos, dev)  # first call sizes the lists
+    t = torch.as_tensor(types, device=dev)
+    x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
+    o = torch.as_tensor(off, device=dev)
+    h = torch.as_tensor(H.reshape(-1).copy(), device=dev)
+    pe = torch.zeros(N, dtype=torch.float64, device=dev)
+    f = torch.zeros(3 * N, dtype=torch.float64, device=dev)
+    w = torch.zeros(9 * N, dtype=torch.float64, device=dev)
+    ce = torch.zeros(ncells, dtype=torch.float64, device=dev)
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        pe.zero_(); f.zero_(); w.zero_()
+        pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce)  # warm-up on the capture stream
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        pe.zero_(); f.zero_(); w.zero_()
+        pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(pe.cpu().numpy(), ref[0])
+    assert np.abs(f.view(3, N).cpu().numpy() - ref[1]).max() < 1e-6
+    assert np.array_equal(ce.cpu().numpy(), ref[3])
+    # new positions in the same buffers: the replay re-evaluates them
+    pos2 = pos + np.random.default_rng(3).normal(0, 0.02, size=pos.shape)
+    x.copy_(torch.as_tensor(pos2.reshape(-1)))
+    g.replay()
+    torch.cuda.synchronize()
+    orc = O.Oracle(l3k3_path)
+    for c in (0, 7, ncells - 1):
+        a, b = off[c], off[c + 1]
+        pe0, f0, _ = orc.efs(boxes[c].cpu_h, boxes[c].pbc, types[a:b], pos2[:, a:b])
+        assert np.abs(pe.cpu().numpy()[a:b] - pe0).max() < 1e-6
+    del g
+    pot.close()
+
+
+def test_param_grad_batch_equals_sum_over_cells(l3k3_path, batch):
+    import ctypes
+    off, H, boxes, types, pos = batch
+    dev = torch.device("cuda")
+    N = types.size
+    pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr", "sus2_float=0"])
+    info = pot.info()
+    nsc, nrad = info["scalars"], info["k_max"] * (info["l_max"] + 1) * info["rb_size"]
+    rng = np.random.default_rng(9)
+    ew = rng.normal(size=N)
+    fw = rng.normal(size=(3, N)) * 0.1
+    T = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    gw = torch.zeros(nsc, dtype=torch.float64, device=dev)
+    gc = torch.zeros(nrad, dtype=torch.float64, device=dev)
+    pot.param_grad_batch(T(off, torch.int32), T(H.reshape(-1)), T(types, torch.int32), T(pos.reshape(-1)),
+                         T(ew), T(fw.reshape(-1)), gw, gc)
+    torch.cuda.synchronize()
+    from sus2sh import _lib
+    lib = _lib.load()
+    sw, sc = np.zeros(nsc), np.zeros(nrad)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    for c, box in enumerate(boxes):
+        a, b = off[c], off[c + 1]
+        n = b - a
+        gw1 = torch.zeros(nsc, dtype=torch.float64, device=dev)
+        gc1 = torch.zeros(nrad, dtype=torch.float64, device=dev)
+        tt, xx = T(types[a:b], torch.int32), T(pos[:, a:b].reshape(-1))
+        e1, f1 = T(ew[a:b]), T(fw[:, a:b].reshape(-1))
+        rc = lib.sus2sh_param_grad(pot.handle, n, box.cpu_h.ctypes.data_as(ctypes.c_void_p),
+                                   box.pbc.ctypes.data_as(ctypes.c_void_p), p(tt), p(xx), p(e1), p(f1),
+                                   p(gw1), p(gc1), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0
+        sw += gw1.cpu().numpy()
+        sc += gc1.cpu().numpy()
+    assert np.abs(gw.cpu().numpy() - sw).max() < 1e-9 * max(1.0, np.abs(sw).max())
+    assert np.abs(gc.cpu().numpy() - sc).max() < 1e-9 * max(1.0, np.abs(sc).max())
+    pot.close()
