@@ -53,6 +53,7 @@ def parse_args():
     ap.add_argument("--fp64-steps", type=int, default=50)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batch-cell and large-model fields")
     return ap.parse_args()
 
 
@@ -236,6 +237,101 @@ def e2e_run(torch, pot, box, types, x_dev, steps):
     return N * steps / dt, 28 * N, 32 * N + 72
 
 
+def batch_cells_run(torch, path, ncells=4096, reps=10):
+    """Uneven-cell batch workload: 4096 periodic random-insertion cells with
+    16-512 atoms, density 0.06 A^-3, d_min 2.1 A, orthorhombic edge ratios
+    0.8-1.25; energies, forces, virials and per-cell sums through one CUDA
+    graph replay per evaluation; then the batched parameter gradients."""
+    from sus2sh import SUS2_SH, structures
+    off, H, boxes, types, pos = structures.cell_batch(ncells, 16, 512, seed=4242)
+    N = types.size
+    dev = torch.device("cuda")
+    pot = SUS2_SH(path, N, ["Cu", "Zr"])
+    t = torch.as_tensor(types, device=dev)
+    x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
+    o = torch.as_tensor(off, device=dev)
+    h = torch.as_tensor(H.reshape(-1).copy(), device=dev)
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)
+    pe, f, w, ce, cw = z(N), z(3 * N), z(9 * N), z(ncells), z(9 * ncells)
+    pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce, cell_virial=cw)  # sizes lists, tunes tiles
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        pe.zero_(); f.zero_(); w.zero_()
+        pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce, cell_virial=cw)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        pe.zero_(); f.zero_(); w.zero_()
+        pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce, cell_virial=cw)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flags = pot.sync()
+    info = pot.info()
+    nsc = info["scalars"]
+    nrad = info["k_max"] * (info["l_max"] + 1) * info["rb_size"]
+    ew = torch.ones(N, dtype=torch.float64, device=dev)
+    fw = torch.full((3 * N,), 0.01, dtype=torch.float64, device=dev)
+    gw, gc = z(nsc), z(nrad)
+    pot.param_grad_batch(o, h, t, x, ew, fw, gw, gc)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(3):
+        pot.param_grad_batch(o, h, t, x, ew, fw, gw, gc)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_grad = e0.elapsed_time(e1) / 3
+    del g
+    pot.close()
+    return {"workload": "4096 uneven periodic cells (16-512 atoms), l3k3 FP32, one CUDA graph per evaluation",
+            "cells": ncells, "atoms": N, "ms_per_eval": ms, "atom_evals_per_s": N / (ms * 1e-3),
+            "param_grad_ms": ms_grad, "status_flags": flags,
+            "tiles": {"basic_block": info["basic_block"], "force_block": info["force_block"]}}
+
+
+def large_model_run(torch, model_dir, reps=5):
+    """Large-model workload: Cu-Zr-Al body-5 L=4 K=4 rb10 rational-map model
+    (5985 moments, 33,389 products) on 262,144 random-insertion atoms
+    (0.06 A^-3, d_min 2.1 A, 50/35/15), FP32; static positions, one
+    energy/force/virial evaluation per step."""
+    from sus2sh import SUS2_SH, models, structures
+    path = models.preset_model("l4k4", model_dir)
+    box, types, pos = structures.random_insertion(262144, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=77)
+    N = types.size
+    dev = torch.device("cuda")
+    pot = SUS2_SH(path, N, ["Cu", "Zr", "Al"])
+    t = torch.as_tensor(types, device=dev)
+    x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)
+    pe, f, w = z(N), z(3 * N), z(9 * N)
+    for _ in range(2):
+        pot.compute(box, t, x, pe, f, w)
+    torch.cuda.synchronize()
+    pot.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        pot.compute(box, t, x, pe, f, w)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    prof = pot.profile_read()
+    flags = pot.sync()
+    pot.close()
+    return {"workload": "262,144-atom Cu-Zr-Al l4k4 body-5 rational model, FP32", "atoms": N,
+            "ms_per_eval": ms, "atom_steps_per_s": N / (ms * 1e-3), "status_flags": flags,
+            "stage_ms_per_eval": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"}}
+
+
 def cpu_baseline_sample(path, cells=20, reps=3):
     sys.path.insert(0, ORACLE)
     import sus2sh_oracle
@@ -367,6 +463,9 @@ def main():
                 "gpu_launches": launches,
                 "clocks": clk,
             }
+            if world == 1 and not args.no_extra:
+                line["batch_cells"] = batch_cells_run(torch, path)
+                line["large_model"] = large_model_run(torch, d)
             if world == 1 and not args.no_cpu_baseline:
                 line["cpu_baseline"] = cpu_baseline_sample(path)
             print(json.dumps(line), flush=True)

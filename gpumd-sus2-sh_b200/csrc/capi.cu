@@ -5,6 +5,7 @@
 #include "cg_codegen.h"
 #include "engine.cuh"
 #include "mtp_model.h"
+#include "zbl.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -313,6 +314,10 @@ struct Engine {
   double prof_ms[5] = {0, 0, 0, 0, 0};
   long long prof_calls = 0;
   long long launches = 0;  // kernels launched by this handle
+  // ZBL tables
+  DevBuf<int> d_zbl_z;
+  DevBuf<double> d_zbl_in, d_zbl_out;
+  double list_cutoff = 0.0;  // max(rc, largest ZBL outer cutoff)
   // batches of cells
   bool batch_active = false;
   int batch_ncells = 0;
@@ -322,6 +327,9 @@ struct Engine {
   DevBuf<int> d_fl, d_fr, d_ft, d_smap;
   DevBuf<double> d_fc, d_sw;
   DevBuf<unsigned char> pg_buf;
+  // tile autotuner: CTA sizes of the edge kernels, timed on the first call
+  int basic_block = 128, force_block = 128;
+  bool tuned = false;
   // model-specialised CG kernel (NVRTC); empty cubin -> interpreter
   CgSource cg_src;
   CgBinary cg_bin;
@@ -379,6 +387,33 @@ struct Engine {
       throw InputError("SUS2_SH engine has no compiled kernel for sh_l_max=" + std::to_string(model.l_max) +
                        ", sh_k_max=" + std::to_string(model.k_max) +
                        ", radial_basis_size=" + std::to_string(model.rb_size) + ".");
+    }
+    list_cutoff = model.rc;
+    if (model.zbl_enabled) {
+      // atomic numbers from the model, else from the element symbols after the
+      // file name (SUS2_SH constructor, sus2_sh.cu:7824-7860)
+      std::vector<int> z = model.zbl_atomic_numbers;
+      if (z.empty()) {
+        if (nopts < model.species_count)
+          throw InputError(
+              "SUS2_SH ZBL model requires zbl_atomic_numbers metadata or element symbols after the model file.");
+        for (int t = 0; t < model.species_count; ++t) {
+          const std::string sym = opts[t] ? opts[t] : "";
+          const int an = zbl::atomic_number(sym);
+          if (an <= 0) throw InputError("SUS2_SH ZBL cannot map element symbol to an atomic number: " + sym);
+          z.push_back(an);
+        }
+      }
+      if (static_cast<int>(z.size()) != model.species_count)
+        throw InputError("SUS2_SH ZBL metadata should provide one atomic number per species.");
+      std::vector<double> pin, pout;
+      const std::string err = zbl::pair_cutoffs(z, model.zbl_inner, model.zbl_outer, model.zbl_typewise,
+                                                model.zbl_typewise ? model.zbl_typewise_factor : 0.0, pin, pout);
+      if (!err.empty()) throw InputError("SUS2_SH ZBL metadata error: " + err);
+      d_zbl_z.upload(z);
+      d_zbl_in.upload(pin);
+      d_zbl_out.upload(pout);
+      for (double o : pout) list_cutoff = std::max(list_cutoff, o);
     }
     const int S = model.species_count, kmu = model.radial_funcs, rb = model.rb_size;
     // radial tables: unscaled c[mu][n] uniform; per-pair (scal, shift) and
@@ -556,12 +591,12 @@ struct Engine {
     batch_active = true;
     have_ref = false;  // the single-box list is no longer current
     force_next = true;
-    launch_batch_geometry(s, ncells, cell_h, cell_pbc, model.rc, d_cell_hinv.p, d_cell_reach.p,
+    launch_batch_geometry(s, ncells, cell_h, cell_pbc, list_cutoff, d_cell_hinv.p, d_cell_reach.p,
                           reinterpret_cast<double(*)[3]>(d_cell_shift.p), &d_status.p->thin_cell);
     launch_batch_pack(s, N, ncells, off, x, type, cell_h, d_cell_hinv.p, cell_pbc, model.species_count,
                       d_batch_cell.p, pos4.p, d_status.p);
     launches += 2;
-    const double cutoff2 = model.rc * model.rc;
+    const double cutoff2 = list_cutoff * list_cutoff;
     if (cap == 0) {
       ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
       launch_batch_fill(s, N, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nullptr, ncount.p, 0, 1,
@@ -587,7 +622,7 @@ struct Engine {
     bool box_changed = false;
     for (int k = 0; k < 9; ++k) box_changed |= h[k] != last_h[k];
     for (int k = 0; k < 3; ++k) box_changed |= (pbc[k] ? 1 : 0) != last_pbc[k];
-    const double cutoff = model.rc + opt.skin;
+    const double cutoff = list_cutoff + opt.skin;
     if (box_changed) {
       ncells = make_geometry(h, pbc, cutoff, N, geom);
       std::memcpy(last_h, h, sizeof(last_h));
@@ -640,11 +675,68 @@ struct Engine {
     nbr.resize(static_cast<size_t>(cap) * N);
   }
 
+  ZblTables zbl_tables() const {
+    ZblTables z{};
+    z.species = model.species_count;
+    z.z = d_zbl_z.p;
+    z.inner = d_zbl_in.p;
+    z.outer = d_zbl_out.p;
+    return z;
+  }
+
+  // Tile autotuner: times every supported CTA size of k_basic and k_force on
+  // the live neighbour list (scratch outputs, so the caller's arrays are not
+  // touched) and keeps the fastest.  Runs once per handle, at the first
+  // evaluation, where the neighbour-list sizing already synchronises.
+  template <typename T>
+  void autotune(cudaStream_t s, const EdgeArgs<T>& a) {
+    tuned = true;
+    if (!opt.autotune || sizeof(T) != 4) return;
+    DevBuf<double> f_scratch, w_scratch;
+    f_scratch.resize(3ull * N);
+    w_scratch.resize(9ull * N);
+    ck(cudaMemsetAsync(Gbuf.p, 0, Gbuf.n, s), "memset");
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "cudaEventCreate");
+    ck(cudaEventCreate(&e1), "cudaEventCreate");
+    auto time_it = [&](auto&& launch) {
+      launch();  // warm
+      ck(cudaEventRecord(e0, s), "cudaEventRecord");
+      launch();
+      ck(cudaEventRecord(e1, s), "cudaEventRecord");
+      ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      float ms = 0.0f;
+      ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+      return ms;
+    };
+    float best_b = 1e30f, best_f = 1e30f;
+    for (int block : {64, 128, 256}) {
+      const float tb = time_it([&] { launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block); });
+      const float tf = time_it([&] {
+        launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), nullptr, ftmp.p, f_scratch.p, w_scratch.p, 1.0,
+                        block);
+      });
+      launches += 4;
+      if (tb < best_b) {
+        best_b = tb;
+        basic_block = block;
+      }
+      if (tf < best_f) {
+        best_f = tf;
+        force_block = block;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ck(cudaGetLastError(), "autotune");
+  }
+
   template <typename T>
   void forward_impl(cudaStream_t s, double* pe, int pe_assign, EvSet* ev = nullptr) {
     const EdgeArgs<T> a = edge_args<T>();
+    if (!tuned) autotune<T>(s, a);
     mark(ev, 1, s);
-    if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p)) != 0)
+    if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), basic_block) != 0)
       throw InputError("SUS2_SH basic kernel shape not compiled.");
     mark(ev, 2, s);
     if (!cg_bin.cubin.empty()) {
@@ -659,6 +751,11 @@ struct Engine {
                         d_shift.p, d_species.p, pe, pe_assign);
     }
     launches += 2;
+    if (model.zbl_enabled && pe) {
+      launch_zbl(s, 0, N, cap, pos4.p, nbr.p, ncount.p, a.shift, a.atom_cell, zbl_tables(), nullptr, pe, nullptr,
+                 nullptr, 1.0);
+      launches += 1;
+    }
   }
 
   template <typename T>
@@ -667,8 +764,14 @@ struct Engine {
     const EdgeArgs<T> a = edge_args<T>();
     ck(cudaMemsetAsync(ftmp.p, 0, ftmp.n, s), "memset");
     mark(ev, 3, s);
-    if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign) != 0)
+    if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign,
+                        force_block) != 0)
       throw InputError("SUS2_SH force kernel shape not compiled.");
+    if (model.zbl_enabled) {
+      launch_zbl(s, 1, N, cap, pos4.p, nbr.p, ncount.p, a.shift, a.atom_cell, zbl_tables(), weight, nullptr, force,
+                 virial, sign);
+      launches += 1;
+    }
     mark(ev, 4, s);
     launch_finalize<T>(s, N, ftmp.p, force, sign);
     mark(ev, 5, s);
@@ -986,15 +1089,16 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[24] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[26] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
                      e.prog.nvalue, e.prog.nrows, e.model.standard_graph_matched ? 1 : 0,
                      e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0,
                      static_cast<int>(e.launches & 0x7fffffff), e.rs.shared_xi, e.prod_global ? 1 : 0,
-                     e.cg_bin.cubin.empty() ? 0 : 1, e.cg_bin.registers, static_cast<int>(e.cg_compile_ms)};
-  const int k = std::min(n, 24);
+                     e.cg_bin.cubin.empty() ? 0 : 1, e.cg_bin.registers, static_cast<int>(e.cg_compile_ms),
+                     e.basic_block, e.force_block};
+  const int k = std::min(n, 26);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -1117,6 +1221,14 @@ int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text
       text[k] = 0;
     }
   });
+}
+
+int sus2sh_zbl_pair(int zi, int zj, double r, double inner, double outer, double* energy, double* dEdr) {
+  if (!energy || !dEdr) return SUS2SH_E_ARG;
+  const sus2sh::zbl::PairValue v = sus2sh::zbl::pair(zi, zj, r, inner, outer);
+  *energy = v.energy;
+  *dEdr = v.dEdr;
+  return SUS2SH_OK;
 }
 
 int sus2sh_measure_fma_peak(int fp64, double* tflops) {

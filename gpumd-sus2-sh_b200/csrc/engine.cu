@@ -18,6 +18,7 @@
 #include "edge_common.cuh"
 #include "engine.cuh"
 #include "sh_math.cuh"
+#include "zbl.cuh"
 
 #include <cstdio>
 
@@ -25,7 +26,6 @@ namespace sus2sh {
 namespace {
 using namespace edge;
 
-constexpr int kEdgeBlock = 128;
 // Minimum resident CTAs per SM of the FP32 edge kernels (register caps).
 // Measured on the 1.024M-atom l3k3 workload: k_force at 4 CTAs (128 registers,
 // 8 B spill) runs 1.55 ms vs 1.87 ms at its natural 167 registers; capping
@@ -241,8 +241,8 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
 // ---------------------------------------------------------------------------
 // basic moments
 // ---------------------------------------------------------------------------
-template <typename T, int L, int K, int RB>
-__global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_BASIC_MIN_BLOCKS : 1) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
+template <typename T, int L, int K, int RB, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK : 1) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_tab = reinterpret_cast<T*>(smem_raw);
   load_pair_table(a, s_tab);
@@ -309,8 +309,8 @@ struct Scatter<double> {
   }
 };
 
-template <typename T, int L, int K, int RB>
-__global__ void __launch_bounds__(kEdgeBlock, sizeof(T) == 4 ? SUS2_FORCE_MIN_BLOCKS : 1)
+template <typename T, int L, int K, int RB, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK : 1)
     k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
             void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
             double sign) {
@@ -508,6 +508,66 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---------------------------------------------------------------------------
+// ZBL pair term (gpu_sh_apply_zbl, src/force/sus2_sh.cu:7522-7627): half of
+// each pair energy on each end of the full list, FP64 throughout.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    k_zbl(int mode, int N, int cap, const double4* __restrict__ pos4, const int* __restrict__ nbr,
+          const int* __restrict__ ncount, const double (*__restrict__ shift)[3], const int* __restrict__ atom_cell,
+          const ZblTables z, const double* __restrict__ weight, double* __restrict__ pe, double* __restrict__ force,
+          double* __restrict__ virial, double sign) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double4 pi = pos4[i];
+  const double(*cell_shift)[3] = shift + (atom_cell ? 125 * atom_cell[i] : 0);
+  const int ti = type_of(pi);
+  const int zi = z.z[ti];
+  const int cnt = min(ncount[i], cap);
+  const double wi = weight ? weight[i] : 1.0;
+  double e = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+  double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int n = 0; n < cnt; ++n) {
+    const int word = __ldg(nbr + static_cast<size_t>(n) * N + i);
+    const int j = word & 0xFFFFFF;
+    const double4 pj = pos4[j];
+    double sx, sy, sz;
+    image_shift(cell_shift, static_cast<unsigned>(word) >> 24, sx, sy, sz);
+    const double dx = pj.x - pi.x + sx, dy = pj.y - pi.y + sy, dz = pj.z - pi.z + sz;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const int pair = ti * z.species + type_of(pj);
+    const double outer = z.outer[pair];
+    if (r2 <= 0.0 || r2 >= outer * outer) continue;
+    const double r = sqrt(r2);
+    const zbl::PairValue v = zbl::pair(zi, z.z[type_of(pj)], r, z.inner[pair], outer);
+    if (v.energy == 0.0 && v.dEdr == 0.0) continue;
+    if (mode == 0) {
+      e += 0.5 * v.energy;
+      continue;
+    }
+    const double sc = 0.5 * v.dEdr / r * wi;
+    const double ex = sc * dx, ey = sc * dy, ez = sc * dz;
+    fx += ex;
+    fy += ey;
+    fz += ez;
+    atomicAdd(force + j, -sign * ex);
+    atomicAdd(force + j + N, -sign * ey);
+    atomicAdd(force + j + 2 * N, -sign * ez);
+    w[0] -= dx * ex; w[1] -= dy * ey; w[2] -= dz * ez;
+    w[3] -= dx * ey; w[4] -= dx * ez; w[5] -= dy * ez;
+    w[6] -= dy * ex; w[7] -= dz * ex; w[8] -= dz * ey;
+  }
+  if (mode == 0) {
+    pe[i] += e;
+    return;
+  }
+  atomicAdd(force + i, sign * fx);
+  atomicAdd(force + i + N, sign * fy);
+  atomicAdd(force + i + 2 * N, sign * fz);
+  if (virial)
+    for (int q = 0; q < 9; ++q) virial[static_cast<size_t>(q) * N + i] += w[q];
+}
+
+// ---------------------------------------------------------------------------
 // MD integrator (velocity Verlet); units A, fs, amu, eV.
 // ---------------------------------------------------------------------------
 constexpr double kAccel = 9.648533212331002e-3;  // (eV/A/amu) -> A/fs^2
@@ -669,15 +729,41 @@ static size_t pair_smem(const EdgeArgs<T>& a) {
   return sizeof(T) * static_cast<size_t>(a.rs.species) * a.rs.species * a.rs.pair_stride;
 }
 
-template <typename T>
-int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B) {
+// CTA sizes the tile autotuner may choose for the FP32 edge kernels (the FP64
+// engine always uses 128).
+bool block_supported(int block, bool fp32) { return block == 128 || (fp32 && (block == 64 || block == 256)); }
+
+template <typename T, int L, int K, int RB>
+int launch_basic_shape(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
   const size_t sm = pair_smem(a);
-  const int grid = blocks_for(a.N, kEdgeBlock);
-#define SUS2_BASIC(L, K, RB)                                                 \
-  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) {                       \
-    k_basic<T, L, K, RB><<<grid, kEdgeBlock, sm, s>>>(a, B);                 \
-    return 0;                                                                \
+  if (sizeof(T) == 4 && block == 64) {
+    k_basic<T, L, K, RB, 64><<<blocks_for(a.N, 64), 64, sm, s>>>(a, B);
+  } else if (sizeof(T) == 4 && block == 256) {
+    k_basic<T, L, K, RB, 256><<<blocks_for(a.N, 256), 256, sm, s>>>(a, B);
+  } else {
+    k_basic<T, L, K, RB, 128><<<blocks_for(a.N, 128), 128, sm, s>>>(a, B);
   }
+  return 0;
+}
+
+template <typename T, int L, int K, int RB>
+int launch_force_shape(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight, void* ftmp,
+                       double* force, double* virial, double sign, int block) {
+  const size_t sm = pair_smem(a);
+  if (sizeof(T) == 4 && block == 64) {
+    k_force<T, L, K, RB, 64><<<blocks_for(a.N, 64), 64, sm, s>>>(a, G, weight, ftmp, force, virial, sign);
+  } else if (sizeof(T) == 4 && block == 256) {
+    k_force<T, L, K, RB, 256><<<blocks_for(a.N, 256), 256, sm, s>>>(a, G, weight, ftmp, force, virial, sign);
+  } else {
+    k_force<T, L, K, RB, 128><<<blocks_for(a.N, 128), 128, sm, s>>>(a, G, weight, ftmp, force, virial, sign);
+  }
+  return 0;
+}
+
+template <typename T>
+int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
+#define SUS2_BASIC(L, K, RB) \
+  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) return launch_basic_shape<T, L, K, RB>(s, a, B, block);
   SUS2_SHAPES(SUS2_BASIC)
 #undef SUS2_BASIC
   return -1;
@@ -685,14 +771,10 @@ int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B) {
 
 template <typename T>
 int launch_force(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight, void* ftmp,
-                 double* force, double* virial, double sign) {
-  const size_t sm = pair_smem(a);
-  const int grid = blocks_for(a.N, kEdgeBlock);
-#define SUS2_FORCE(L, K, RB)                                                          \
-  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) {                                \
-    k_force<T, L, K, RB><<<grid, kEdgeBlock, sm, s>>>(a, G, weight, ftmp, force, virial, sign); \
-    return 0;                                                                         \
-  }
+                 double* force, double* virial, double sign, int block) {
+#define SUS2_FORCE(L, K, RB)                                                                         \
+  if (a.l_max == L && a.k_max == K && a.rs.rb == RB)                                                 \
+    return launch_force_shape<T, L, K, RB>(s, a, G, weight, ftmp, force, virial, sign, block);
   SUS2_SHAPES(SUS2_FORCE)
 #undef SUS2_FORCE
   return -1;
@@ -727,17 +809,24 @@ void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_m
   k_kick_drift<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel, pos, pe, vir);
 }
 
+void launch_zbl(cudaStream_t s, int mode, int N, int cap, const double4* pos4, const int* nbr, const int* ncount,
+                const double (*shift)[3], const int* atom_cell, const ZblTables& z, const double* weight,
+                double* pe, double* force, double* virial, double sign) {
+  k_zbl<<<blocks_for(N, 128), 128, 0, s>>>(mode, N, cap, pos4, nbr, ncount, shift, atom_cell, z, weight, pe, force,
+                                           virial, sign);
+}
+
 void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_type, const int* type,
                      const double* force, double* vel) {
   k_kick<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel);
 }
 
-template int launch_basic<float>(cudaStream_t, const EdgeArgs<float>&, float*);
-template int launch_basic<double>(cudaStream_t, const EdgeArgs<double>&, double*);
+template int launch_basic<float>(cudaStream_t, const EdgeArgs<float>&, float*, int);
+template int launch_basic<double>(cudaStream_t, const EdgeArgs<double>&, double*, int);
 template int launch_force<float>(cudaStream_t, const EdgeArgs<float>&, const float*, const double*, void*,
-                                 double*, double*, double);
+                                 double*, double*, double, int);
 template int launch_force<double>(cudaStream_t, const EdgeArgs<double>&, const double*, const double*, void*,
-                                  double*, double*, double);
+                                  double*, double*, double, int);
 template void launch_product<float>(cudaStream_t, int, const ProgramDev&, const double4*, const float*, float*,
                                     float*, size_t, int, const double*, const double*, double*, int);
 template void launch_product<double>(cudaStream_t, int, const ProgramDev&, const double4*, const double*,

@@ -117,11 +117,13 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
                   int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
                   int cap, int count_only, Status* st);
 
+// Edge kernels with CTA size `block` (64, 128 or 256 for FP32; 128 for FP64).
 template <typename T>
-int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B);
+int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block);
 template <typename T>
 int launch_force(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight,
-                 void* ftmp, double* force, double* virial, double sign);
+                 void* ftmp, double* force, double* virial, double sign, int block);
+bool block_supported(int block, bool fp32);
 // Sums per-atom energy and virial into out[0] and out[1..9] (FP64 atomics).
 void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial, double* out);
 template <typename T>
@@ -144,6 +146,19 @@ void launch_batch_fill(cudaStream_t s, int N, const int* off, const int* atom_ce
                        int cap, int count_only, Status* st);
 void launch_cell_reduce(cudaStream_t s, int ncells, int N, const int* off, const double* pe, const double* virial,
                         double* cell_energy, double* cell_virial);
+
+// ZBL pair term over the neighbour list (FP64).  mode 0: pe[i] += E_i;
+// mode 1: weighted forces (force[i] += sign w_i sum dE, force[j] -= sign w_i dE
+// by FP64 atomics) and, if virial != NULL, virial[i] -= w_i r_ij (x) dE.
+struct ZblTables {
+  int species;
+  const int* z;         // [S] atomic numbers
+  const double* inner;  // [S*S]
+  const double* outer;  // [S*S]
+};
+void launch_zbl(cudaStream_t s, int mode, int N, int cap, const double4* pos4, const int* nbr, const int* ncount,
+                const double (*shift)[3], const int* atom_cell, const ZblTables& z, const double* weight,
+                double* pe, double* force, double* virial, double sign);
 
 // Integrator kernels for the benchmark MD driver.
 void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_mass_type,

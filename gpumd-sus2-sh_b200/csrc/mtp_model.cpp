@@ -180,8 +180,18 @@ HostModel load_model(const std::string& path) {
                      ". Supported: RBChebyshev_sss[_lmp], RBChebyshev_sss_rational[_lmp].");
   }
   m.rc = double_of(text, "max_dist =");
-  if (contains(text, "zbl_enabled =") && parse_bool(value_of(text, "zbl_enabled ="), "zbl_enabled"))
-    throw InputError("SUS2_SH ZBL models are not supported by this engine yet.");
+  m.zbl_enabled = contains(text, "zbl_enabled =") && parse_bool(value_of(text, "zbl_enabled ="), "zbl_enabled =");
+  if (m.zbl_enabled) {
+    if (contains(text, "zbl_inner =")) m.zbl_inner = double_of(text, "zbl_inner =");
+    if (contains(text, "zbl_outer =")) m.zbl_outer = double_of(text, "zbl_outer =");
+    m.zbl_typewise = contains(text, "zbl_typewise_cutoff_enabled =")
+                         ? parse_bool(value_of(text, "zbl_typewise_cutoff_enabled ="), "zbl_typewise_cutoff_enabled =")
+                         : contains(text, "zbl_typewise_cutoff_factor =");
+    if (contains(text, "zbl_typewise_cutoff_factor ="))
+      m.zbl_typewise_factor = double_of(text, "zbl_typewise_cutoff_factor =");
+    if (contains(text, "zbl_atomic_numbers ="))
+      m.zbl_atomic_numbers = numbers<int>(braced(text, "zbl_atomic_numbers ="));
+  }
   m.rb_size = int_of(text, "radial_basis_size =");
   m.radial_funcs = int_of(text, "radial_funcs_count =");
   m.moments = int_of(text, "alpha_moments_count =");
@@ -755,6 +765,8 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       o.rebuild_interval = std::atoi(val.c_str());
     } else if (key == "sus2_sh_profile" || key == "sus2_profile") {
       o.profile = parse_bool(val, key);
+    } else if (key == "sus2_sh_autotune") {
+      o.autotune = parse_bool(val, key);
     } else if (key == "sus2_sh_cg_jit") {
       o.cg_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_reference_rounding") {

@@ -53,6 +53,13 @@ struct HostModel {
   std::vector<double> radial_coeffs;    // [Kmu][rb]
   std::vector<double> radial_type_coeffs;  // [S]
   bool standard_graph_matched = false;
+  // ZBL short-range term (load_sh_model, sus2_sh.cu:2132-2147)
+  bool zbl_enabled = false;
+  double zbl_inner = 0.7;
+  double zbl_outer = 1.4;
+  bool zbl_typewise = false;
+  double zbl_typewise_factor = 0.7;
+  std::vector<int> zbl_atomic_numbers;  // empty: from the element symbols
 };
 
 // Parses a SUS2-SH v1.1.0 .mtp file with the reference reader's semantics.
@@ -102,6 +109,7 @@ struct Options {
   bool reference_rounding = false;  // sus2_sh_reference_rounding=
   bool profile = false;             // sus2_sh_profile / sus2_profile / SUS2_SH_GPUMD_PROFILE
   bool cg_jit = true;               // sus2_sh_cg_jit=0 runs the CG row interpreter instead
+  bool autotune = true;             // sus2_sh_autotune=0 keeps 128-thread edge-kernel CTAs
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

@@ -49,3 +49,27 @@ def preset_model(name: str, directory: str) -> str:
         write_model(path + ".tmp", **PRESETS[name])
         os.replace(path + ".tmp", path)
     return path
+
+
+def add_zbl(src: str, dst: str, atomic_numbers=None, inner=None, outer=None, typewise=None, factor=None,
+            enabled: str = "1") -> str:
+    """Copies model ``src`` to ``dst`` with ZBL metadata appended (the keys
+    load_sh_model reads, src/force/sus2_sh.cu:2132-2147); None leaves a key
+    out so the reader's default applies."""
+    with open(src) as fh:
+        text = fh.read()
+    lines = [f"zbl_enabled = {enabled}"]
+    if inner is not None:
+        lines.append(f"zbl_inner = {inner!r}")
+    if outer is not None:
+        lines.append(f"zbl_outer = {outer!r}")
+    if typewise is not None:
+        lines.append(f"zbl_typewise_cutoff_enabled = {1 if typewise else 0}")
+    if factor is not None:
+        lines.append(f"zbl_typewise_cutoff_factor = {factor!r}")
+    if atomic_numbers is not None:
+        lines.append("zbl_atomic_numbers = {" + ", ".join(str(int(z)) for z in atomic_numbers) + "}")
+    with open(dst + ".tmp", "w") as fh:
+        fh.write(text.rstrip("\n") + "\n" + "\n".join(lines) + "\n")
+    os.replace(dst + ".tmp", dst)
+    return dst

@@ -178,7 +178,10 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * [17] neighbour builds so far (valid after sus2sh_sync) [18] kernels
  * launched by this handle [19] shared radial argument [20] product slots in
  * HBM [21] model-specialised CG kernel in use [22] its registers per thread
- * [23] its NVRTC compile time (ms).  Returns the number written. */
+ * [23] its NVRTC compile time (ms) [24] CTA size of the basic-moment kernel
+ * [25] CTA size of the force kernel (both picked by the tile autotuner at the
+ * first evaluation; option sus2_sh_autotune=0 keeps 128).  Returns the number
+ * written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

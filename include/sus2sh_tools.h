@@ -51,6 +51,11 @@ int sus2sh_reduce(int N, const double* potential, const double* virial, double* 
  * above the straight-line limit (12000 products) return SUS2SH_E_INPUT. */
 int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text, size_t text_size);
 
+/* The engine's ZBL pair function (energy and dE/dr at distance r for atomic
+ * numbers zi, zj and the pair's inner/outer cutoffs), for checks against the
+ * reference's sus2_zbl_pair. */
+int sus2sh_zbl_pair(int zi, int zj, double r, double inner, double outer, double* energy, double* dEdr);
+
 /* FMA-chain microbenchmark of the current device: measured FP32 (fp64 = 0)
  * or FP64 (fp64 = 1) CUDA-core throughput in TFLOP/s (2 flops per FMA).  It is
  * the roofline denominator of the SIMT kernels. */

@@ -553,11 +553,18 @@ class MtpModel:
     products: list           # [(l, r, t, c)]
     radial_coeffs: list      # [Kmu * rb]
     radial_type_coeffs: list # [S]
+    # ZBL short-range term (load_sh_model, sus2_sh.cu:2132-2147)
+    zbl_enabled: bool = False
+    zbl_inner: float = 0.7
+    zbl_outer: float = 1.4
+    zbl_typewise: bool = False
+    zbl_typewise_factor: float = 0.7
+    zbl_atomic_numbers: list = None
 
 
 def load_mtp(path: str) -> MtpModel:
-    """Restates load_sh_model (sus2_sh.cu:2105-2482) for the non-gate, non-ZBL
-    models the engine targets.  ``RBChebyshev_sss_rational`` is accepted as the
+    """Restates load_sh_model (sus2_sh.cu:2105-2482) for the non-gate models
+    the engine targets, ZBL metadata included (:2132-2147).  ``RBChebyshev_sss_rational`` is accepted as the
     rational map the reference documents (README.md:45,55-56)."""
     with open(path) as fh:
         text = fh.read()
@@ -664,8 +671,32 @@ def load_mtp(path: str) -> MtpModel:
         explicit_metadata(M, Bb, prods, mapping)
     except ValueError as exc:
         raise MtpError(str(exc)) from exc
-    return MtpModel(S, L, K, body, rtype, rational, max_dist, rb, kmu, M, Bb, nsc, scaling,
-                    blmax, shift, scal, species, moment, mapping, basic, prods, radial, rtc)
+    model = MtpModel(S, L, K, body, rtype, rational, max_dist, rb, kmu, M, Bb, nsc, scaling,
+                     blmax, shift, scal, species, moment, mapping, basic, prods, radial, rtc)
+    if "zbl_enabled =" in text and _bool(_after(text, "zbl_enabled =")):
+        model.zbl_enabled = True
+        if "zbl_inner =" in text:
+            model.zbl_inner = float(_after(text, "zbl_inner ="))
+        if "zbl_outer =" in text:
+            model.zbl_outer = float(_after(text, "zbl_outer ="))
+        if "zbl_typewise_cutoff_enabled =" in text:
+            model.zbl_typewise = _bool(_after(text, "zbl_typewise_cutoff_enabled ="))
+        else:
+            model.zbl_typewise = "zbl_typewise_cutoff_factor =" in text
+        if "zbl_typewise_cutoff_factor =" in text:
+            model.zbl_typewise_factor = float(_after(text, "zbl_typewise_cutoff_factor ="))
+        if "zbl_atomic_numbers =" in text:
+            model.zbl_atomic_numbers = _numbers(_braced(text, "zbl_atomic_numbers ="), int)
+    return model
+
+
+def _bool(token: str) -> bool:
+    """parse_optional_bool_after (sus2_sh.cu:343-361): exact tokens."""
+    if token in ("1", "true", "TRUE", "yes", "on"):
+        return True
+    if token in ("0", "false", "FALSE", "no", "off"):
+        return False
+    raise MtpError("Invalid boolean token in SUS2-SH model file: " + token)
 
 
 def standard_graph_matches(model: MtpModel, graph: StandardGraph) -> bool:

@@ -548,3 +548,156 @@ int oracle_cg_energy(const OracleModel* m, int N, const int* type, const double*
   }
   return fail ? -1 : 0;
 }
+
+/* ---- ZBL short-range term ------------------------------------------------
+ * Restates src/force/sus2_zbl_common.cuh:18-225 (pair function, covalent
+ * radii, pair cutoff tables) and gpu_sh_apply_zbl (sus2_sh.cu:7522-7627):
+ * every listed pair with r < outer(ti,tj) puts E/2 on atom i, dE = E'/2 d/r,
+ * F_i += dE, F_j -= dE, W_i -= d (x) dE.  Outputs are accumulated (+=) onto
+ * the SUS2 outputs of oracle_efs.  Test infrastructure only.               */
+
+static const double kOracleCovalent[94] = {
+    0.426667, 0.613333, 1.6,      1.25333,  1.02667,  1.0,      0.946667, 0.84,     0.853333, 0.893333,
+    1.86667,  1.66667,  1.50667,  1.38667,  1.46667,  1.36,     1.32,     1.28,     2.34667,  2.05333,
+    1.77333,  1.62667,  1.61333,  1.46667,  1.42667,  1.38667,  1.33333,  1.32,     1.34667,  1.45333,
+    1.49333,  1.45333,  1.53333,  1.46667,  1.52,     1.56,     2.52,     2.22667,  1.96,     1.85333,
+    1.76,     1.65333,  1.53333,  1.50667,  1.50667,  1.44,     1.53333,  1.64,     1.70667,  1.68,
+    1.68,     1.64,     1.76,     1.74667,  2.78667,  2.34667,  2.16,     1.96,     2.10667,  2.09333,
+    2.08,     2.06667,  2.01333,  2.02667,  2.01333,  2.0,      1.98667,  1.98667,  1.97333,  2.04,
+    1.94667,  1.82667,  1.74667,  1.64,     1.57333,  1.54667,  1.48,     1.49333,  1.50667,  1.76,
+    1.73333,  1.73333,  1.81333,  1.74667,  1.84,     1.89333,  2.68,     2.41333,  2.22667,  2.10667,
+    2.02667,  2.04,     2.05333,  2.06667};
+
+double oracle_zbl_covalent_radius(int z) { return (z >= 1 && z <= 94) ? kOracleCovalent[z - 1] : 0.0; }
+
+/* Energy and dE/dr of one pair (screened Coulomb, four-exponential universal
+ * screening, cosine switch between inner and outer). */
+void oracle_zbl_pair(int zi, int zj, double r, double inner, double outer, double* e, double* de) {
+  *e = 0.0;
+  *de = 0.0;
+  if (zi <= 0 || zj <= 0 || r <= 0.0 || outer <= 0.0 || r >= outer) return;
+  static const double amp[4] = {0.18175, 0.50986, 0.28022, 0.02817};
+  static const double rate[4] = {3.1998, 0.94229, 0.4029, 0.20162};
+  const double ainv = 2.134563 * (pow((double)zi, 0.23) + pow((double)zj, 0.23));
+  const double x = ainv * r;
+  double phi = 0.0, dphi = 0.0;
+  for (int q = 0; q < 4; ++q) {
+    const double ex = exp(-rate[q] * x);
+    phi += amp[q] * ex;
+    dphi -= amp[q] * rate[q] * ainv * ex;
+  }
+  const double k = 14.3996454784255 * (double)zi * (double)zj;
+  const double e0 = k * phi / r, de0 = k * (dphi / r - phi / (r * r));
+  double s = 1.0, ds = 0.0;
+  if (r > inner) {
+    const double w = 3.141592653589793238462643383279502884 / (outer - inner);
+    s = 0.5 * cos(w * (r - inner)) + 0.5;
+    ds = -0.5 * w * sin(w * (r - inner));
+  }
+  *e = s * e0;
+  *de = s * de0 + ds * e0;
+}
+
+/* Per species pair cutoffs [S*S]; 0 on success, else a code naming the
+ * failed check (1 no species, 2 inner < 0, 3 outer <= 0, 4 factor < 0.5,
+ * 5 outer <= inner, 6 atomic number out of range, 7 pair inner >= outer). */
+int oracle_zbl_tables(int S, const int* z, double inner, double outer, int typewise, double factor, double* pin,
+                      double* pout) {
+  if (S <= 0) return 1;
+  if (inner < 0.0) return 2;
+  if (outer <= 0.0) return 3;
+  if (typewise) {
+    if (factor < 0.5) return 4;
+  } else if (outer <= inner) {
+    return 5;
+  }
+  for (int a = 0; a < S; ++a)
+    for (int b = 0; b < S; ++b) {
+      const double ra = oracle_zbl_covalent_radius(z[a]), rb = oracle_zbl_covalent_radius(z[b]);
+      if (z[a] <= 0 || z[b] <= 0 || (typewise && (ra <= 0.0 || rb <= 0.0))) return 6;
+      double lo = inner, hi = outer;
+      if (typewise) {
+        lo = 0.0;
+        hi = factor * (ra + rb);
+        if (hi > outer) hi = outer;
+      }
+      if (hi <= lo) return 7;
+      pin[a * S + b] = lo;
+      pout[a * S + b] = hi;
+    }
+  return 0;
+}
+
+int oracle_zbl_efs(int S, const int* z, const double* pin, const double* pout, int N, const double* h,
+                   const int* pbc, const int* type, const double* pos, double* pe, double* f, double* vir,
+                   int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int nt = omp_get_max_threads();
+#else
+  (void)nthreads;
+  const int nt = 1;
+#endif
+  double rmax = 0.0;
+  for (int p = 0; p < S * S; ++p)
+    if (pout[p] > rmax) rmax = pout[p];
+  if (rmax <= 0.0) return -1;
+  Geo g;
+  geo_init(&g, h, pbc, rmax);
+  NList nl;
+  if (build_nlist(&g, N, pos, rmax, &nl) != 0) return -1;
+  double* fbuf = (double*)calloc((size_t)nt * 3 * N, sizeof(double));
+  if (!fbuf) return -1;
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    double* fl = fbuf + (size_t)omp_get_thread_num() * 3 * N;
+#else
+    double* fl = fbuf;
+#endif
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < N; ++i) {
+      const int ti = type[i];
+      double e = 0.0, w9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int q = nl.start[i]; q < nl.start[i + 1]; ++q) {
+        const Edge* ed = nl.e + q;
+        const int p = ti * S + type[ed->j];
+        const double dx = ed->d[0], dy = ed->d[1], dz = ed->d[2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= 0.0 || r2 >= pout[p] * pout[p]) continue;
+        const double r = sqrt(r2);
+        double v, dv;
+        oracle_zbl_pair(z[ti], z[type[ed->j]], r, pin[p], pout[p], &v, &dv);
+        e += 0.5 * v;
+        const double c = 0.5 * dv / r;
+        const double ex = c * dx, ey = c * dy, ez = c * dz;
+        fl[i] += ex;
+        fl[i + N] += ey;
+        fl[i + 2 * N] += ez;
+        fl[ed->j] -= ex;
+        fl[ed->j + N] -= ey;
+        fl[ed->j + 2 * N] -= ez;
+        w9[0] -= dx * ex;
+        w9[1] -= dy * ey;
+        w9[2] -= dz * ez;
+        w9[3] -= dx * ey;
+        w9[4] -= dx * ez;
+        w9[5] -= dy * ez;
+        w9[6] -= dy * ex;
+        w9[7] -= dz * ex;
+        w9[8] -= dz * ey;
+      }
+      pe[i] += e;
+      for (int k = 0; k < 9; ++k) vir[(size_t)k * N + i] += w9[k];
+    }
+  }
+  for (int a = 0; a < 3 * N; ++a) {
+    double s = 0.0;
+    for (int t = 0; t < nt; ++t) s += fbuf[(size_t)t * 3 * N + a];
+    f[a] += s;
+  }
+  free(fbuf);
+  free(nl.start);
+  free(nl.e);
+  return 0;
+}

@@ -104,10 +104,58 @@ class OracleArrays:
                              ptr(self.shift_e), ptr(self.species))
 
 
-class Oracle:
-    """FP64 energy/force/virial of one model (C oracle, OpenMP)."""
+_ELEMENTS = ("H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se "
+             "Br Kr Rb Sr Y Zr Nb Mo Tc Ru Rh Pd Ag Cd In Sn Sb Te I Xe Cs Ba La Ce Pr Nd Pm Sm Eu Gd Tb "
+             "Dy Ho Er Tm Yb Lu Hf Ta W Re Os Ir Pt Au Hg Tl Pb Bi Po At Rn Fr Ra Ac Th Pa U Np Pu").split()
 
-    def __init__(self, model_or_path, reference_rounding: bool = False):
+_ZBL_TABLE_ERRORS = {
+    1: "ZBL requires one atomic number per model species.",
+    2: "ZBL inner cutoff should be non-negative.",
+    3: "ZBL outer cutoff should be positive.",
+    4: "ZBL typewise cutoff factor should be at least 0.5.",
+    5: "ZBL cutoffs should satisfy 0 <= inner < outer.",
+    6: "ZBL atomic numbers should be in [1, 94].",
+    7: "ZBL pair cutoffs should satisfy inner < outer.",
+}
+
+
+def atomic_number(symbol: str) -> int:
+    """sus2_zbl_atomic_number_from_symbol (sus2_zbl_common.cuh:54-71); 0 if unknown."""
+    return _ELEMENTS.index(symbol) + 1 if symbol in _ELEMENTS else 0
+
+
+def zbl_tables(z, inner: float, outer: float, typewise: bool, factor: float):
+    """Pair inner/outer cutoffs [S*S] (sus2_zbl_fill_pair_cutoff_tables,
+    sus2_zbl_common.cuh:89-169) through the C restatement; ValueError with the
+    reference's message on a failed check."""
+    lib = ctypes.CDLL(build_oracle())
+    S = len(z)
+    za = np.ascontiguousarray(np.asarray(z, dtype=np.int32))
+    pin = np.zeros(max(S * S, 1))
+    pout = np.zeros(max(S * S, 1))
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = lib.oracle_zbl_tables(S, ptr(za), ctypes.c_double(inner), ctypes.c_double(outer), int(typewise),
+                               ctypes.c_double(factor), ptr(pin), ptr(pout))
+    if rc != 0:
+        raise ValueError(_ZBL_TABLE_ERRORS[rc])
+    return pin[:S * S], pout[:S * S]
+
+
+def zbl_pair(zi: int, zj: int, r: float, inner: float, outer: float):
+    """Energy and dE/dr of one ZBL pair (C restatement)."""
+    lib = ctypes.CDLL(build_oracle())
+    e, de = ctypes.c_double(), ctypes.c_double()
+    lib.oracle_zbl_pair(zi, zj, ctypes.c_double(r), ctypes.c_double(inner), ctypes.c_double(outer),
+                        ctypes.byref(e), ctypes.byref(de))
+    return e.value, de.value
+
+
+class Oracle:
+    """FP64 energy/force/virial of one model (C oracle, OpenMP).  ZBL models
+    take their atomic numbers from ``zbl_atomic_numbers`` or, as the
+    reference's constructor does (sus2_sh.cu:7824-7860), from ``symbols``."""
+
+    def __init__(self, model_or_path, reference_rounding: bool = False, symbols=None):
         m = load_mtp(model_or_path) if isinstance(model_or_path, str) else model_or_path
         self.model = m
         self.arrays = OracleArrays.from_model(m, reference_rounding)
@@ -116,6 +164,21 @@ class Oracle:
         self.lib.oracle_efs.restype = ctypes.c_int
         self.lib.oracle_basics.restype = ctypes.c_int
         self.lib.oracle_neighbor_counts.restype = ctypes.c_int
+        self.zbl = None
+        if m.zbl_enabled:
+            z = m.zbl_atomic_numbers
+            if not z:
+                if symbols is None or len(symbols) < m.species_count:
+                    raise ValueError("SUS2_SH ZBL model requires zbl_atomic_numbers metadata or element "
+                                     "symbols after the model file.")
+                z = [atomic_number(sym) for sym in symbols[:m.species_count]]
+                if min(z) <= 0:
+                    raise ValueError("SUS2_SH ZBL cannot map element symbol to an atomic number")
+            if len(z) != m.species_count:
+                raise ValueError("SUS2_SH ZBL metadata should provide one atomic number per species.")
+            pin, pout = zbl_tables(z, m.zbl_inner, m.zbl_outer, m.zbl_typewise,
+                                   m.zbl_typewise_factor if m.zbl_typewise else 0.0)
+            self.zbl = (np.asarray(z, dtype=np.int32), pin, pout)
 
     def efs(self, h, pbc, types, pos, nthreads: int = 0):
         """Per-atom energy (N), forces (3, N) and virial (9, N); ``pos`` is (3, N)."""
@@ -132,6 +195,11 @@ class Oracle:
                                  ptr(pe), ptr(f), ptr(vir), nthreads)
         if rc != 0:
             raise RuntimeError("oracle_efs failed")
+        if self.zbl is not None:
+            z, pin, pout = self.zbl
+            if self.lib.oracle_zbl_efs(self.model.species_count, ptr(z), ptr(pin), ptr(pout), N, ptr(h),
+                                       ptr(pbc), ptr(types), ptr(pos), ptr(pe), ptr(f), ptr(vir), nthreads) != 0:
+                raise RuntimeError("oracle_zbl_efs failed")
         return pe, f, vir
 
     def basics(self, h, pbc, types, pos, nthreads: int = 0):
