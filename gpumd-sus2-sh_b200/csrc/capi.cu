@@ -3,8 +3,10 @@
 #include "../../include/sus2sh.h"
 #include "../../include/sus2sh_tools.h"
 #include "cg_codegen.h"
+#include "edge_jit.h"
 #include "engine.cuh"
 #include "mtp_model.h"
+#include "sh_math.cuh"
 #include "zbl.cuh"
 
 #include <algorithm>
@@ -330,6 +332,10 @@ struct Engine {
   // tile autotuner: CTA sizes of the edge kernels, timed on the first call
   int basic_block = 128, force_block = 128;
   bool tuned = false;
+  // edge kernels built with NVRTC at load (shapes without an ahead-of-time build)
+  bool edge_jit = false;
+  std::shared_ptr<const EdgeJitBinary> ejit_bin;
+  EdgeJitModule ejit_mod;
   // model-specialised CG kernel (NVRTC); empty cubin -> interpreter
   CgSource cg_src;
   CgBinary cg_bin;
@@ -383,11 +389,10 @@ struct Engine {
     profile = opt.profile;
     lay = layer_products(model);
     prog = compile_program(model, lay);
-    if (!shape_supported(model.l_max, model.k_max, model.rb_size)) {
-      throw InputError("SUS2_SH engine has no compiled kernel for sh_l_max=" + std::to_string(model.l_max) +
-                       ", sh_k_max=" + std::to_string(model.k_max) +
-                       ", radial_basis_size=" + std::to_string(model.rb_size) + ".");
-    }
+    // shapes without an ahead-of-time build (or sus2_sh_edge_jit=1) get their
+    // edge kernels from NVRTC now
+    edge_jit = opt.edge_jit || !shape_supported(model.l_max, model.k_max, model.rb_size);
+    if (edge_jit) ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128);
     list_cutoff = model.rc;
     if (model.zbl_enabled) {
       // atomic numbers from the model, else from the element symbols after the
@@ -689,9 +694,43 @@ struct Engine {
   // touched) and keeps the fastest.  Runs once per handle, at the first
   // evaluation, where the neighbour-list sizing already synchronises.
   template <typename T>
+  size_t edge_smem() const {
+    return sizeof(T) * static_cast<size_t>(rs.species) * rs.species * rs.pair_stride;
+  }
+
+  // k_basic / k_force through the ahead-of-time build or the NVRTC module.
+  template <typename T>
+  void run_basic(cudaStream_t s, const EdgeArgs<T>& a, int block) {
+    if (edge_jit) {
+      std::string err;
+      if (!ejit_mod.load(*ejit_bin, &err) ||
+          !ejit_mod.launch_basic(s, a.N, 128, edge_smem<T>(), &a, Bbuf.p, &err))
+        throw CudaError(err);
+      return;
+    }
+    if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block) != 0)
+      throw InputError("SUS2_SH basic kernel shape not compiled.");
+  }
+
+  template <typename T>
+  void run_force(cudaStream_t s, const EdgeArgs<T>& a, const double* weight, double* force, double* virial,
+                 double sign, int block) {
+    if (edge_jit) {
+      std::string err;
+      if (!ejit_mod.load(*ejit_bin, &err) ||
+          !ejit_mod.launch_force(s, a.N, 128, edge_smem<T>(), &a, Gbuf.p, weight, ftmp.p, force, virial, sign,
+                                 &err))
+        throw CudaError(err);
+      return;
+    }
+    if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign, block) != 0)
+      throw InputError("SUS2_SH force kernel shape not compiled.");
+  }
+
+  template <typename T>
   void autotune(cudaStream_t s, const EdgeArgs<T>& a) {
     tuned = true;
-    if (!opt.autotune || sizeof(T) != 4) return;
+    if (!opt.autotune || sizeof(T) != 4 || edge_jit) return;
     DevBuf<double> f_scratch, w_scratch;
     f_scratch.resize(3ull * N);
     w_scratch.resize(9ull * N);
@@ -736,8 +775,7 @@ struct Engine {
     const EdgeArgs<T> a = edge_args<T>();
     if (!tuned) autotune<T>(s, a);
     mark(ev, 1, s);
-    if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), basic_block) != 0)
-      throw InputError("SUS2_SH basic kernel shape not compiled.");
+    run_basic<T>(s, a, basic_block);
     mark(ev, 2, s);
     if (!cg_bin.cubin.empty()) {
       std::string err;
@@ -764,9 +802,7 @@ struct Engine {
     const EdgeArgs<T> a = edge_args<T>();
     ck(cudaMemsetAsync(ftmp.p, 0, ftmp.n, s), "memset");
     mark(ev, 3, s);
-    if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign,
-                        force_block) != 0)
-      throw InputError("SUS2_SH force kernel shape not compiled.");
+    run_force<T>(s, a, weight, force, virial, sign, force_block);
     if (model.zbl_enabled) {
       launch_zbl(s, 1, N, cap, pos4.p, nbr.p, ncount.p, a.shift, a.atom_cell, zbl_tables(), weight, nullptr, force,
                  virial, sign);
@@ -799,7 +835,8 @@ struct Engine {
     fp.scalar_w = d_sw.p;
     if (launch_param_grad<T>(s, edge_args<T>(), fp, model.moments, d_species.p, ew, fw, base, base + nb,
                              base + 4 * nb, base + 2 * nb, base + 3 * nb, grad_w, grad_c) != 0)
-      throw InputError("SUS2_SH parameter-gradient kernel shape not compiled.");
+      throw InputError("SUS2_SH parameter gradients are built ahead of time for the common shapes only; "
+                       "this model shape (sh_l_max, sh_k_max, radial_basis_size) has none.");
     launches += 3;
   }
 
@@ -896,6 +933,14 @@ bool check_box(const double* h, const int* pbc) {
     return false;
   }
   return true;
+}
+}  // namespace
+
+namespace {
+template <int L>
+void real_sh_host(double x, double y, double z, double* Y, const double* G, double* V) {
+  sus2sh::sh_values<L, double>(x, y, z, Y);
+  if (G && V) sus2sh::sh_grad_contract<L, double>(x, y, z, G, V[0], V[1], V[2]);
 }
 }  // namespace
 
@@ -1089,7 +1134,7 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[26] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[30] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
@@ -1097,8 +1142,10 @@ int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
                      e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0,
                      static_cast<int>(e.launches & 0x7fffffff), e.rs.shared_xi, e.prod_global ? 1 : 0,
                      e.cg_bin.cubin.empty() ? 0 : 1, e.cg_bin.registers, static_cast<int>(e.cg_compile_ms),
-                     e.basic_block, e.force_block};
-  const int k = std::min(n, 26);
+                     e.basic_block, e.force_block, e.edge_jit ? 1 : 0,
+                     e.ejit_bin ? e.ejit_bin->basic_registers : -1, e.ejit_bin ? e.ejit_bin->force_registers : -1,
+                     e.ejit_bin ? static_cast<int>(e.ejit_bin->compile_ms) : 0};
+  const int k = std::min(n, 30);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -1219,6 +1266,37 @@ int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text
       const size_t k = std::min(text_size - 1, t.size());
       std::memcpy(text, t.data(), k);
       text[k] = 0;
+    }
+  });
+}
+
+int sus2sh_real_sh(int l_max, double x, double y, double z, double* Y, const double* G, double* V) {
+  if (!Y) return SUS2SH_E_ARG;
+  switch (l_max) {
+    case 0: real_sh_host<0>(x, y, z, Y, G, V); break;
+    case 1: real_sh_host<1>(x, y, z, Y, G, V); break;
+    case 2: real_sh_host<2>(x, y, z, Y, G, V); break;
+    case 3: real_sh_host<3>(x, y, z, Y, G, V); break;
+    case 4: real_sh_host<4>(x, y, z, Y, G, V); break;
+    case 5: real_sh_host<5>(x, y, z, Y, G, V); break;
+    case 6: real_sh_host<6>(x, y, z, Y, G, V); break;
+    default: return SUS2SH_E_ARG;
+  }
+  return SUS2SH_OK;
+}
+
+int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_registers, int* force_registers,
+                            double* compile_ms, char* log, size_t log_len) {
+  return guarded([&] {
+    if (l_max < 0 || l_max > 6 || k_max <= 0 || k_max * (l_max + 1) > 48 || rb <= 0 || rb > 16)
+      throw sus2sh::InputError("SUS2_SH edge-kernel shape out of range.");
+    const auto bin = sus2sh::compile_edge_kernels(fp32 != 0, l_max, k_max, rb, 128);
+    if (basic_registers) *basic_registers = bin->basic_registers;
+    if (force_registers) *force_registers = bin->force_registers;
+    if (compile_ms) *compile_ms = bin->compile_ms;
+    if (log && log_len) {
+      std::strncpy(log, bin->log.c_str(), log_len - 1);
+      log[log_len - 1] = '\0';
     }
   });
 }

@@ -1,6 +1,7 @@
 // Straight-line CG product kernels generated per model and compiled with
 // NVRTC (see cg_codegen.h).
 #include "cg_codegen.h"
+#include "driver_api.h"
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -234,22 +235,7 @@ CgBinary compile_cg_source(const CgSource& src) {
 // ---------------------------------------------------------------------------
 // driver API through the runtime's entry-point query
 // ---------------------------------------------------------------------------
-namespace {
-using PFN_load = CUresult (*)(CUmodule*, const void*);
-using PFN_get = CUresult (*)(CUfunction*, CUmodule, const char*);
-using PFN_launch = CUresult (*)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
-                                CUstream, void**, void**);
-using PFN_unload = CUresult (*)(CUmodule);
-
-template <typename F>
-F entry(const char* name) {
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  if (cudaGetDriverEntryPoint(name, &fn, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
-    return nullptr;
-  return reinterpret_cast<F>(fn);
-}
-}  // namespace
+using namespace drv;
 
 CgModule::~CgModule() {
   if (module_) {

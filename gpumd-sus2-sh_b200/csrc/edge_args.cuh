@@ -1,0 +1,38 @@
+// Arguments of the per-edge kernels (k_basic, k_force and the parameter-
+// gradient edge kernels), shared by the ahead-of-time build and the NVRTC
+// build of model shapes compiled at load (no host headers here).
+#pragma once
+
+namespace sus2sh {
+
+constexpr int kMaxPairTable = 8192;  // floats of per-pair radial table
+constexpr int kMaxCoef = 48 * 16;
+
+// Radial table: per pair p = t_i*S + t_j: [KMU] (scal, shift) pairs then the
+// pair scale; shared_xi means every mu of a pair uses the same (scal, shift).
+struct RadialSetup {
+  int species;
+  int kmu;
+  int rb;
+  int rational;
+  int shared_xi;
+  int pair_stride;  // floats per pair in the table
+  double rc;
+};
+
+template <typename T>
+struct EdgeArgs {
+  int N;
+  int cap;
+  int l_max, k_max;
+  RadialSetup rs;
+  const double4* pos4;
+  const int* nbr;
+  const int* ncount;
+  const void* pair_table;   // T[S*S][pair_stride]
+  const double (*shift)[3];  // image vectors [cells][125][3] (one box: BoxGeom::shift)
+  const int* atom_cell;      // cell of each atom in a batch of boxes, NULL for one box
+  T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
+};
+
+}  // namespace sus2sh

@@ -3,7 +3,7 @@
 // the radial basis (values, and values + derivatives).
 #pragma once
 
-#include "engine.cuh"
+#include "edge_args.cuh"
 #include "sh_math.cuh"
 
 namespace sus2sh {

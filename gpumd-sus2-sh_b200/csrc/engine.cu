@@ -16,6 +16,7 @@
 // per-atom sums are private and only the F_j scatter uses atomics (one
 // 128-bit vector red per edge in FP32).
 #include "edge_common.cuh"
+#include "edge_kernels.cuh"
 #include "engine.cuh"
 #include "sh_math.cuh"
 #include "zbl.cuh"
@@ -26,16 +27,6 @@ namespace sus2sh {
 namespace {
 using namespace edge;
 
-// Minimum resident CTAs per SM of the FP32 edge kernels (register caps).
-// Measured on the 1.024M-atom l3k3 workload: k_force at 4 CTAs (128 registers,
-// 8 B spill) runs 1.55 ms vs 1.87 ms at its natural 167 registers; capping
-// k_basic below its natural 126 registers (5 CTAs) spills and loses.
-#ifndef SUS2_BASIC_MIN_BLOCKS
-#define SUS2_BASIC_MIN_BLOCKS 1
-#endif
-#ifndef SUS2_FORCE_MIN_BLOCKS
-#define SUS2_FORCE_MIN_BLOCKS 4
-#endif
 // ---------------------------------------------------------------------------
 // positions
 // ---------------------------------------------------------------------------
@@ -236,165 +227,6 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
   atomicMax(&st->max_count, k);
   if (k > cap && !count_only) st->overflow = 1;
   if (!count_only) pos4[i] = p;
-}
-
-// ---------------------------------------------------------------------------
-// basic moments
-// ---------------------------------------------------------------------------
-template <typename T, int L, int K, int RB, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK : 1) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_tab = reinterpret_cast<T*>(smem_raw);
-  load_pair_table(a, s_tab);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
-  constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
-  T acc[NB];
-#pragma unroll
-  for (int b = 0; b < NB; ++b) acc[b] = T(0);
-  const double4 pi = a.pos4[i];
-  const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
-  const int S = a.rs.species;
-  const int row_i = type_of(pi) * S;
-  const int cnt = min(a.ncount[i], a.cap);
-  const double rc = a.rs.rc, rc2 = rc * rc;
-  NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
-  for (int n = 0; n < cnt; ++n) {
-    int w;
-    double4 pj;
-    ns.next(n, w, pj);
-    double sx, sy, sz;
-    image_shift(cell_shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
-    const double dx = pj.x - pi.x + sx;
-    const double dy = pj.y - pi.y + sy;
-    const double dz = pj.z - pi.z + sz;
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 >= rc2) continue;
-    const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
-    const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
-    T R[KMU];
-    radial_values<T, KMU, RB>(a, row, e, R);
-    T Y[C];
-    sh_values<L>(e.ux, e.uy, e.uz, Y);
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int l = 0; l <= L; ++l)
-#pragma unroll
-        for (int m = 0; m <= 2 * l; ++m)
-          acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], Y[l * l + m], acc[k * C + l * l + m]);
-  }
-#pragma unroll
-  for (int b = 0; b < NB; ++b) B[static_cast<size_t>(b) * a.N + i] = acc[b];
-}
-
-// ---------------------------------------------------------------------------
-// forces and virial
-// ---------------------------------------------------------------------------
-template <typename T>
-struct Scatter;
-template <>
-struct Scatter<float> {
-  __device__ __forceinline__ static void add(void* buf, int j, float x, float y, float z) {
-    atomicAdd(reinterpret_cast<float4*>(buf) + j, make_float4(x, y, z, 0.0f));
-  }
-};
-template <>
-struct Scatter<double> {
-  __device__ __forceinline__ static void add(void* buf, int j, double x, double y, double z) {
-    double* p = reinterpret_cast<double*>(reinterpret_cast<double4*>(buf) + j);
-    atomicAdd(p, x);
-    atomicAdd(p + 1, y);
-    atomicAdd(p + 2, z);
-  }
-};
-
-template <typename T, int L, int K, int RB, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK : 1)
-    k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
-            void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
-            double sign) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_tab = reinterpret_cast<T*>(smem_raw);
-  load_pair_table(a, s_tab);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
-  constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
-  const T wscale = weight ? static_cast<T>(weight[i]) : T(1);
-  T g[NB];
-#pragma unroll
-  for (int b = 0; b < NB; ++b) g[b] = wscale * G[static_cast<size_t>(b) * a.N + i];
-  T fx = T(0), fy = T(0), fz = T(0);
-  T w[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) w[q] = T(0);
-  const double4 pi = a.pos4[i];
-  const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
-  const int S = a.rs.species;
-  const int row_i = type_of(pi) * S;
-  const int cnt = min(a.ncount[i], a.cap);
-  const double rc = a.rs.rc, rc2 = rc * rc;
-  NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
-  for (int n = 0; n < cnt; ++n) {
-    int wd;
-    double4 pj;
-    ns.next(n, wd, pj);
-    const int j = wd & 0xFFFFFF;
-    double sx, sy, sz;
-    image_shift(cell_shift, static_cast<unsigned>(wd) >> 24, sx, sy, sz);
-    const double dx = pj.x - pi.x + sx;
-    const double dy = pj.y - pi.y + sy;
-    const double dz = pj.z - pi.z + sz;
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 >= rc2) continue;
-    const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
-    const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
-    T R[KMU], dR[KMU];
-    radial_values_ders<T, KMU, RB>(a, row, e, R, dR);
-    T Y[C];
-    sh_values<L>(e.ux, e.uy, e.uz, Y);
-    T Gy[C];
-    T s = T(0);
-#pragma unroll
-    for (int l = 0; l <= L; ++l)
-#pragma unroll
-      for (int m = 0; m <= 2 * l; ++m) {
-        T gv = T(0), hv = T(0);
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          gv = fma(g[k * C + l * l + m], R[k * (L + 1) + l], gv);
-          hv = fma(g[k * C + l * l + m], dR[k * (L + 1) + l], hv);
-        }
-        Gy[l * l + m] = gv;
-        s = fma(hv, Y[l * l + m], s);
-      }
-    T vx, vy, vz;
-    sh_grad_contract<L>(e.ux, e.uy, e.uz, Gy, vx, vy, vz);
-    const T uv = e.ux * vx + e.uy * vy + e.uz * vz;
-    const T dEx = s * e.ux + (vx - uv * e.ux) * e.rinv;
-    const T dEy = s * e.uy + (vy - uv * e.uy) * e.rinv;
-    const T dEz = s * e.uz + (vz - uv * e.uz) * e.rinv;
-    fx += dEx;
-    fy += dEy;
-    fz += dEz;
-    Scatter<T>::add(ftmp, j, -dEx, -dEy, -dEz);
-    w[0] -= e.dx * dEx;
-    w[1] -= e.dy * dEy;
-    w[2] -= e.dz * dEz;
-    w[3] -= e.dx * dEy;
-    w[4] -= e.dx * dEz;
-    w[5] -= e.dy * dEz;
-    w[6] -= e.dy * dEx;
-    w[7] -= e.dz * dEx;
-    w[8] -= e.dz * dEy;
-  }
-  force[i] += sign * static_cast<double>(fx);
-  force[i + a.N] += sign * static_cast<double>(fy);
-  force[i + 2 * a.N] += sign * static_cast<double>(fz);
-  if (virial) {
-#pragma unroll
-    for (int q = 0; q < 9; ++q) virial[static_cast<size_t>(q) * a.N + i] += static_cast<double>(w[q]);
-  }
 }
 
 template <typename T>
@@ -733,9 +565,19 @@ static size_t pair_smem(const EdgeArgs<T>& a) {
 // engine always uses 128).
 bool block_supported(int block, bool fp32) { return block == 128 || (fp32 && (block == 64 || block == 256)); }
 
+// Opts a kernel into more than 48 KB of dynamic shared memory (large species
+// counts with many radial functions) once per kernel.
+template <typename K>
+void allow_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+
 template <typename T, int L, int K, int RB>
 int launch_basic_shape(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
   const size_t sm = pair_smem(a);
+  allow_smem(k_basic<T, L, K, RB, 64>, sm);
+  allow_smem(k_basic<T, L, K, RB, 128>, sm);
+  allow_smem(k_basic<T, L, K, RB, 256>, sm);
   if (sizeof(T) == 4 && block == 64) {
     k_basic<T, L, K, RB, 64><<<blocks_for(a.N, 64), 64, sm, s>>>(a, B);
   } else if (sizeof(T) == 4 && block == 256) {
@@ -750,6 +592,9 @@ template <typename T, int L, int K, int RB>
 int launch_force_shape(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight, void* ftmp,
                        double* force, double* virial, double sign, int block) {
   const size_t sm = pair_smem(a);
+  allow_smem(k_force<T, L, K, RB, 64>, sm);
+  allow_smem(k_force<T, L, K, RB, 128>, sm);
+  allow_smem(k_force<T, L, K, RB, 256>, sm);
   if (sizeof(T) == 4 && block == 64) {
     k_force<T, L, K, RB, 64><<<blocks_for(a.N, 64), 64, sm, s>>>(a, G, weight, ftmp, force, virial, sign);
   } else if (sizeof(T) == 4 && block == 256) {

@@ -15,10 +15,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "edge_args.cuh"
+
 namespace sus2sh {
 
-constexpr int kMaxPairTable = 8192;  // floats of per-pair radial table
-constexpr int kMaxCoef = 48 * 16;
 
 // Box and cell grid for one neighbour build (host computed).
 struct BoxGeom {
@@ -39,33 +39,6 @@ struct Status {
   int bad_type;                // a species index outside [0, species_count) was seen (sticky)
   int thin_cell;               // a batch cell thinner than half the cutoff (sticky)
   int pad;
-};
-
-// Radial table: per pair p = t_i*S + t_j: [KMU] (scal, shift) pairs then the
-// pair scale; shared_xi means every mu of a pair uses the same (scal, shift).
-struct RadialSetup {
-  int species;
-  int kmu;
-  int rb;
-  int rational;
-  int shared_xi;
-  int pair_stride;  // floats per pair in the table
-  double rc;
-};
-
-template <typename T>
-struct EdgeArgs {
-  int N;
-  int cap;
-  int l_max, k_max;
-  RadialSetup rs;
-  const double4* pos4;
-  const int* nbr;
-  const int* ncount;
-  const void* pair_table;   // T[S*S][pair_stride]
-  const double (*shift)[3];  // image vectors [cells][125][3] (one box: BoxGeom::shift)
-  const int* atom_cell;      // cell of each atom in a batch of boxes, NULL for one box
-  T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
 };
 
 struct ProgramDev {

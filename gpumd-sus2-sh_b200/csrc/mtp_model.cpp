@@ -202,8 +202,8 @@ HostModel load_model(const std::string& path) {
     throw InputError("SUS2_SH two-layer gate models are not supported by this engine.");
 
   if (scaling_map != "LK") throw InputError("SUS2_SH requires scaling_map = LK.");
-  if (m.l_max < 0 || m.l_max > 4)
-    throw InputError("SUS2_SH engine supports sh_l_max in [0,4].");
+  if (m.l_max < 0 || m.l_max > 6)
+    throw InputError("SUS2_SH supports sh_l_max in [0,6].");
   if (m.body_order < 2 || m.body_order > 6)
     throw InputError("SUS2_SH supports sh_body_order in [2,6].");
   if (m.k_max <= 0 || m.radial_funcs != m.k_max * (m.l_max + 1))
@@ -767,6 +767,8 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       o.profile = parse_bool(val, key);
     } else if (key == "sus2_sh_autotune") {
       o.autotune = parse_bool(val, key);
+    } else if (key == "sus2_sh_edge_jit") {
+      o.edge_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_cg_jit") {
       o.cg_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_reference_rounding") {
@@ -790,7 +792,7 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
 // in the text layout the reference reader accepts.
 // ---------------------------------------------------------------------------
 void write_synthetic_model(const std::string& path, const SynthSpec& sp) {
-  if (sp.species <= 0 || sp.l_max < 0 || sp.l_max > 4 || sp.k_max <= 0 || sp.body_order < 2 ||
+  if (sp.species <= 0 || sp.l_max < 0 || sp.l_max > 6 || sp.k_max <= 0 || sp.body_order < 2 ||
       sp.body_order > 6 || sp.rb_size <= 0 || sp.rb_size > 16 ||
       static_cast<int>(sp.shift.size()) != sp.species)
     throw InputError("Invalid synthetic model specification.");

@@ -110,6 +110,8 @@ struct Options {
   bool profile = false;             // sus2_sh_profile / sus2_profile / SUS2_SH_GPUMD_PROFILE
   bool cg_jit = true;               // sus2_sh_cg_jit=0 runs the CG row interpreter instead
   bool autotune = true;             // sus2_sh_autotune=0 keeps 128-thread edge-kernel CTAs
+  bool edge_jit = false;            // sus2_sh_edge_jit=1 compiles the edge kernels at load even
+                                    // for a shape built ahead of time
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

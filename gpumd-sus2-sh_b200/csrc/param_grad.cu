@@ -15,6 +15,7 @@
 // The flat product pass follows the reference's simplest form
 // (gpu_sh_forward_energy_backward, src/force/sus2_sh.cu:4799-4846).
 #include "edge_common.cuh"
+#include "engine.cuh"
 
 namespace sus2sh {
 namespace {

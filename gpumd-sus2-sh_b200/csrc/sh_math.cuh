@@ -1,10 +1,13 @@
 // Per-edge math of the SUS2-SH descriptor, shared by the CUDA kernels and by
 // host-side unit tests (every function is __host__ __device__).
 //
-//  * Real spherical harmonics Y_lm(u), l <= 4, orthonormal, no Condon-Shortley
+//  * Real spherical harmonics Y_lm(u), l <= 6, orthonormal, no Condon-Shortley
 //    phase, flat index l*l + l + m (same basis and ordering as the reference's
-//    eval_real_sh, src/force/sus2_sh.cu:3032-3169).  The polynomial forms are
-//    the standard real-harmonic table evaluated on the unit vector u = d/|d|.
+//    eval_real_sh, src/force/sus2_sh.cu:3032-3169, and its solid-harmonic
+//    path for l_max > 4, :2880-3030).  For L <= 4 the polynomial forms are the
+//    standard real-harmonic table evaluated on the unit vector u = d/|d|; for
+//    L = 5, 6 every l comes from the associated-Legendre recurrences of the
+//    complex solid harmonics (sh_values_solid below).
 //  * Gradients use the tangential projection: for Y(d) = F(d/r),
 //        dY/dd = (grad F(u) - (u . grad F(u)) u) / r,
 //    with F the homogeneous Cartesian polynomial of each harmonic.  The force
@@ -18,7 +21,9 @@
 //    scaling folded per pair (build_direct_radial_tables, sus2_sh.cu:2484-2517).
 #pragma once
 
+#if !defined(__CUDACC_RTC__)
 #include <cmath>
+#endif
 
 #if defined(__CUDACC__)
 #define SUS2_HD __host__ __device__ __forceinline__
@@ -49,9 +54,183 @@ struct YC {
   static constexpr double c44 = 0.62583573544917613459;   // 3/16 sqrt(35/pi)
 };
 
+// Normalisation of the solid-harmonic path: N_l0 for m = 0 and sqrt(2) N_lm
+// for m > 0, N_lm^2 = (2l+1)/(4 pi) (l-m)!/(l+m)!, keyed by 8 l + m.
+SUS2_HD constexpr double solid_norm(int key) {
+  switch (key) {
+    case 0: return 0.28209479177387814;
+    case 8: return 0.4886025119029199;
+    case 9: return 0.48860251190292;
+    case 16: return 0.6307831305050401;
+    case 17: return 0.36418281019735976;
+    case 18: return 0.18209140509867988;
+    case 24: return 0.7463526651802308;
+    case 25: return 0.3046971996429772;
+    case 26: return 0.09635371475468515;
+    case 27: return 0.03933623932844291;
+    case 32: return 0.8462843753216345;
+    case 33: return 0.2676186174229157;
+    case 34: return 0.063078313050504;
+    case 35: return 0.016858388283618388;
+    case 36: return 0.005960340337611203;
+    case 40: return 0.9356025796273888;
+    case 41: return 0.2415715473043717;
+    case 42: return 0.045652731285460234;
+    case 43: return 0.009318824751147628;
+    case 44: return 0.002196468058075176;
+    case 45: return 0.0006945841871324552;
+    case 48: return 1.0171072362820548;
+    case 49: return 0.22195099524523101;
+    case 50: return 0.03509353369580661;
+    case 51: return 0.005848922282634435;
+    case 52: return 0.0010678622237644956;
+    case 53: return 0.00022766899107568562;
+    case 54: return 6.57223766418388e-05;
+    default: return 0.0;
+  }
+}
+
+// Every Y_lm, l <= L, from the complex solid harmonics
+// Q_l^m = r^l P_l^m(cos t) e^{i m p} (associated Legendre without the
+// Condon-Shortley phase), built by the standard recurrences
+//   Q_m^m = (2m-1) (x + i y) Q_{m-1}^{m-1},   Q_{m+1}^m = (2m+1) z Q_m^m,
+//   (l-m) Q_l^m = (2l-1) z Q_{l-1}^m - (l+m-1) r^2 Q_{l-2}^m,
+// with Y_l0 = N_l0 Re Q_l^0 and (Y_l,m, Y_l,-m) = sqrt2 N_lm (Re, Im) Q_l^m.
+// r^2 is formed from (x, y, z), so the polynomials stay homogeneous and their
+// gradients (sh_grad_solid) obey the tangential-projection identity.
+template <int L, typename T>
+SUS2_HD void sh_values_solid(T x, T y, T z, T* Y) {
+  const T r2 = x * x + y * y + z * z;
+  T dre = T(1), dim = T(0);
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if (m > 0) {
+      const T c = T(2 * m - 1);
+      const T re = c * (x * dre - y * dim), im = c * (x * dim + y * dre);
+      dre = re;
+      dim = im;
+    }
+    T p1re = dre, p1im = dim, p2re = T(0), p2im = T(0);
+#pragma unroll
+    for (int l = m; l <= L; ++l) {
+      if (l == m + 1) {
+        const T c = T(2 * m + 1) * z;
+        p2re = p1re;
+        p2im = p1im;
+        p1re = c * p2re;
+        p1im = c * p2im;
+      } else if (l > m + 1) {
+        const T a = T(2 * l - 1) * z, b = T(l + m - 1) * r2, inv = T(1.0 / (l - m));
+        const T qre = (a * p1re - b * p2re) * inv, qim = (a * p1im - b * p2im) * inv;
+        p2re = p1re;
+        p2im = p1im;
+        p1re = qre;
+        p1im = qim;
+      }
+      const T nrm = T(solid_norm(8 * l + m));
+      Y[l * l + l + m] = nrm * p1re;
+      if (m > 0) Y[l * l + l - m] = nrm * p1im;
+    }
+  }
+}
+
+// V = sum_lm G[lm] grad P_lm on the solid-harmonic path (forward-mode
+// derivatives carried through the same recurrences).
+template <int L, typename T>
+SUS2_HD void sh_grad_solid(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
+  const T r2 = x * x + y * y + z * z;
+  vx = vy = vz = T(0);
+  // diagonal Q_m^m: value and gradient (re, im)
+  T dre = T(1), dim = T(0);
+  T dgre[3] = {T(0), T(0), T(0)}, dgim[3] = {T(0), T(0), T(0)};
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if (m > 0) {
+      const T c = T(2 * m - 1);
+      T gre[3], gim[3];
+      gre[0] = c * (x * dgre[0] - y * dgim[0] + dre);
+      gre[1] = c * (x * dgre[1] - y * dgim[1] - dim);
+      gre[2] = c * (x * dgre[2] - y * dgim[2]);
+      gim[0] = c * (x * dgim[0] + y * dgre[0] + dim);
+      gim[1] = c * (x * dgim[1] + y * dgre[1] + dre);
+      gim[2] = c * (x * dgim[2] + y * dgre[2]);
+      const T re = c * (x * dre - y * dim), im = c * (x * dim + y * dre);
+      dre = re;
+      dim = im;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        dgre[a] = gre[a];
+        dgim[a] = gim[a];
+      }
+    }
+    T p1re = dre, p1im = dim, p2re = T(0), p2im = T(0);
+    T g1re[3], g1im[3], g2re[3] = {T(0), T(0), T(0)}, g2im[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      g1re[a] = dgre[a];
+      g1im[a] = dgim[a];
+    }
+#pragma unroll
+    for (int l = m; l <= L; ++l) {
+      if (l == m + 1) {
+        const T c = T(2 * m + 1);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          g2re[a] = g1re[a];
+          g2im[a] = g1im[a];
+          g1re[a] = c * (z * g2re[a] + (a == 2 ? p1re : T(0)));
+          g1im[a] = c * (z * g2im[a] + (a == 2 ? p1im : T(0)));
+        }
+        p2re = p1re;
+        p2im = p1im;
+        p1re = c * z * p2re;
+        p1im = c * z * p2im;
+      } else if (l > m + 1) {
+        const T a2 = T(2 * l - 1), b2 = T(l + m - 1), inv = T(1.0 / (l - m));
+        const T q[3] = {x, y, z};
+        T nre[3], nim[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          nre[a] = (a2 * (z * g1re[a] + (a == 2 ? p1re : T(0))) -
+                    b2 * (r2 * g2re[a] + T(2) * q[a] * p2re)) * inv;
+          nim[a] = (a2 * (z * g1im[a] + (a == 2 ? p1im : T(0))) -
+                    b2 * (r2 * g2im[a] + T(2) * q[a] * p2im)) * inv;
+        }
+        const T qre = (a2 * z * p1re - b2 * r2 * p2re) * inv, qim = (a2 * z * p1im - b2 * r2 * p2im) * inv;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          g2re[a] = g1re[a];
+          g2im[a] = g1im[a];
+          g1re[a] = nre[a];
+          g1im[a] = nim[a];
+        }
+        p2re = p1re;
+        p2im = p1im;
+        p1re = qre;
+        p1im = qim;
+      }
+      const T nrm = T(solid_norm(8 * l + m));
+      const T cre = nrm * G[l * l + l + m];
+      vx = fma(cre, g1re[0], vx);
+      vy = fma(cre, g1re[1], vy);
+      vz = fma(cre, g1re[2], vz);
+      if (m > 0) {
+        const T cim = nrm * G[l * l + l - m];
+        vx = fma(cim, g1im[0], vx);
+        vy = fma(cim, g1im[1], vy);
+        vz = fma(cim, g1im[2], vz);
+      }
+    }
+  }
+}
+
 // Y[l*l+l+m] for l <= L at unit vector (x, y, z).
 template <int L, typename T>
 SUS2_HD void sh_values(T x, T y, T z, T* Y) {
+  if constexpr (L > 4) {
+    sh_values_solid<L>(x, y, z, Y);
+    return;
+  }
   Y[0] = T(YC::c00);
   if (L < 1) return;
   Y[1] = T(YC::c1) * y;
@@ -89,6 +268,10 @@ SUS2_HD void sh_values(T x, T y, T z, T* Y) {
 // V = sum_lm G[lm] * grad P_lm(u), P_lm the homogeneous polynomial of Y_lm.
 template <int L, typename T>
 SUS2_HD void sh_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
+  if constexpr (L > 4) {
+    sh_grad_solid<L>(x, y, z, G, vx, vy, vz);
+    return;
+  }
   vx = T(0);
   vy = T(0);
   vz = T(0);

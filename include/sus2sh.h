@@ -180,8 +180,10 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * HBM [21] model-specialised CG kernel in use [22] its registers per thread
  * [23] its NVRTC compile time (ms) [24] CTA size of the basic-moment kernel
  * [25] CTA size of the force kernel (both picked by the tile autotuner at the
- * first evaluation; option sus2_sh_autotune=0 keeps 128).  Returns the number
- * written. */
+ * first evaluation; option sus2_sh_autotune=0 keeps 128) [26] edge kernels
+ * compiled with NVRTC at load (shape without an ahead-of-time build, or
+ * sus2_sh_edge_jit=1) [27] [28] their registers per thread (basic, force)
+ * [29] their compile time (ms).  Returns the number written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

@@ -51,6 +51,22 @@ int sus2sh_reduce(int N, const double* potential, const double* virial, double* 
  * above the straight-line limit (12000 products) return SUS2SH_E_INPUT. */
 int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text, size_t text_size);
 
+/* Compiles the per-edge kernels (k_basic, k_force, 128-thread CTAs) of one
+ * model shape with NVRTC for sm_100a, as model load does for shapes without
+ * an ahead-of-time build, and reports their register counts, the compile time
+ * and the compiler log (truncated to log_len).  Needs no GPU.  No reference
+ * counterpart (the reference dispatches among fixed kernels). */
+int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_registers, int* force_registers,
+                            double* compile_ms, char* log, size_t log_len);
+
+/* The engine's real spherical harmonics, evaluated on the host in FP64: Y at
+ * the unit vector (x, y, z) for every l <= l_max (l_max <= 6, flat index
+ * l*l + l + m) and, when G and V are non-NULL, V = sum_lm G[lm] grad P_lm
+ * (P_lm the homogeneous polynomial of Y_lm).  No reference counterpart; the
+ * reference evaluates them inside its kernels (eval_real_sh,
+ * src/force/sus2_sh.cu:2880-3169). */
+int sus2sh_real_sh(int l_max, double x, double y, double z, double* Y, const double* G, double* V);
+
 /* The engine's ZBL pair function (energy and dE/dr at distance r for atomic
  * numbers zi, zj and the pair's inner/outer cutoffs), for checks against the
  * reference's sus2_zbl_pair. */

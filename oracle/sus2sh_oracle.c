@@ -115,11 +115,76 @@ static double ycoef(int idx) {
 
 static int l_of(int idx) { return idx < 1 ? 0 : idx < 4 ? 1 : idx < 9 ? 2 : idx < 16 ? 3 : 4; }
 
-/* Y[idx] and dY[3*idx+a] at displacement d (not normalised). */
+static double fact(int n) {
+  double f = 1.0;
+  for (int k = 2; k <= n; ++k) f *= k;
+  return f;
+}
+
+static double binom(int n, int k) { return fact(n) / (fact(k) * fact(n - k)); }
+
+/* l = 5, 6 from the closed form of the complex solid harmonic (Rodrigues'
+ * formula for P_l differentiated m times, no Condon-Shortley phase):
+ *   r^l P_l^m(cos t) e^{imp} = (x + iy)^m sum_k a_k z^(l-2k-m) r^(2k),
+ *   a_k = 2^-l (-1)^k C(l,k) C(2l-2k,l) (l-2k)!/(l-2k-m)!,
+ * real harmonics Y_l0 = N_l0 Re, (Y_l,m, Y_l,-m) = sqrt2 N_lm (Re, Im),
+ * N_lm^2 = (2l+1)/(4 pi) (l-m)!/(l+m)!; divided by r^l with the quotient rule
+ * for the gradient. */
+static void solid_closed_form(int l, double x, double y, double z, double* Y, double* dY) {
+  const double pi = 3.14159265358979323846;
+  const double r2 = x * x + y * y + z * z, r = sqrt(r2);
+  const double rl = pow(r, -l), drl = -l * rl / r2;
+  for (int m = 0; m <= l; ++m) {
+    /* w = (x + iy)^m and its gradient (m (x+iy)^(m-1) (1, i, 0)) */
+    double wre = 1.0, wim = 0.0, pre = 1.0, pim = 0.0; /* p = (x+iy)^(m-1) */
+    for (int k = 0; k < m; ++k) {
+      pre = wre;
+      pim = wim;
+      const double a = wre * x - wim * y, b = wre * y + wim * x;
+      wre = a;
+      wim = b;
+    }
+    double gw_re[3] = {0, 0, 0}, gw_im[3] = {0, 0, 0};
+    if (m > 0) {
+      gw_re[0] = m * pre;  gw_im[0] = m * pim;
+      gw_re[1] = -m * pim; gw_im[1] = m * pre;
+    }
+    double sv = 0.0, gs[3] = {0, 0, 0};
+    for (int k = 0; 2 * k <= l - m; ++k) {
+      const int e = l - 2 * k - m;
+      const double a = ldexp(1.0, -l) * ((k & 1) ? -1.0 : 1.0) * binom(l, k) * binom(2 * l - 2 * k, l) *
+                       fact(l - 2 * k) / fact(e);
+      const double ze = pow(z, e), rk = pow(r2, k);
+      sv += a * ze * rk;
+      const double dze = e > 0 ? e * pow(z, e - 1) : 0.0;
+      const double drk = k > 0 ? k * pow(r2, k - 1) : 0.0;
+      gs[0] += a * ze * drk * 2.0 * x;
+      gs[1] += a * ze * drk * 2.0 * y;
+      gs[2] += a * (dze * rk + ze * drk * 2.0 * z);
+    }
+    double nrm = sqrt((2 * l + 1) / (4.0 * pi) * fact(l - m) / fact(l + m));
+    if (m > 0) nrm *= sqrt(2.0);
+    const double qre = wre * sv, qim = wim * sv;
+    const double q[3] = {x, y, z};
+    const int ip = l * l + l + m, in = l * l + l - m;
+    Y[ip] = nrm * qre * rl;
+    if (m > 0) Y[in] = nrm * qim * rl;
+    if (dY) {
+      for (int a = 0; a < 3; ++a) {
+        const double gre = gw_re[a] * sv + wre * gs[a], gim = gw_im[a] * sv + wim * gs[a];
+        dY[3 * ip + a] = nrm * (gre * rl + qre * drl * q[a]);
+        if (m > 0) dY[3 * in + a] = nrm * (gim * rl + qim * drl * q[a]);
+      }
+    }
+  }
+}
+
+/* Y[idx] and dY[3*idx+a] at displacement d (not normalised), l <= 6. */
 void oracle_real_sh(int L, double x, double y, double z, double* Y, double* dY) {
   const double r2 = x * x + y * y + z * z;
   const double r = sqrt(r2);
-  const int C = (L + 1) * (L + 1);
+  for (int l = 5; l <= L; ++l) solid_closed_form(l, x, y, z, Y, dY);
+  const int C = (L < 4 ? (L + 1) * (L + 1) : 25);
   for (int idx = 0; idx < C; ++idx) {
     double p, gx, gy, gz;
     poly(idx, x, y, z, &p, &gx, &gy, &gz);
@@ -396,7 +461,7 @@ int oracle_efs(const OracleModel* m, int N, const double* h, const int* pbc, con
     double* fl = fbuf + (size_t)tid * 3 * N;
     double* Mv = (double*)malloc(sizeof(double) * m->M);
     double* gv = (double*)malloc(sizeof(double) * m->M);
-    double R[64], dR[64], Y[32], dY[96];
+    double R[64], dR[64], Y[49], dY[147];
 #pragma omp for schedule(dynamic, 32)
     for (int i = 0; i < N; ++i) {
       const int ti = type[i];
@@ -485,7 +550,7 @@ int oracle_basics(const OracleModel* m, int N, const double* h, const int* pbc, 
   if (build_nlist(&g, N, pos, m->rc, &nl) != 0) return -1;
 #pragma omp parallel for schedule(dynamic, 32)
   for (int i = 0; i < N; ++i) {
-    double R[64], Y[32];
+    double R[64], Y[49];
     for (int b = 0; b < m->nbasic; ++b) B[(size_t)b * N + i] = 0.0;
     for (int q = nl.start[i]; q < nl.start[i + 1]; ++q) {
       const Edge* e = nl.e + q;

@@ -78,7 +78,7 @@ def test_clebsch_gordan_identities():
 def test_cpp_builder_matches_oracle():
     from sus2sh import standard_graph_counts
     for spec in ([3, 3, 4, None], [3, 3, 5, [3, 3, 3, 3]], [3, 3, 5, [3, 3, 2, 2]], [4, 4, 5, [4, 4, 2, 2]],
-                 [2, 2, 6, None], [1, 2, 3, None]):
+                 [2, 2, 6, None], [1, 2, 3, None], [5, 2, 4, None], [6, 2, 4, None], [6, 1, 5, None]):
         L, K, body, bl = spec
         c = standard_graph_counts(L, K, body, bl)
         g = build_standard_graph(L, K, body, body_lmax_from_list(L, body, bl) if bl else None)
@@ -104,3 +104,9 @@ def test_written_model_matches_standard_graph(l3k3_path, model_dir):
     m = load_mtp(p)
     g = build_standard_graph(2, 2, 6)
     assert standard_graph_matches(m, g)
+    # l = 6 (solid-harmonic path of the reference)
+    p = models.write_model(os.path.join(model_dir, "l6_b4.mtp"), l_max=6, k_max=2, body_order=4, rb_size=8,
+                           seed=6)
+    m = load_mtp(p)
+    assert m.sh_l_max == 6
+    assert standard_graph_matches(m, build_standard_graph(6, 2, 4))
