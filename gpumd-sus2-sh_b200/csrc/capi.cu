@@ -332,6 +332,13 @@ struct Engine {
   // tile autotuner: CTA sizes of the edge kernels, timed on the first call
   int basic_block = 128, force_block = 128;
   bool tuned = false;
+  // two-layer gate models
+  bool gate = false;
+  std::vector<double> gate_coef;  // [kmu][rb] first-layer radial coefficients
+  GateProgDev gprog{};
+  DevBuf<int> d_g_basic, d_g_prod, d_g_qslot, d_g_qbody;
+  DevBuf<double> d_g_coef, d_g_w, d_g_mix, d_g_add;
+  DevBuf<char> Bg, Gg, gslots, gmult, gderiv, gadj;
   // edge kernels built with NVRTC at load (shapes without an ahead-of-time build)
   bool edge_jit = false;
   std::shared_ptr<const EdgeJitBinary> ejit_bin;
@@ -392,7 +399,8 @@ struct Engine {
     // shapes without an ahead-of-time build (or sus2_sh_edge_jit=1) get their
     // edge kernels from NVRTC now
     edge_jit = opt.edge_jit || !shape_supported(model.l_max, model.k_max, model.rb_size);
-    if (edge_jit) ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128);
+    gate = model.gate.enabled;
+    if (edge_jit) ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
     list_cutoff = model.rc;
     if (model.zbl_enabled) {
       // atomic numbers from the model, else from the element symbols after the
@@ -445,8 +453,10 @@ struct Engine {
         row[2 * kmu] = model.scaling * model.radial_type_coeffs[zi] * model.radial_type_coeffs[zj];
       }
     rs.shared_xi = shared;
+    if (gate) gate_coef = model.gate.radial_coeffs;
     if (opt.reference_rounding) {
       // the reference's FP32 radial tables (sus2_sh.cu:2499-2512)
+      for (double& x : gate_coef) x = static_cast<double>(static_cast<float>(x));
       for (double& x : coef) x = static_cast<double>(static_cast<float>(x));
       for (double& x : pair_table) x = static_cast<double>(static_cast<float>(x));
     }
@@ -462,6 +472,7 @@ struct Engine {
       d_pair_d.upload(pair_table);
     }
     d_basic_canon.upload(prog.basic_canon);
+    if (gate) build_gate_program();
     d_canon_basic.upload(prog.canon_basic);
     d_shift.upload(model.shift_coeffs);
     d_species.upload(model.species_coeffs);
@@ -534,6 +545,15 @@ struct Engine {
     Gbuf.resize(nb * N * elem());
     ftmp.resize(static_cast<size_t>(N) * (use_float ? sizeof(float4) : sizeof(double4)));
     if (prod_global) scratch.resize(2ull * prog.nvalue * N * elem());
+    if (gate) {
+      const size_t kmu = static_cast<size_t>(model.radial_funcs);
+      Bg.resize(nb * N * elem());
+      Gg.resize(nb * N * elem());
+      gslots.resize(2ull * gprog.nslots * N * elem());
+      gmult.resize(kmu * N * elem());
+      gderiv.resize(kmu * N * elem());
+      gadj.resize(kmu * N * elem());
+    }
     cap = 0;
     nbr.release();
     have_ref = false;
@@ -561,6 +581,74 @@ struct Engine {
     }
     for (size_t k = 0; k < coef.size(); ++k) a.coef[k] = static_cast<T>(coef[k]);
     return a;
+  }
+
+  // EdgeArgs of the gate's first layer: same pair tables, gate coefficients.
+  template <typename T>
+  EdgeArgs<T> edge_args_gate() const {
+    EdgeArgs<T> a = edge_args<T>();
+    for (size_t k = 0; k < gate_coef.size(); ++k) a.coef[k] = static_cast<T>(gate_coef[k]);
+    return a;
+  }
+
+  // Slots for the moments the gate signals need (basics first), the needed
+  // products below the gate's product limit in file order, and the signal maps.
+  void build_gate_program() {
+    const GateModel& g = model.gate;
+    if (model.radial_funcs > 48) throw InputError("SUS2_SH gate supports radial_funcs_count <= 48.");
+    std::vector<int> slot(model.moments, -1);
+    std::vector<int> bcanon;
+    int ns = 0;
+    for (int b = 0; b < model.basic_count; ++b)
+      if (g.needed[b]) {
+        slot[b] = ns++;
+        bcanon.push_back(prog.basic_canon[b]);
+      }
+    const int nbasic = ns;
+    for (int m = model.basic_count; m < model.moments; ++m)
+      if (g.needed[m]) slot[m] = ns++;
+    std::vector<int> qslot, qbody;
+    for (size_t q = 0; q < g.moment_of.size(); ++q) {
+      int& sl = slot[g.moment_of[q]];
+      if (sl < 0) sl = ns++;  // zero-weight signal: a zero slot keeps every read in bounds
+      qslot.push_back(sl);
+      qbody.push_back(g.body_of[q]);
+    }
+    std::vector<int> pr;
+    std::vector<double> pc;
+    for (int p = 0; p < g.product_limit; ++p) {
+      const Product& x = model.products[p];
+      if (!g.needed[x.target]) continue;
+      pr.push_back(slot[x.left]);
+      pr.push_back(slot[x.right]);
+      pr.push_back(slot[x.target]);
+      pc.push_back(x.coeff);
+    }
+    d_g_basic.upload(bcanon);
+    d_g_prod.upload(pr);
+    d_g_coef.upload(pc);
+    d_g_qslot.upload(qslot);
+    d_g_qbody.upload(qbody);
+    d_g_w.upload(g.weights);
+    d_g_mix.upload(g.body_mix.empty() ? std::vector<double>(1, 0.0) : g.body_mix);
+    d_g_add.upload(g.additive);
+    gprog = GateProgDev{};
+    gprog.nslots = ns;
+    gprog.nbasic = nbasic;
+    gprog.basic_canon = d_g_basic.p;
+    gprog.nprod = static_cast<int>(pc.size());
+    gprog.prod = d_g_prod.p;
+    gprog.coef = d_g_coef.p;
+    gprog.nq = static_cast<int>(qslot.size());
+    gprog.q_slot = d_g_qslot.p;
+    gprog.q_body = d_g_qbody.p;
+    gprog.kmu = model.radial_funcs;
+    gprog.nbody = g.body_count;
+    gprog.mode = g.mode == GateMode::MuBodyLinearCombo ? 1 : 2;
+    gprog.amplitude = g.amplitude;
+    gprog.weights = d_g_w.p;
+    gprog.body_mix = d_g_mix.p;
+    gprog.additive = d_g_add.p;
   }
 
   ProgramDev program_dev() const {
@@ -700,37 +788,38 @@ struct Engine {
 
   // k_basic / k_force through the ahead-of-time build or the NVRTC module.
   template <typename T>
-  void run_basic(cudaStream_t s, const EdgeArgs<T>& a, int block) {
+  void run_basic(cudaStream_t s, const EdgeArgs<T>& a, void* out, bool gated, int block) {
     if (edge_jit) {
       std::string err;
       if (!ejit_mod.load(*ejit_bin, &err) ||
-          !ejit_mod.launch_basic(s, a.N, 128, edge_smem<T>(), &a, Bbuf.p, &err))
+          !ejit_mod.launch_basic(s, a.N, 128, edge_smem<T>(), &a, out, gated, &err))
         throw CudaError(err);
       return;
     }
-    if (launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block) != 0)
+    if (launch_basic<T>(s, a, reinterpret_cast<T*>(out), gated ? 128 : block, gated) != 0)
       throw InputError("SUS2_SH basic kernel shape not compiled.");
   }
 
   template <typename T>
-  void run_force(cudaStream_t s, const EdgeArgs<T>& a, const double* weight, double* force, double* virial,
-                 double sign, int block) {
+  void run_force(cudaStream_t s, const EdgeArgs<T>& a, const void* G, bool gated, const double* weight,
+                 double* force, double* virial, double sign, int block) {
     if (edge_jit) {
       std::string err;
       if (!ejit_mod.load(*ejit_bin, &err) ||
-          !ejit_mod.launch_force(s, a.N, 128, edge_smem<T>(), &a, Gbuf.p, weight, ftmp.p, force, virial, sign,
+          !ejit_mod.launch_force(s, a.N, 128, edge_smem<T>(), &a, G, weight, ftmp.p, force, virial, sign, gated,
                                  &err))
         throw CudaError(err);
       return;
     }
-    if (launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), weight, ftmp.p, force, virial, sign, block) != 0)
+    if (launch_force<T>(s, a, reinterpret_cast<const T*>(G), weight, ftmp.p, force, virial, sign,
+                        gated ? 128 : block, gated) != 0)
       throw InputError("SUS2_SH force kernel shape not compiled.");
   }
 
   template <typename T>
   void autotune(cudaStream_t s, const EdgeArgs<T>& a) {
     tuned = true;
-    if (!opt.autotune || sizeof(T) != 4 || edge_jit) return;
+    if (!opt.autotune || sizeof(T) != 4 || edge_jit || gate) return;
     DevBuf<double> f_scratch, w_scratch;
     f_scratch.resize(3ull * N);
     w_scratch.resize(9ull * N);
@@ -750,7 +839,7 @@ struct Engine {
     };
     float best_b = 1e30f, best_f = 1e30f;
     for (int block : {64, 128, 256}) {
-      const float tb = time_it([&] { launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block); });
+      const float tb = time_it([&] { launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block, false); });
       const float tf = time_it([&] {
         launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), nullptr, ftmp.p, f_scratch.p, w_scratch.p, 1.0,
                         block);
@@ -772,10 +861,20 @@ struct Engine {
 
   template <typename T>
   void forward_impl(cudaStream_t s, double* pe, int pe_assign, EvSet* ev = nullptr) {
-    const EdgeArgs<T> a = edge_args<T>();
+    EdgeArgs<T> a = edge_args<T>();
     if (!tuned) autotune<T>(s, a);
     mark(ev, 1, s);
-    run_basic<T>(s, a, basic_block);
+    if (gate) {
+      const EdgeArgs<T> ag = edge_args_gate<T>();
+      run_basic<T>(s, ag, Bg.p, false, basic_block);
+      launch_gate_forward<T>(s, N, gprog, pos4.p, reinterpret_cast<const T*>(Bg.p), reinterpret_cast<T*>(gslots.p),
+                             reinterpret_cast<T*>(gmult.p), reinterpret_cast<T*>(gderiv.p));
+      a.gate_mult = reinterpret_cast<const T*>(gmult.p);
+      run_basic<T>(s, a, Bbuf.p, true, 128);
+      launches += 3;
+    } else {
+      run_basic<T>(s, a, Bbuf.p, false, basic_block);
+    }
     mark(ev, 2, s);
     if (!cg_bin.cubin.empty()) {
       std::string err;
@@ -799,10 +898,27 @@ struct Engine {
   template <typename T>
   void backward_impl(cudaStream_t s, const double* weight, double* force, double* virial, double sign,
                      EvSet* ev = nullptr) {
-    const EdgeArgs<T> a = edge_args<T>();
+    EdgeArgs<T> a = edge_args<T>();
     ck(cudaMemsetAsync(ftmp.p, 0, ftmp.n, s), "memset");
     mark(ev, 3, s);
-    run_force<T>(s, a, weight, force, virial, sign, force_block);
+    if (gate) {
+      // main pass (gate multipliers, dE/dh), gate back-propagation, first-layer
+      // pass; the per-atom weights are folded into dE/dh by the main pass
+      ck(cudaMemsetAsync(gadj.p, 0, gadj.n, s), "memset");
+      ck(cudaMemsetAsync(Gg.p, 0, Gg.n, s), "memset");
+      a.gate_mult = reinterpret_cast<const T*>(gmult.p);
+      a.gate_deriv = reinterpret_cast<const T*>(gderiv.p);
+      a.gate_adj = reinterpret_cast<T*>(gadj.p);
+      run_force<T>(s, a, Gbuf.p, true, weight, force, virial, sign, 128);
+      T* M = reinterpret_cast<T*>(gslots.p);
+      launch_gate_backward<T>(s, N, gprog, M, M + static_cast<size_t>(gprog.nslots) * N,
+                              reinterpret_cast<const T*>(gadj.p), reinterpret_cast<T*>(Gg.p));
+      const EdgeArgs<T> ag = edge_args_gate<T>();
+      run_force<T>(s, ag, Gg.p, false, nullptr, force, virial, sign, force_block);
+      launches += 2;
+    } else {
+      run_force<T>(s, a, Gbuf.p, false, weight, force, virial, sign, force_block);
+    }
     if (model.zbl_enabled) {
       launch_zbl(s, 1, N, cap, pos4.p, nbr.p, ncount.p, a.shift, a.atom_cell, zbl_tables(), weight, nullptr, force,
                  virial, sign);
@@ -817,6 +933,7 @@ struct Engine {
   // dL/dw and dL/dc of a loss with upstream weights ew = dL/dE_i, fw = dL/dF_i.
   template <typename T>
   void param_grad_impl(cudaStream_t s, const double* ew, const double* fw, double* grad_w, double* grad_c) {
+    if (gate) throw InputError("SUS2_SH parameter gradients do not cover two-layer gate models.");
     const size_t nb = static_cast<size_t>(prog.ncanon) * N;
     const size_t work = 4ull * model.moments * N;
     pg_buf.resize((4 * nb + work) * sizeof(T));
@@ -1134,7 +1251,7 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[30] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[31] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
@@ -1144,8 +1261,9 @@ int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
                      e.cg_bin.cubin.empty() ? 0 : 1, e.cg_bin.registers, static_cast<int>(e.cg_compile_ms),
                      e.basic_block, e.force_block, e.edge_jit ? 1 : 0,
                      e.ejit_bin ? e.ejit_bin->basic_registers : -1, e.ejit_bin ? e.ejit_bin->force_registers : -1,
-                     e.ejit_bin ? static_cast<int>(e.ejit_bin->compile_ms) : 0};
-  const int k = std::min(n, 30);
+                     e.ejit_bin ? static_cast<int>(e.ejit_bin->compile_ms) : 0,
+                     e.gate ? static_cast<int>(e.model.gate.mode) : 0};
+  const int k = std::min(n, 31);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -1290,7 +1408,7 @@ int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_r
   return guarded([&] {
     if (l_max < 0 || l_max > 6 || k_max <= 0 || k_max * (l_max + 1) > 48 || rb <= 0 || rb > 16)
       throw sus2sh::InputError("SUS2_SH edge-kernel shape out of range.");
-    const auto bin = sus2sh::compile_edge_kernels(fp32 != 0, l_max, k_max, rb, 128);
+    const auto bin = sus2sh::compile_edge_kernels(fp32 != 0, l_max, k_max, rb, 128, false);
     if (basic_registers) *basic_registers = bin->basic_registers;
     if (force_registers) *force_registers = bin->force_registers;
     if (compile_ms) *compile_ms = bin->compile_ms;

@@ -32,6 +32,10 @@ struct EdgeArgs {
   const void* pair_table;   // T[S*S][pair_stride]
   const double (*shift)[3];  // image vectors [cells][125][3] (one box: BoxGeom::shift)
   const int* atom_cell;      // cell of each atom in a batch of boxes, NULL for one box
+  // two-layer gate models only (kernels instantiated with GATE = true):
+  const T* gate_mult;        // [Kmu][N] G_{j,mu} = 1 + A tanh(a_j h_{j,mu})
+  const T* gate_deriv;       // [Kmu][N] dG/dh
+  T* gate_adj;               // [Kmu][N] dE/dh accumulated by k_force (atomics)
   T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
 };
 

@@ -17,9 +17,9 @@ namespace {
 
 #include "edge_jit_sources.inc"
 
-std::string shape_key(bool fp32, int l, int k, int rb, int block) {
+std::string shape_key(bool fp32, int l, int k, int rb, int block, bool gate) {
   return std::string(fp32 ? "f" : "d") + "/" + std::to_string(l) + "/" + std::to_string(k) + "/" +
-         std::to_string(rb) + "/" + std::to_string(block);
+         std::to_string(rb) + "/" + std::to_string(block) + (gate ? "/gate" : "");
 }
 
 // "Used N registers" following "Compiling entry function '<name>'" in the
@@ -32,13 +32,17 @@ int registers_of(const std::string& log, const std::string& name) {
   return std::atoi(log.c_str() + u + 5);
 }
 
-std::shared_ptr<const EdgeJitBinary> build(bool fp32, int l, int k, int rb, int block) {
+std::shared_ptr<const EdgeJitBinary> build(bool fp32, int l, int k, int rb, int block, bool gate) {
   const auto t0 = std::chrono::steady_clock::now();
   const std::string T = fp32 ? "float" : "double";
   const std::string targs = "<" + T + ", " + std::to_string(l) + ", " + std::to_string(k) + ", " +
                             std::to_string(rb) + ", " + std::to_string(block) + ">";
   const std::string basic_expr = "&sus2sh::edge::k_basic" + targs;
   const std::string force_expr = "&sus2sh::edge::k_force" + targs;
+  const std::string gargs = "<" + T + ", " + std::to_string(l) + ", " + std::to_string(k) + ", " +
+                            std::to_string(rb) + ", 128, true>";
+  const std::string basic_gate_expr = "&sus2sh::edge::k_basic" + gargs;
+  const std::string force_gate_expr = "&sus2sh::edge::k_force" + gargs;
   const char* src = "#include \"edge_kernels.cuh\"\n";
   nvrtcProgram prog;
   if (nvrtcCreateProgram(&prog, src, "sus2sh_edge.cu", kJitHeaderCount, kJitHeaderSources, kJitHeaderNames) !=
@@ -46,6 +50,10 @@ std::shared_ptr<const EdgeJitBinary> build(bool fp32, int l, int k, int rb, int 
     throw InputError("NVRTC could not create the edge-kernel program.");
   nvrtcAddNameExpression(prog, basic_expr.c_str());
   nvrtcAddNameExpression(prog, force_expr.c_str());
+  if (gate) {
+    nvrtcAddNameExpression(prog, basic_gate_expr.c_str());
+    nvrtcAddNameExpression(prog, force_gate_expr.c_str());
+  }
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=true", "--ptxas-options=--verbose",
                         "--generate-line-info"};
   const nvrtcResult rc = nvrtcCompileProgram(prog, 5, opts);
@@ -66,6 +74,14 @@ std::shared_ptr<const EdgeJitBinary> build(bool fp32, int l, int k, int rb, int 
   lowered = nullptr;
   nvrtcGetLoweredName(prog, force_expr.c_str(), &lowered);
   out->force_name = lowered ? lowered : "";
+  if (gate) {
+    lowered = nullptr;
+    nvrtcGetLoweredName(prog, basic_gate_expr.c_str(), &lowered);
+    out->basic_gate_name = lowered ? lowered : "";
+    lowered = nullptr;
+    nvrtcGetLoweredName(prog, force_gate_expr.c_str(), &lowered);
+    out->force_gate_name = lowered ? lowered : "";
+  }
   size_t n = 0;
   nvrtcGetCUBINSize(prog, &n);
   out->cubin.resize(n);
@@ -80,16 +96,17 @@ std::shared_ptr<const EdgeJitBinary> build(bool fp32, int l, int k, int rb, int 
 
 }  // namespace
 
-std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block) {
+std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block,
+                                                          bool gate) {
   static std::mutex mu;
   static std::map<std::string, std::shared_ptr<const EdgeJitBinary>> cache;
-  const std::string key = shape_key(fp32, l_max, k_max, rb, block);
+  const std::string key = shape_key(fp32, l_max, k_max, rb, block, gate);
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
   }
-  auto bin = build(fp32, l_max, k_max, rb, block);
+  auto bin = build(fp32, l_max, k_max, rb, block, gate);
   std::lock_guard<std::mutex> lock(mu);
   return cache.emplace(key, bin).first->second;
 }
@@ -116,9 +133,13 @@ bool EdgeJitModule::load(const EdgeJitBinary& bin, std::string* err) {
     if (err) *err = "cuModuleLoadData failed for the edge kernels";
     return false;
   }
-  CUfunction fb = nullptr, ff = nullptr;
-  if (get_fn(&fb, mod, bin.basic_name.c_str()) != CUDA_SUCCESS ||
-      get_fn(&ff, mod, bin.force_name.c_str()) != CUDA_SUCCESS) {
+  CUfunction fb = nullptr, ff = nullptr, gb = nullptr, gf = nullptr;
+  bool ok = get_fn(&fb, mod, bin.basic_name.c_str()) == CUDA_SUCCESS &&
+            get_fn(&ff, mod, bin.force_name.c_str()) == CUDA_SUCCESS;
+  if (ok && !bin.basic_gate_name.empty())
+    ok = get_fn(&gb, mod, bin.basic_gate_name.c_str()) == CUDA_SUCCESS &&
+         get_fn(&gf, mod, bin.force_gate_name.c_str()) == CUDA_SUCCESS;
+  if (!ok) {
     if (auto unload = entry<PFN_unload>("cuModuleUnload")) unload(mod);
     if (err) *err = "cuModuleGetFunction failed for the edge kernels";
     return false;
@@ -126,6 +147,8 @@ bool EdgeJitModule::load(const EdgeJitBinary& bin, std::string* err) {
   module_ = mod;
   basic_ = fb;
   force_ = ff;
+  basic_gate_ = gb;
+  force_gate_ = gf;
   return true;
 }
 
@@ -141,17 +164,18 @@ bool EdgeJitModule::set_smem(void* fn, size_t smem, int* have, std::string* err)
   return true;
 }
 
-bool EdgeJitModule::launch_basic(void* stream, int N, int block, size_t smem, const void* args, void* B,
+bool EdgeJitModule::launch_basic(void* stream, int N, int block, size_t smem, const void* args, void* B, bool gate,
                                  std::string* err) {
   static PFN_launch launch_fn = entry<PFN_launch>("cuLaunchKernel");
-  if (!launch_fn || !basic_) {
+  void* fn = gate ? basic_gate_ : basic_;
+  if (!launch_fn || !fn) {
     if (err) *err = "edge kernels not loaded";
     return false;
   }
-  if (!set_smem(basic_, smem, &basic_smem_, err)) return false;
+  if (!set_smem(fn, smem, gate ? &basic_gate_smem_ : &basic_smem_, err)) return false;
   void* params[] = {const_cast<void*>(args), &B};
   const unsigned grid = static_cast<unsigned>((N + block - 1) / block);
-  if (launch_fn(static_cast<CUfunction>(basic_), grid, 1, 1, static_cast<unsigned>(block), 1, 1,
+  if (launch_fn(static_cast<CUfunction>(fn), grid, 1, 1, static_cast<unsigned>(block), 1, 1,
                 static_cast<unsigned>(smem), static_cast<CUstream>(stream), params, nullptr) != CUDA_SUCCESS) {
     if (err) *err = "cuLaunchKernel failed for k_basic";
     return false;
@@ -161,16 +185,17 @@ bool EdgeJitModule::launch_basic(void* stream, int N, int block, size_t smem, co
 
 bool EdgeJitModule::launch_force(void* stream, int N, int block, size_t smem, const void* args, const void* G,
                                  const double* weight, void* ftmp, double* force, double* virial, double sign,
-                                 std::string* err) {
+                                 bool gate, std::string* err) {
   static PFN_launch launch_fn = entry<PFN_launch>("cuLaunchKernel");
-  if (!launch_fn || !force_) {
+  void* fn = gate ? force_gate_ : force_;
+  if (!launch_fn || !fn) {
     if (err) *err = "edge kernels not loaded";
     return false;
   }
-  if (!set_smem(force_, smem, &force_smem_, err)) return false;
+  if (!set_smem(fn, smem, gate ? &force_gate_smem_ : &force_smem_, err)) return false;
   void* params[] = {const_cast<void*>(args), &G, &weight, &ftmp, &force, &virial, &sign};
   const unsigned grid = static_cast<unsigned>((N + block - 1) / block);
-  if (launch_fn(static_cast<CUfunction>(force_), grid, 1, 1, static_cast<unsigned>(block), 1, 1,
+  if (launch_fn(static_cast<CUfunction>(fn), grid, 1, 1, static_cast<unsigned>(block), 1, 1,
                 static_cast<unsigned>(smem), static_cast<CUstream>(stream), params, nullptr) != CUDA_SUCCESS) {
     if (err) *err = "cuLaunchKernel failed for k_force";
     return false;

@@ -14,15 +14,17 @@ namespace sus2sh {
 struct EdgeJitBinary {
   std::vector<char> cubin;
   std::string basic_name, force_name;  // lowered (mangled) kernel names
+  std::string basic_gate_name, force_gate_name;  // GATE variants (gate models only)
   std::string log;                     // NVRTC + ptxas report
   int basic_registers = -1, force_registers = -1;
   double compile_ms = 0.0;
 };
 
 // Compiles k_basic<T, L, K, RB, BLOCK> and k_force<...> (T = float if fp32,
-// else double).  Results are cached for the life of the process; throws
+// else double), and their GATE variants when gate is set.  Results are cached for the life of the process; throws
 // InputError with the compiler log on failure.
-std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block);
+std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block,
+                                                          bool gate);
 
 // Module of one compiled shape, loaded into the current context.
 class EdgeJitModule {
@@ -34,9 +36,10 @@ class EdgeJitModule {
   bool load(const EdgeJitBinary& bin, std::string* err);
   bool loaded() const { return basic_ != nullptr; }
   // args: pointer to the host EdgeArgs<T> passed by value to the kernel.
-  bool launch_basic(void* stream, int N, int block, size_t smem, const void* args, void* B, std::string* err);
+  bool launch_basic(void* stream, int N, int block, size_t smem, const void* args, void* B, bool gate,
+                    std::string* err);
   bool launch_force(void* stream, int N, int block, size_t smem, const void* args, const void* G,
-                    const double* weight, void* ftmp, double* force, double* virial, double sign,
+                    const double* weight, void* ftmp, double* force, double* virial, double sign, bool gate,
                     std::string* err);
 
  private:
@@ -44,7 +47,10 @@ class EdgeJitModule {
   void* module_ = nullptr;
   void* basic_ = nullptr;
   void* force_ = nullptr;
-  int basic_smem_ = 48 * 1024, force_smem_ = 48 * 1024;
+  void* basic_gate_ = nullptr;
+  void* force_gate_ = nullptr;
+  int basic_smem_ = 48 * 1024, force_smem_ = 48 * 1024, basic_gate_smem_ = 48 * 1024,
+      force_gate_smem_ = 48 * 1024;
 };
 
 }  // namespace sus2sh

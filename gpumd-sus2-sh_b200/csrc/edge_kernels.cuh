@@ -32,7 +32,9 @@ namespace edge {
 // ---------------------------------------------------------------------------
 // basic moments
 // ---------------------------------------------------------------------------
-template <typename T, int L, int K, int RB, int BLOCK>
+// GATE: two-layer gate models' main pass, every R_mu of neighbour j scaled by
+// the gate multiplier G_{j,mu} (gpu_sh_compute_basic_gate_main, sus2_sh.cu:4247-4314).
+template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
 __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK : 1) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_tab = reinterpret_cast<T*>(smem_raw);
@@ -65,6 +67,11 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_BASIC_MIN_BLOCKS
     const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
     T R[KMU];
     radial_values<T, KMU, RB>(a, row, e, R);
+    if constexpr (GATE) {
+      const int j = w & 0xFFFFFF;
+#pragma unroll
+      for (int mu = 0; mu < KMU; ++mu) R[mu] *= a.gate_mult[static_cast<size_t>(mu) * a.N + j];
+    }
     T Y[C];
     sh_values<L>(e.ux, e.uy, e.uz, Y);
 #pragma unroll
@@ -100,7 +107,11 @@ struct Scatter<double> {
   }
 };
 
-template <typename T, int L, int K, int RB, int BLOCK>
+// GATE: the main pass of a gate model (gpu_sh_compute_forces_gate_main_cached_grads,
+// sus2_sh.cu:6555-6693 with compute_sh_edge_derivative_gate_main_cached_grads
+// :6077-6121): R, R' scaled by G_{j,mu}, and dE/dh_{j,mu} += dG/dh_{j,mu}
+// R_mu sum_m g_{mu,m} Y_m accumulated on the neighbour.
+template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
 __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK : 1)
     k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
             void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
@@ -144,6 +155,22 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS
     radial_values_ders<T, KMU, RB>(a, row, e, R, dR);
     T Y[C];
     sh_values<L>(e.ux, e.uy, e.uz, Y);
+    if constexpr (GATE) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int l = 0; l <= L; ++l) {
+          const int mu = k * (L + 1) + l;
+          T p = T(0);
+#pragma unroll
+          for (int m = 0; m <= 2 * l; ++m) p = fma(g[k * C + l * l + m], Y[l * l + m], p);
+          const size_t at = static_cast<size_t>(mu) * a.N + j;
+          atomicAdd(a.gate_adj + at, p * R[mu] * a.gate_deriv[at]);
+          const T gm = a.gate_mult[at];
+          R[mu] *= gm;
+          dR[mu] *= gm;
+        }
+    }
     T Gy[C];
     T s = T(0);
 #pragma unroll

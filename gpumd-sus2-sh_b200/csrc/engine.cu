@@ -573,8 +573,13 @@ void allow_smem(K kernel, size_t bytes) {
 }
 
 template <typename T, int L, int K, int RB>
-int launch_basic_shape(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
+int launch_basic_shape(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block, bool gate) {
   const size_t sm = pair_smem(a);
+  if (gate) {  // gate models: 128-thread CTAs only
+    allow_smem(k_basic<T, L, K, RB, 128, true>, sm);
+    k_basic<T, L, K, RB, 128, true><<<blocks_for(a.N, 128), 128, sm, s>>>(a, B);
+    return 0;
+  }
   allow_smem(k_basic<T, L, K, RB, 64>, sm);
   allow_smem(k_basic<T, L, K, RB, 128>, sm);
   allow_smem(k_basic<T, L, K, RB, 256>, sm);
@@ -590,8 +595,13 @@ int launch_basic_shape(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
 
 template <typename T, int L, int K, int RB>
 int launch_force_shape(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight, void* ftmp,
-                       double* force, double* virial, double sign, int block) {
+                       double* force, double* virial, double sign, int block, bool gate) {
   const size_t sm = pair_smem(a);
+  if (gate) {
+    allow_smem(k_force<T, L, K, RB, 128, true>, sm);
+    k_force<T, L, K, RB, 128, true><<<blocks_for(a.N, 128), 128, sm, s>>>(a, G, weight, ftmp, force, virial, sign);
+    return 0;
+  }
   allow_smem(k_force<T, L, K, RB, 64>, sm);
   allow_smem(k_force<T, L, K, RB, 128>, sm);
   allow_smem(k_force<T, L, K, RB, 256>, sm);
@@ -606,9 +616,9 @@ int launch_force_shape(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const d
 }
 
 template <typename T>
-int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
+int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block, bool gate) {
 #define SUS2_BASIC(L, K, RB) \
-  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) return launch_basic_shape<T, L, K, RB>(s, a, B, block);
+  if (a.l_max == L && a.k_max == K && a.rs.rb == RB) return launch_basic_shape<T, L, K, RB>(s, a, B, block, gate);
   SUS2_SHAPES(SUS2_BASIC)
 #undef SUS2_BASIC
   return -1;
@@ -616,10 +626,10 @@ int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block) {
 
 template <typename T>
 int launch_force(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight, void* ftmp,
-                 double* force, double* virial, double sign, int block) {
+                 double* force, double* virial, double sign, int block, bool gate) {
 #define SUS2_FORCE(L, K, RB)                                                                         \
   if (a.l_max == L && a.k_max == K && a.rs.rb == RB)                                                 \
-    return launch_force_shape<T, L, K, RB>(s, a, G, weight, ftmp, force, virial, sign, block);
+    return launch_force_shape<T, L, K, RB>(s, a, G, weight, ftmp, force, virial, sign, block, gate);
   SUS2_SHAPES(SUS2_FORCE)
 #undef SUS2_FORCE
   return -1;
@@ -666,12 +676,12 @@ void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_ty
   k_kick<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel);
 }
 
-template int launch_basic<float>(cudaStream_t, const EdgeArgs<float>&, float*, int);
-template int launch_basic<double>(cudaStream_t, const EdgeArgs<double>&, double*, int);
+template int launch_basic<float>(cudaStream_t, const EdgeArgs<float>&, float*, int, bool);
+template int launch_basic<double>(cudaStream_t, const EdgeArgs<double>&, double*, int, bool);
 template int launch_force<float>(cudaStream_t, const EdgeArgs<float>&, const float*, const double*, void*,
-                                 double*, double*, double, int);
+                                 double*, double*, double, int, bool);
 template int launch_force<double>(cudaStream_t, const EdgeArgs<double>&, const double*, const double*, void*,
-                                  double*, double*, double, int);
+                                  double*, double*, double, int, bool);
 template void launch_product<float>(cudaStream_t, int, const ProgramDev&, const double4*, const float*, float*,
                                     float*, size_t, int, const double*, const double*, double*, int);
 template void launch_product<double>(cudaStream_t, int, const ProgramDev&, const double4*, const double*,

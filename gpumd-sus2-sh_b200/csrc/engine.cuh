@@ -90,13 +90,42 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
                   int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
                   int cap, int count_only, Status* st);
 
-// Edge kernels with CTA size `block` (64, 128 or 256 for FP32; 128 for FP64).
+// Edge kernels with CTA size `block` (64, 128 or 256 for FP32; 128 for FP64);
+// gate = true selects the gate-model main-pass variants (128 only).
 template <typename T>
-int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block);
+int launch_basic(cudaStream_t s, const EdgeArgs<T>& a, T* B, int block, bool gate = false);
 template <typename T>
 int launch_force(cudaStream_t s, const EdgeArgs<T>& a, const T* G, const double* weight,
-                 void* ftmp, double* force, double* virial, double sign, int block);
+                 void* ftmp, double* force, double* virial, double sign, int block, bool gate = false);
 bool block_supported(int block, bool fp32);
+
+// Two-layer gate: the first-layer graph program (needed moments only) and the
+// signal -> multiplier map (gate.cu).
+struct GateProgDev {
+  int nslots;             // needed moments; basics first
+  int nbasic;             // needed basics: slot b <-> canonical row basic_canon[b]
+  const int* basic_canon;
+  int nprod;              // needed products in file order
+  const int* prod;        // [nprod][3] left, right, target slot
+  const double* coef;     // [nprod]
+  int nq;                 // gate scalars
+  const int* q_slot;      // [nq]
+  const int* q_body;      // [nq]
+  int kmu, nbody, mode;   // mode 1 mu-body-linear-combo, 2 mu-scalar-full
+  double amplitude;
+  const double* weights;  // full [kmu][nq], combo [nq]
+  const double* body_mix; // combo [kmu][nbody]
+  const double* additive; // [S]
+};
+// Gate signals from the first-layer basics Bg: slots M (value scratch
+// [nslots][N]), G and dG/dh ([kmu][N]).
+template <typename T>
+void launch_gate_forward(cudaStream_t s, int N, const GateProgDev& p, const double4* pos4, const T* Bg, T* M,
+                         T* gmult, T* gderiv);
+// dE/dh ([kmu][N]) -> first-layer basic adjoints Gg (canonical rows, written
+// for the needed basics; the caller zeroes Gg), grads scratch gM [nslots][N].
+template <typename T>
+void launch_gate_backward(cudaStream_t s, int N, const GateProgDev& p, const T* M, T* gM, const T* adjh, T* Gg);
 // Sums per-atom energy and virial into out[0] and out[1..9] (FP64 atomics).
 void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial, double* out);
 template <typename T>

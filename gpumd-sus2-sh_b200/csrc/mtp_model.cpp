@@ -154,6 +154,132 @@ bool is_sus2_sh_file(const std::string& path) {
 // Reader (load_sh_model, sus2_sh.cu:2105-2482).  The two-layer gate and ZBL
 // fields are outside this engine and are rejected explicitly.
 // ---------------------------------------------------------------------------
+namespace {
+// Gate keys (sus2_sh.cu:2153-2268), validated in the reference's order with its
+// messages.  Only the neighbour-site, shared-radial mu-body modes exist.
+void parse_gate(const std::string& text, HostModel& m) {
+  GateModel& g = m.gate;
+  g.enabled = true;
+  std::string mode = contains(text, "two_layer_gate_mode =") ? value_of(text, "two_layer_gate_mode =") : "legacy";
+  if (mode == "mu-body-linear-combo") {
+    g.mode = GateMode::MuBodyLinearCombo;
+  } else if (mode == "mu-scalar-full" || mode == "mu-body-order") {
+    g.mode = GateMode::MuScalarFull;
+  } else if (mode == "legacy") {
+    throw InputError(
+        "GPUMD SUS2_SH mu-body-order branch requires two_layer_gate_mode = "
+        "mu-body-linear-combo or mu-scalar-full; legacy gate models are not supported here.");
+  } else {
+    throw InputError("Unsupported SUS2_SH two_layer_gate_mode in GPUMD: " + mode);
+  }
+  if (contains(text, "two_layer_gate_include_one_body =") &&
+      parse_bool(value_of(text, "two_layer_gate_include_one_body ="), "two_layer_gate_include_one_body ="))
+    throw InputError("GPUMD SUS2_SH gate backend requires two_layer_gate_include_one_body = false.");
+  if (contains(text, "two_layer_gate_scale_mode ="))
+    throw InputError("GPUMD SUS2_SH mu-body gate does not support two_layer_gate_scale_mode.");
+  if (contains(text, "two_layer_gate_bias ="))
+    throw InputError("GPUMD SUS2_SH mu-body gate does not support two_layer_gate_bias.");
+  if (contains(text, "two_layer_residual_enabled =") &&
+      parse_bool(value_of(text, "two_layer_residual_enabled ="), "two_layer_residual_enabled ="))
+    throw InputError("GPUMD SUS2_SH mu-body gate does not support residual gate fields.");
+  if (contains(text, "two_layer_gate_site_mode =")) {
+    const std::string site = value_of(text, "two_layer_gate_site_mode =");
+    if (site == "double")
+      throw InputError(
+          "GPUMD SUS2_SH mu-body gate currently supports two_layer_gate_site_mode = neighbor. "
+          "Double-site gate will be added after the single-gate CUDA path is verified.");
+    if (site != "neighbor") throw InputError("Unsupported SUS2_SH two_layer_gate_site_mode in GPUMD: " + site);
+  }
+  if (contains(text, "two_layer_gate_tanh_amplitude ="))
+    g.amplitude = double_of(text, "two_layer_gate_tanh_amplitude =");
+  if (!std::isfinite(g.amplitude) || g.amplitude < 0.0 || g.amplitude > 1.0)
+    throw InputError("SUS2_SH two_layer_gate_tanh_amplitude should be finite and in [0,1].");
+  const std::string radial_mode =
+      contains(text, "two_layer_gate_radial_mode =") ? value_of(text, "two_layer_gate_radial_mode =") : "";
+  if (radial_mode != "shared-radial")
+    throw InputError("GPUMD SUS2_SH gate backend currently requires shared-radial gate mode.");
+  const int body_max = int_of(text, "two_layer_gate_body_order_max =");
+  if (body_max != m.k_max + 1) throw InputError("SUS2_SH two_layer_gate_body_order_max should equal sh_k_max + 1.");
+  g.body_count = body_max - 1;
+  const int radial_count = int_of(text, "two_layer_gate_radial_coeff_count =");
+  if (radial_count != m.radial_funcs * m.rb_size)
+    throw InputError("SUS2_SH two-layer gate radial coefficient count is inconsistent.");
+  g.radial_coeffs = numbers<double>(braced(text, "two_layer_gate_radial_coeffs ="));
+  if (static_cast<int>(g.radial_coeffs.size()) != radial_count)
+    throw InputError("SUS2_SH two-layer gate radial coeff list has wrong size.");
+  if (contains(text, "two_layer_gate_additive_coeff_count =")) {
+    const int n = int_of(text, "two_layer_gate_additive_coeff_count =");
+    if (n != m.species_count) throw InputError("SUS2_SH two-layer gate additive coefficient count is inconsistent.");
+    g.additive = numbers<double>(braced(text, "two_layer_gate_additive_coeffs ="));
+    if (static_cast<int>(g.additive.size()) != n)
+      throw InputError("SUS2_SH two-layer gate additive coeff list has wrong size.");
+  } else {
+    g.additive.assign(m.species_count, 1.0);
+  }
+  const int weight_count = int_of(text, "two_layer_gate_weight_count =");
+  if (weight_count <= 0) throw InputError("SUS2_SH two-layer gate should contain at least one scalar weight.");
+  g.scalar_indices = numbers<int>(braced(text, "two_layer_gate_scalar_indices ="));
+  g.weights = numbers<double>(braced(text, "two_layer_gate_weights ="));
+  const int nq = static_cast<int>(g.scalar_indices.size());
+  if (nq <= 0) throw InputError("SUS2_SH two-layer gate scalar index list is empty.");
+  const int expected = g.mode == GateMode::MuScalarFull ? m.radial_funcs * nq : nq;
+  if (weight_count != expected || static_cast<int>(g.weights.size()) != expected)
+    throw InputError("SUS2_SH two-layer gate scalar index/weight dimensions are inconsistent.");
+  if (g.mode == GateMode::MuBodyLinearCombo) {
+    const int n = int_of(text, "two_layer_gate_body_mix_weight_count =");
+    if (n != m.radial_funcs * g.body_count)
+      throw InputError("SUS2_SH two-layer gate body-mix weight count is inconsistent.");
+    g.body_mix = numbers<double>(braced(text, "two_layer_gate_body_mix_weights ="));
+    if (static_cast<int>(g.body_mix.size()) != n)
+      throw InputError("SUS2_SH two-layer gate body-mix weight list has wrong size.");
+  } else if (contains(text, "two_layer_gate_body_mix_weights =") ||
+             contains(text, "two_layer_gate_body_mix_weight_count =")) {
+    throw InputError("SUS2_SH mu-scalar-full gate should not contain body-mix weights.");
+  }
+}
+
+// Gate scalar -> moment and body bucket, the moments the gate signals need and
+// the last product that can feed one (sus2_sh.cu:2412-2478).
+void gate_metadata(HostModel& m) {
+  GateModel& g = m.gate;
+  const int nq = static_cast<int>(g.scalar_indices.size());
+  g.moment_of.assign(nq, 0);
+  g.body_of.assign(nq, 0);
+  g.needed.assign(m.moments, 0);
+  std::vector<unsigned char> present(g.body_count, 0);
+  for (int q = 0; q < nq; ++q) {
+    const int s = g.scalar_indices[q];
+    if (s < 0 || s >= m.scalar_count) throw InputError("SUS2_SH two-layer gate scalar index is out of range.");
+    const int body = m.scalar_body[s] - 2;
+    if (body < 0 || body >= g.body_count)
+      throw InputError("SUS2_SH two-layer gate scalar body order is outside the gate range.");
+    g.body_of[q] = body;
+    present[body] = 1;
+    const int mom = m.moment_mapping[s];
+    if (mom < 0 || mom >= m.moments) throw InputError("SUS2_SH two-layer gate mapped moment index is out of range.");
+    g.moment_of[q] = mom;
+    bool effective = false;
+    if (g.mode == GateMode::MuScalarFull) {
+      for (int mu = 0; mu < m.radial_funcs && !effective; ++mu) effective = g.weights[mu * nq + q] != 0.0;
+    } else if (g.weights[q] != 0.0) {
+      for (int mu = 0; mu < m.radial_funcs && !effective; ++mu)
+        effective = g.body_mix[mu * g.body_count + body] != 0.0;
+    }
+    if (effective) g.needed[mom] = 1;
+  }
+  for (int b = 0; b < g.body_count; ++b)
+    if (!present[b]) throw InputError("SUS2_SH two-layer gate scalar list misses a required body-order bucket.");
+  g.product_limit = 0;
+  for (int p = static_cast<int>(m.products.size()) - 1; p >= 0; --p) {
+    const Product& pr = m.products[p];
+    if (!g.needed[pr.target]) continue;
+    g.needed[pr.left] = 1;
+    g.needed[pr.right] = 1;
+    if (g.product_limit == 0) g.product_limit = p + 1;
+  }
+}
+}  // namespace
+
 HostModel load_model(const std::string& path) {
   const std::string text = slurp(path);
   HostModel m;
@@ -198,8 +324,8 @@ HostModel load_model(const std::string& path) {
   m.basic_count = int_of(text, "alpha_index_basic_count =");
   m.scalar_count = int_of(text, "alpha_scalar_moments =");
   if (contains(text, "two_layer_gate_enabled =") &&
-      parse_bool(value_of(text, "two_layer_gate_enabled ="), "two_layer_gate_enabled"))
-    throw InputError("SUS2_SH two-layer gate models are not supported by this engine.");
+      parse_bool(value_of(text, "two_layer_gate_enabled ="), "two_layer_gate_enabled ="))
+    parse_gate(text, m);
 
   if (scaling_map != "LK") throw InputError("SUS2_SH requires scaling_map = LK.");
   if (m.l_max < 0 || m.l_max > 6)
@@ -264,6 +390,22 @@ HostModel load_model(const std::string& path) {
       throw InputError("SUS2_SH product index out of range.");
   }
 
+  if (contains(text, "sh_scalar_info_count =")) {
+    const int count = int_of(text, "sh_scalar_info_count =");
+    if (count != m.scalar_count) throw InputError("SUS2_SH sh_scalar_info_count should equal alpha_scalar_moments.");
+    const auto info = inner_groups(braced(text, "sh_scalar_info ="));
+    if (static_cast<int>(info.size()) != count) throw InputError("Unexpected SUS2_SH sh_scalar_info size.");
+    m.scalar_body.assign(count, 0);
+    for (int q = 0; q < count; ++q) {
+      const auto v = numbers<int>(info[q]);
+      if (v.empty()) throw InputError("Invalid SUS2_SH sh_scalar_info entry.");
+      if (v[0] < 2 || v[0] > m.body_order) throw InputError("SUS2_SH sh_scalar_info body order is out of range.");
+      m.scalar_body[q] = v[0];
+    }
+  } else if (m.gate.enabled) {
+    throw InputError("GPUMD SUS2_SH mu-body gate requires sh_scalar_info metadata.");
+  }
+
   m.radial_coeffs.assign(static_cast<size_t>(m.radial_funcs) * m.rb_size, 0.0);
   m.radial_type_coeffs.assign(m.species_count, 1.0);
   const size_t r0 = locate(text, "radial_coeffs");
@@ -287,6 +429,8 @@ HostModel load_model(const std::string& path) {
       static_cast<int>(m.moment_mapping.size()) != m.scalar_count ||
       static_cast<int>(m.moment_coeffs.size()) != m.scalar_count)
     throw InputError("Unexpected SUS2_SH coefficient dimensions.");
+
+  if (m.gate.enabled) gate_metadata(m);
 
   // Standard-graph match is informational (prepare_sh_graph_metadata,
   // sus2_sh.cu:2095-2103); execution always follows the saved products.
@@ -401,7 +545,10 @@ class GraphBuilder {
     StandardGraph g;
     for (const Spec& s : specs_) {
       const int node = build_scalar(s);
-      if (node >= 0) g.scalars.push_back(node);
+      if (node >= 0) {
+        g.scalars.push_back(node);
+        g.scalar_body.push_back(s.body);
+      }
     }
     for (const Product& p : products_)
       if (std::abs(p.coeff) >= 1.0e-12) g.products.push_back(p);
@@ -852,6 +999,9 @@ void write_synthetic_model(const std::string& path, const SynthSpec& sp) {
   std::fprintf(f, "}\n");
   std::fprintf(f, "alpha_scalar_moments = %d\nalpha_moment_mapping = {", static_cast<int>(g.scalars.size()));
   for (size_t s = 0; s < g.scalars.size(); ++s) std::fprintf(f, "%s%d", s ? ", " : "", g.scalars[s]);
+  std::fprintf(f, "}\n");
+  std::fprintf(f, "sh_scalar_info_count = %d\nsh_scalar_info = {", static_cast<int>(g.scalars.size()));
+  for (size_t s = 0; s < g.scalar_body.size(); ++s) std::fprintf(f, "%s{%d}", s ? ", " : "", g.scalar_body[s]);
   std::fprintf(f, "}\n");
   list("species_coeffs", std::vector<double>(S, 1.0));
   std::vector<double> w(g.scalars.size());

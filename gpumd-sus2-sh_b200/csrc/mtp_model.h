@@ -28,6 +28,25 @@ struct Product {
 
 enum class RadialMap { Tanh = 0, Rational = 1 };
 
+enum class GateMode { MuBodyLinearCombo = 1, MuScalarFull = 2 };
+
+struct GateModel {
+  bool enabled = false;
+  GateMode mode = GateMode::MuScalarFull;
+  double amplitude = 0.8;              // A in G = 1 + A tanh(a h)
+  int body_count = 0;                  // two_layer_gate_body_order_max - 1 (= K)
+  std::vector<double> radial_coeffs;   // [Kmu][rb] gate radial coefficients
+  std::vector<double> additive;        // [S] a per species of the gated atom
+  std::vector<int> scalar_indices;     // [Q] scalar ids
+  std::vector<double> weights;         // full: [Kmu][Q]; combo: [Q]
+  std::vector<double> body_mix;        // combo: [Kmu][body_count]
+  // derived
+  std::vector<int> moment_of;          // [Q] moment id of each gate scalar
+  std::vector<int> body_of;            // [Q] body id (body order - 2)
+  std::vector<unsigned char> needed;   // [moments] needed by the gate signals
+  int product_limit = 0;               // products [0, limit) can feed a needed moment
+};
+
 struct HostModel {
   int species_count = 0;
   int l_max = 0;
@@ -60,6 +79,11 @@ struct HostModel {
   bool zbl_typewise = false;
   double zbl_typewise_factor = 0.7;
   std::vector<int> zbl_atomic_numbers;  // empty: from the element symbols
+  // body order of each scalar (sh_scalar_info, sus2_sh.cu:2354-2378), empty if absent
+  std::vector<int> scalar_body;
+  // Two-layer mu-body gate (load_sh_model, sus2_sh.cu:2153-2268; metadata
+  // :2412-2478).  Neighbour site mode, shared radial (scal, shift) tables.
+  GateModel gate;
 };
 
 // Parses a SUS2-SH v1.1.0 .mtp file with the reference reader's semantics.
@@ -74,6 +98,7 @@ struct StandardGraph {
   std::vector<int> basic_k, basic_l, basic_m;
   std::vector<Product> products;
   std::vector<int> scalars;
+  std::vector<int> scalar_body;  // body order of each scalar
   int tensor_blocks = 0;
   int cg_blocks = 0;
   int cg_terms = 0;

@@ -73,3 +73,51 @@ def add_zbl(src: str, dst: str, atomic_numbers=None, inner=None, outer=None, typ
         fh.write(text.rstrip("\n") + "\n" + "\n".join(lines) + "\n")
     os.replace(dst + ".tmp", dst)
     return dst
+
+
+def add_gate(src: str, dst: str, mode: str = "mu-scalar-full", seed: int = 0, amplitude: float = 0.5,
+             radial_sigma: float = 0.1, weight_sigma: float = 0.002, mix_sigma: float = 1.0,
+             additive=None) -> str:
+    """Copies model ``src`` to ``dst`` as a two-layer mu-body gate model (keys of
+    load_sh_model, src/force/sus2_sh.cu:2153-2268): every scalar whose body
+    order is at most sh_k_max + 1 is a gate signal, gate radial coefficients
+    ~N(0, radial_sigma), signal weights ~N(0, weight_sigma), body-mix weights
+    ~N(0, mix_sigma) (mu-body-linear-combo), seeded."""
+    import re
+
+    import numpy as np
+
+    with open(src) as fh:
+        text = fh.read()
+
+    def value(key):
+        return re.search(re.escape(key) + r"\s*(\S+)", text).group(1)
+
+    K = int(value("sh_k_max ="))
+    L = int(value("sh_l_max ="))
+    rb = int(value("radial_basis_size ="))
+    S = int(value("species_count ="))
+    kmu = K * (L + 1)
+    info = re.search(r"sh_scalar_info = \{(.*)\}\s*$", text, re.M).group(1)
+    bodies = [int(b) for b in re.findall(r"\{(\d+)", info)]
+    qidx = [q for q, b in enumerate(bodies) if b <= K + 1]
+    rng = np.random.default_rng(seed)
+    fmt = lambda v: "{" + ", ".join(repr(float(x)) for x in v) + "}"  # noqa: E731
+    lines = ["two_layer_gate_enabled = 1", f"two_layer_gate_mode = {mode}", "two_layer_gate_site_mode = neighbor",
+             "two_layer_gate_radial_mode = shared-radial", f"two_layer_gate_tanh_amplitude = {amplitude!r}",
+             f"two_layer_gate_body_order_max = {K + 1}",
+             f"two_layer_gate_radial_coeff_count = {kmu * rb}",
+             "two_layer_gate_radial_coeffs = " + fmt(rng.normal(0.0, radial_sigma, kmu * rb))]
+    if additive is not None:
+        lines += [f"two_layer_gate_additive_coeff_count = {S}", "two_layer_gate_additive_coeffs = " + fmt(additive)]
+    nw = kmu * len(qidx) if mode != "mu-body-linear-combo" else len(qidx)
+    lines += [f"two_layer_gate_weight_count = {nw}",
+              "two_layer_gate_scalar_indices = {" + ", ".join(str(q) for q in qidx) + "}",
+              "two_layer_gate_weights = " + fmt(rng.normal(0.0, weight_sigma, nw))]
+    if mode == "mu-body-linear-combo":
+        lines += [f"two_layer_gate_body_mix_weight_count = {kmu * K}",
+                  "two_layer_gate_body_mix_weights = " + fmt(rng.normal(0.0, mix_sigma, kmu * K))]
+    with open(dst + ".tmp", "w") as fh:
+        fh.write(text.rstrip("\n") + "\n" + "\n".join(lines) + "\n")
+    os.replace(dst + ".tmp", dst)
+    return dst

@@ -183,7 +183,8 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * first evaluation; option sus2_sh_autotune=0 keeps 128) [26] edge kernels
  * compiled with NVRTC at load (shape without an ahead-of-time build, or
  * sus2_sh_edge_jit=1) [27] [28] their registers per thread (basic, force)
- * [29] their compile time (ms).  Returns the number written. */
+ * [29] their compile time (ms) [30] two-layer gate mode (0 none,
+ * 1 mu-body-linear-combo, 2 mu-scalar-full).  Returns the number written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

@@ -560,6 +560,10 @@ class MtpModel:
     zbl_typewise: bool = False
     zbl_typewise_factor: float = 0.7
     zbl_atomic_numbers: list = None
+    # body order of each scalar (sh_scalar_info, sus2_sh.cu:2354-2378)
+    scalar_body: list = None
+    # two-layer mu-body gate (sus2_sh.cu:2153-2268, metadata :2412-2478)
+    gate: dict = None
 
 
 def load_mtp(path: str) -> MtpModel:
@@ -673,6 +677,28 @@ def load_mtp(path: str) -> MtpModel:
         raise MtpError(str(exc)) from exc
     model = MtpModel(S, L, K, body, rtype, rational, max_dist, rb, kmu, M, Bb, nsc, scaling,
                      blmax, shift, scal, species, moment, mapping, basic, prods, radial, rtc)
+    gate = _parse_gate(text, K, kmu, rb, S) if ("two_layer_gate_enabled =" in text
+                                                and _bool(_after(text, "two_layer_gate_enabled ="))) else None
+    if "sh_scalar_info_count =" in text:
+        n = int(_after(text, "sh_scalar_info_count ="))
+        if n != nsc:
+            raise MtpError("SUS2_SH sh_scalar_info_count should equal alpha_scalar_moments.")
+        info = _top_groups(_braced(text, "sh_scalar_info ="))
+        if len(info) != n:
+            raise MtpError("Unexpected SUS2_SH sh_scalar_info size.")
+        model.scalar_body = []
+        for g in info:
+            v = _numbers(g, int)
+            if not v:
+                raise MtpError("Invalid SUS2_SH sh_scalar_info entry.")
+            if v[0] < 2 or v[0] > body:
+                raise MtpError("SUS2_SH sh_scalar_info body order is out of range.")
+            model.scalar_body.append(v[0])
+    elif gate is not None:
+        raise MtpError("GPUMD SUS2_SH mu-body gate requires sh_scalar_info metadata.")
+    if gate is not None:
+        _gate_metadata(model, gate)
+        model.gate = gate
     if "zbl_enabled =" in text and _bool(_after(text, "zbl_enabled =")):
         model.zbl_enabled = True
         if "zbl_inner =" in text:
@@ -688,6 +714,103 @@ def load_mtp(path: str) -> MtpModel:
         if "zbl_atomic_numbers =" in text:
             model.zbl_atomic_numbers = _numbers(_braced(text, "zbl_atomic_numbers ="), int)
     return model
+
+
+def _parse_gate(text: str, K: int, kmu: int, rb: int, S: int) -> dict:
+    """The gate keys of load_sh_model (sus2_sh.cu:2153-2268), same checks and
+    messages; neighbour site mode and shared-radial tables only."""
+    mode = _after(text, "two_layer_gate_mode =") if "two_layer_gate_mode =" in text else "legacy"
+    if mode == "mu-body-linear-combo":
+        mode_id = 1
+    elif mode in ("mu-scalar-full", "mu-body-order"):
+        mode_id = 2
+    elif mode == "legacy":
+        raise MtpError("GPUMD SUS2_SH mu-body-order branch requires two_layer_gate_mode = "
+                       "mu-body-linear-combo or mu-scalar-full; legacy gate models are not supported here.")
+    else:
+        raise MtpError("Unsupported SUS2_SH two_layer_gate_mode in GPUMD: " + mode)
+    if "two_layer_gate_include_one_body =" in text and _bool(_after(text, "two_layer_gate_include_one_body =")):
+        raise MtpError("GPUMD SUS2_SH gate backend requires two_layer_gate_include_one_body = false.")
+    if "two_layer_gate_scale_mode =" in text:
+        raise MtpError("GPUMD SUS2_SH mu-body gate does not support two_layer_gate_scale_mode.")
+    if "two_layer_gate_bias =" in text:
+        raise MtpError("GPUMD SUS2_SH mu-body gate does not support two_layer_gate_bias.")
+    if "two_layer_residual_enabled =" in text and _bool(_after(text, "two_layer_residual_enabled =")):
+        raise MtpError("GPUMD SUS2_SH mu-body gate does not support residual gate fields.")
+    if "two_layer_gate_site_mode =" in text:
+        site = _after(text, "two_layer_gate_site_mode =")
+        if site == "double":
+            raise MtpError("GPUMD SUS2_SH mu-body gate currently supports two_layer_gate_site_mode = neighbor. "
+                           "Double-site gate will be added after the single-gate CUDA path is verified.")
+        if site != "neighbor":
+            raise MtpError("Unsupported SUS2_SH two_layer_gate_site_mode in GPUMD: " + site)
+    amp = float(_after(text, "two_layer_gate_tanh_amplitude =")) if "two_layer_gate_tanh_amplitude =" in text else 0.8
+    if not math.isfinite(amp) or amp < 0.0 or amp > 1.0:
+        raise MtpError("SUS2_SH two_layer_gate_tanh_amplitude should be finite and in [0,1].")
+    radial_mode = _after(text, "two_layer_gate_radial_mode =") if "two_layer_gate_radial_mode =" in text else ""
+    if radial_mode != "shared-radial":
+        raise MtpError("GPUMD SUS2_SH gate backend currently requires shared-radial gate mode.")
+    if int(_after(text, "two_layer_gate_body_order_max =")) != K + 1:
+        raise MtpError("SUS2_SH two_layer_gate_body_order_max should equal sh_k_max + 1.")
+    nbody = K
+    nrad = int(_after(text, "two_layer_gate_radial_coeff_count ="))
+    if nrad != kmu * rb:
+        raise MtpError("SUS2_SH two-layer gate radial coefficient count is inconsistent.")
+    radial = _numbers(_braced(text, "two_layer_gate_radial_coeffs ="))
+    if len(radial) != nrad:
+        raise MtpError("SUS2_SH two-layer gate radial coeff list has wrong size.")
+    if "two_layer_gate_additive_coeff_count =" in text:
+        if int(_after(text, "two_layer_gate_additive_coeff_count =")) != S:
+            raise MtpError("SUS2_SH two-layer gate additive coefficient count is inconsistent.")
+        additive = _numbers(_braced(text, "two_layer_gate_additive_coeffs ="))
+        if len(additive) != S:
+            raise MtpError("SUS2_SH two-layer gate additive coeff list has wrong size.")
+    else:
+        additive = [1.0] * S
+    nw = int(_after(text, "two_layer_gate_weight_count ="))
+    if nw <= 0:
+        raise MtpError("SUS2_SH two-layer gate should contain at least one scalar weight.")
+    qidx = _numbers(_braced(text, "two_layer_gate_scalar_indices ="), int)
+    weights = _numbers(_braced(text, "two_layer_gate_weights ="))
+    if not qidx:
+        raise MtpError("SUS2_SH two-layer gate scalar index list is empty.")
+    expected = kmu * len(qidx) if mode_id == 2 else len(qidx)
+    if nw != expected or len(weights) != expected:
+        raise MtpError("SUS2_SH two-layer gate scalar index/weight dimensions are inconsistent.")
+    mix = []
+    if mode_id == 1:
+        nmix = int(_after(text, "two_layer_gate_body_mix_weight_count ="))
+        if nmix != kmu * nbody:
+            raise MtpError("SUS2_SH two-layer gate body-mix weight count is inconsistent.")
+        mix = _numbers(_braced(text, "two_layer_gate_body_mix_weights ="))
+        if len(mix) != nmix:
+            raise MtpError("SUS2_SH two-layer gate body-mix weight list has wrong size.")
+    elif "two_layer_gate_body_mix_weights =" in text or "two_layer_gate_body_mix_weight_count =" in text:
+        raise MtpError("SUS2_SH mu-scalar-full gate should not contain body-mix weights.")
+    return dict(mode=mode_id, amplitude=amp, nbody=nbody, radial=radial, additive=additive,
+                scalar_indices=qidx, weights=weights, body_mix=mix)
+
+
+def _gate_metadata(m: MtpModel, g: dict) -> None:
+    """Gate scalar -> moment and body bucket (sus2_sh.cu:2412-2461)."""
+    moment_of, body_of = [], []
+    present = [False] * g["nbody"]
+    for q in g["scalar_indices"]:
+        if q < 0 or q >= m.alpha_scalar_moments:
+            raise MtpError("SUS2_SH two-layer gate scalar index is out of range.")
+        b = m.scalar_body[q] - 2
+        if b < 0 or b >= g["nbody"]:
+            raise MtpError("SUS2_SH two-layer gate scalar body order is outside the gate range.")
+        present[b] = True
+        mom = m.alpha_moment_mapping[q]
+        if mom < 0 or mom >= m.alpha_moments_count:
+            raise MtpError("SUS2_SH two-layer gate mapped moment index is out of range.")
+        moment_of.append(mom)
+        body_of.append(b)
+    if not all(present):
+        raise MtpError("SUS2_SH two-layer gate scalar list misses a required body-order bucket.")
+    g["moment_of"] = moment_of
+    g["body_of"] = body_of
 
 
 def _bool(token: str) -> bool:

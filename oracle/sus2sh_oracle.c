@@ -766,3 +766,244 @@ int oracle_zbl_efs(int S, const int* z, const double* pin, const double* pout, i
   free(nl.e);
   return 0;
 }
+
+/* ---- two-layer mu-body gate ---------------------------------------------
+ * Restates the gate path of SUS2_SH::compute (sus2_sh.cu:9821-10120) in its
+ * plain form: first-layer moments Mg from the gate radial coefficients and
+ * every product; signals h_mu (mu-body-linear-combo: b_p = sum_{body(q)=p}
+ * w_q s_q, h_mu = sum_p c_{mu,p} b_p; mu-scalar-full: h_mu = sum_q W_{mu,q}
+ * s_q); G = 1 + A tanh(a_t h), D = A a_t (1 - tanh^2) per atom (:4565-4662);
+ * main moments with R_mu(r_ij) G_{j,mu} (:4247-4314); forces from the main
+ * adjoints with G_j, dE/dh_{j,mu} += D_{j,mu} R_mu sum g Y (:6077-6121);
+ * seeds and reverse products on Mg (:4664-4727); first-layer forces with the
+ * gate radial coefficients (:6695-6790).  Outputs assigned.                */
+typedef struct {
+  int mode;               /* 1 mu-body-linear-combo, 2 mu-scalar-full */
+  int nbody, nq;
+  double amplitude;
+  const double* radial;   /* [kmu][rb] */
+  const double* additive; /* [S] */
+  const int* q_moment;    /* [nq] */
+  const int* q_body;      /* [nq] */
+  const double* weights;  /* full [kmu][nq]; combo [nq] */
+  const double* body_mix; /* combo [kmu][nbody] */
+} OracleGate;
+
+static void moments_of_atom(const OracleModel* m, const NList* nl, int i, const int* type, const double* gmul,
+                            double* Mv) {
+  double R[64], Y[49];
+  const int ti = type[i];
+  memset(Mv, 0, sizeof(double) * m->M);
+  for (int q = nl->start[i]; q < nl->start[i + 1]; ++q) {
+    const Edge* e = nl->e + q;
+    const double r = sqrt(e->d[0] * e->d[0] + e->d[1] * e->d[1] + e->d[2] * e->d[2]);
+    oracle_radial(m, ti * m->S + type[e->j], r, R, NULL);
+    if (gmul)
+      for (int mu = 0; mu < m->kmu; ++mu) R[mu] *= gmul[(size_t)e->j * m->kmu + mu];
+    oracle_real_sh(m->L, e->d[0], e->d[1], e->d[2], Y, NULL);
+    for (int b = 0; b < m->nbasic; ++b) Mv[b] += R[m->basic_mu[b]] * Y[m->basic_y[b]];
+  }
+  for (int p = 0; p < m->nprod; ++p) Mv[m->prod_t[p]] += m->prod_c[p] * Mv[m->prod_l[p]] * Mv[m->prod_r[p]];
+}
+
+/* Edge forces of basic adjoints gb on atom i (radial of model m, optional
+ * gate multipliers of the neighbour and dE/dh accumulation). */
+static void edge_forces(const OracleModel* m, const NList* nl, int i, int N, const int* type, const double* gb,
+                        const double* gmul, const double* gder, double* adjh, double* fl, double* vir) {
+  double R[64], dR[64], Y[49], dY[147];
+  const int ti = type[i];
+  double w9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int q = nl->start[i]; q < nl->start[i + 1]; ++q) {
+    const Edge* e = nl->e + q;
+    const double dx = e->d[0], dy = e->d[1], dz = e->d[2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    oracle_radial(m, ti * m->S + type[e->j], r, R, dR);
+    oracle_real_sh(m->L, dx, dy, dz, Y, dY);
+    if (adjh) {
+      for (int b = 0; b < m->nbasic; ++b) {
+        const int mu = m->basic_mu[b];
+        adjh[(size_t)e->j * m->kmu + mu] += gb[b] * R[mu] * Y[m->basic_y[b]] * gder[(size_t)e->j * m->kmu + mu];
+      }
+    }
+    double ex = 0, ey = 0, ez = 0;
+    for (int b = 0; b < m->nbasic; ++b) {
+      const int mu = m->basic_mu[b], y = m->basic_y[b];
+      const double a = gb[b] * (gmul ? gmul[(size_t)e->j * m->kmu + mu] : 1.0);
+      if (a == 0.0) continue;
+      ex += a * (dR[mu] * dx / r * Y[y] + R[mu] * dY[3 * y + 0]);
+      ey += a * (dR[mu] * dy / r * Y[y] + R[mu] * dY[3 * y + 1]);
+      ez += a * (dR[mu] * dz / r * Y[y] + R[mu] * dY[3 * y + 2]);
+    }
+    fl[i] += ex;
+    fl[i + N] += ey;
+    fl[i + 2 * N] += ez;
+    fl[e->j] -= ex;
+    fl[e->j + N] -= ey;
+    fl[e->j + 2 * N] -= ez;
+    w9[0] -= dx * ex;
+    w9[1] -= dy * ey;
+    w9[2] -= dz * ez;
+    w9[3] -= dx * ey;
+    w9[4] -= dx * ez;
+    w9[5] -= dy * ez;
+    w9[6] -= dy * ex;
+    w9[7] -= dz * ex;
+    w9[8] -= dz * ey;
+  }
+  for (int k = 0; k < 9; ++k) vir[(size_t)k * N + i] += w9[k];
+}
+
+int oracle_efs_gate(const OracleModel* m, const OracleGate* g, int N, const double* h, const int* pbc,
+                    const int* type, const double* pos, double* pe, double* f, double* vir, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int nt = omp_get_max_threads();
+#else
+  (void)nthreads;
+  const int nt = 1;
+#endif
+  const int K = m->kmu;
+  Geo geo;
+  geo_init(&geo, h, pbc, m->rc);
+  NList nl;
+  if (build_nlist(&geo, N, pos, m->rc, &nl) != 0) return -1;
+  OracleModel mg = *m;
+  mg.radial = g->radial;
+  double* Mg = (double*)malloc(sizeof(double) * (size_t)N * m->M);
+  double* gmul = (double*)malloc(sizeof(double) * (size_t)N * K);
+  double* gder = (double*)malloc(sizeof(double) * (size_t)N * K);
+  double* gmain = (double*)malloc(sizeof(double) * (size_t)N * m->nbasic);
+  double* gfirst = (double*)malloc(sizeof(double) * (size_t)N * m->nbasic);
+  double* adjh_t = (double*)calloc((size_t)nt * N * K, sizeof(double));
+  double* fbuf = (double*)calloc((size_t)nt * 3 * N, sizeof(double));
+  if (!Mg || !gmul || !gder || !gmain || !gfirst || !adjh_t || !fbuf) return -1;
+  memset(vir, 0, sizeof(double) * 9 * (size_t)N);
+  /* 1. first layer: moments, signals, multipliers */
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int i = 0; i < N; ++i) {
+    double* Mv = Mg + (size_t)i * m->M;
+    moments_of_atom(&mg, &nl, i, type, NULL, Mv);
+    double hmu[64], body[64];
+    if (g->mode == 1) {
+      for (int b = 0; b < g->nbody; ++b) body[b] = 0.0;
+      for (int q = 0; q < g->nq; ++q) body[g->q_body[q]] += g->weights[q] * Mv[g->q_moment[q]];
+      for (int mu = 0; mu < K; ++mu) {
+        hmu[mu] = 0.0;
+        for (int b = 0; b < g->nbody; ++b) hmu[mu] += g->body_mix[mu * g->nbody + b] * body[b];
+      }
+    } else {
+      for (int mu = 0; mu < K; ++mu) {
+        hmu[mu] = 0.0;
+        for (int q = 0; q < g->nq; ++q) hmu[mu] += g->weights[mu * g->nq + q] * Mv[g->q_moment[q]];
+      }
+    }
+    const double a = g->additive[type[i]];
+    for (int mu = 0; mu < K; ++mu) {
+      const double th = tanh(a * hmu[mu]);
+      gmul[(size_t)i * K + mu] = 1.0 + g->amplitude * th;
+      gder[(size_t)i * K + mu] = g->amplitude * a * (1.0 - th * th);
+    }
+  }
+  /* 2. main layer: energies and basic adjoints */
+#pragma omp parallel
+  {
+    double* Mv = (double*)malloc(sizeof(double) * m->M);
+    double* gv = (double*)malloc(sizeof(double) * m->M);
+#pragma omp for schedule(dynamic, 32)
+    for (int i = 0; i < N; ++i) {
+      moments_of_atom(m, &nl, i, type, gmul, Mv);
+      const int ti = type[i];
+      const double ct = m->species[ti];
+      double E = m->shift_e[ti] + ct;
+      memset(gv, 0, sizeof(double) * m->M);
+      for (int s = 0; s < m->nscalar; ++s) {
+        E += ct * m->w[s] * Mv[m->map[s]];
+        gv[m->map[s]] += ct * m->w[s];
+      }
+      pe[i] = E;
+      for (int p = m->nprod - 1; p >= 0; --p) {
+        const double gt = gv[m->prod_t[p]] * m->prod_c[p];
+        gv[m->prod_l[p]] += gt * Mv[m->prod_r[p]];
+        gv[m->prod_r[p]] += gt * Mv[m->prod_l[p]];
+      }
+      memcpy(gmain + (size_t)i * m->nbasic, gv, sizeof(double) * m->nbasic);
+    }
+    free(Mv);
+    free(gv);
+  }
+  /* 3. main forces with gate multipliers; dE/dh per thread */
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num();
+#else
+    const int tid = 0;
+#endif
+#pragma omp for schedule(dynamic, 32)
+    for (int i = 0; i < N; ++i)
+      edge_forces(m, &nl, i, N, type, gmain + (size_t)i * m->nbasic, gmul, gder, adjh_t + (size_t)tid * N * K,
+                  fbuf + (size_t)tid * 3 * N, vir);
+  }
+  for (size_t a = 0; a < (size_t)N * K; ++a)
+    for (int t = 1; t < nt; ++t) adjh_t[a] += adjh_t[(size_t)t * N * K + a];
+  /* 4. seeds and reverse products on the first layer */
+#pragma omp parallel
+  {
+    double* gv = (double*)malloc(sizeof(double) * m->M);
+#pragma omp for schedule(dynamic, 32)
+    for (int i = 0; i < N; ++i) {
+      const double* Mv = Mg + (size_t)i * m->M;
+      const double* adj = adjh_t + (size_t)i * K;
+      memset(gv, 0, sizeof(double) * m->M);
+      if (g->mode == 1) {
+        double body[64];
+        for (int b = 0; b < g->nbody; ++b) {
+          body[b] = 0.0;
+          for (int mu = 0; mu < K; ++mu) body[b] += adj[mu] * g->body_mix[mu * g->nbody + b];
+        }
+        for (int q = 0; q < g->nq; ++q) gv[g->q_moment[q]] += body[g->q_body[q]] * g->weights[q];
+      } else {
+        for (int q = 0; q < g->nq; ++q) {
+          double seed = 0.0;
+          for (int mu = 0; mu < K; ++mu) seed += adj[mu] * g->weights[mu * g->nq + q];
+          gv[g->q_moment[q]] += seed;
+        }
+      }
+      for (int p = m->nprod - 1; p >= 0; --p) {
+        const double gt = gv[m->prod_t[p]] * m->prod_c[p];
+        gv[m->prod_l[p]] += gt * Mv[m->prod_r[p]];
+        gv[m->prod_r[p]] += gt * Mv[m->prod_l[p]];
+      }
+      memcpy(gfirst + (size_t)i * m->nbasic, gv, sizeof(double) * m->nbasic);
+    }
+    free(gv);
+  }
+  /* 5. first-layer forces */
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    const int tid = omp_get_thread_num();
+#else
+    const int tid = 0;
+#endif
+#pragma omp for schedule(dynamic, 32)
+    for (int i = 0; i < N; ++i)
+      edge_forces(&mg, &nl, i, N, type, gfirst + (size_t)i * m->nbasic, NULL, NULL, NULL,
+                  fbuf + (size_t)tid * 3 * N, vir);
+  }
+  for (int a = 0; a < 3 * N; ++a) {
+    double s = 0.0;
+    for (int t = 0; t < nt; ++t) s += fbuf[(size_t)t * 3 * N + a];
+    f[a] = s;
+  }
+  free(Mg);
+  free(gmul);
+  free(gder);
+  free(gmain);
+  free(gfirst);
+  free(adjh_t);
+  free(fbuf);
+  free(nl.start);
+  free(nl.e);
+  return 0;
+}

@@ -150,6 +150,13 @@ def zbl_pair(zi: int, zj: int, r: float, inner: float, outer: float):
     return e.value, de.value
 
 
+class _COracleGate(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("nbody", ctypes.c_int), ("nq", ctypes.c_int),
+                ("amplitude", ctypes.c_double),
+                ("radial", ctypes.c_void_p), ("additive", ctypes.c_void_p), ("q_moment", ctypes.c_void_p),
+                ("q_body", ctypes.c_void_p), ("weights", ctypes.c_void_p), ("body_mix", ctypes.c_void_p)]
+
+
 class Oracle:
     """FP64 energy/force/virial of one model (C oracle, OpenMP).  ZBL models
     take their atomic numbers from ``zbl_atomic_numbers`` or, as the
@@ -164,6 +171,21 @@ class Oracle:
         self.lib.oracle_efs.restype = ctypes.c_int
         self.lib.oracle_basics.restype = ctypes.c_int
         self.lib.oracle_neighbor_counts.restype = ctypes.c_int
+        self.gate = None
+        if m.gate is not None:
+            g = m.gate
+            f32 = (lambda a: a.astype(np.float32).astype(np.float64)) if reference_rounding else (lambda a: a)
+            arrs = dict(radial=f32(np.asarray(g["radial"], dtype=np.float64)),
+                        additive=np.asarray(g["additive"], dtype=np.float64),
+                        q_moment=np.asarray(g["moment_of"], dtype=np.int32),
+                        q_body=np.asarray(g["body_of"], dtype=np.int32),
+                        weights=np.asarray(g["weights"], dtype=np.float64),
+                        body_mix=np.asarray(g["body_mix"] or [0.0], dtype=np.float64))
+            ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+            self._gate_arrays = arrs
+            self.gate = _COracleGate(g["mode"], g["nbody"], len(g["moment_of"]), g["amplitude"],
+                                     *(ptr(arrs[k]) for k in ("radial", "additive", "q_moment", "q_body",
+                                                              "weights", "body_mix")))
         self.zbl = None
         if m.zbl_enabled:
             z = m.zbl_atomic_numbers
@@ -191,8 +213,12 @@ class Oracle:
         f = np.zeros((3, N))
         vir = np.zeros((9, N))
         ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-        rc = self.lib.oracle_efs(ctypes.byref(self._c), N, ptr(h), ptr(pbc), ptr(types), ptr(pos),
-                                 ptr(pe), ptr(f), ptr(vir), nthreads)
+        if self.gate is not None:
+            rc = self.lib.oracle_efs_gate(ctypes.byref(self._c), ctypes.byref(self.gate), N, ptr(h), ptr(pbc),
+                                          ptr(types), ptr(pos), ptr(pe), ptr(f), ptr(vir), nthreads)
+        else:
+            rc = self.lib.oracle_efs(ctypes.byref(self._c), N, ptr(h), ptr(pbc), ptr(types), ptr(pos),
+                                     ptr(pe), ptr(f), ptr(vir), nthreads)
         if rc != 0:
             raise RuntimeError("oracle_efs failed")
         if self.zbl is not None:

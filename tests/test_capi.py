@@ -55,7 +55,10 @@ CASES = [
     ("alpha_index_basic_count = 48", "alpha_index_basic_count = 47", "alpha_index_basic size"),
     ("sh_product_count = 806", "sh_product_count = 805", "sh_products size"),
     ("sh_parity = even", "sh_parity = odd", "even parity"),
-    ("alpha_scalar_moments = 107", "alpha_scalar_moments = 106", "coefficient dimensions"),
+    # sh_scalar_info is checked before the coefficient dimensions (sus2_sh.cu:2354-2410)
+    ("alpha_scalar_moments = 107", "alpha_scalar_moments = 106", "sh_scalar_info_count should equal"),
+    ("sh_scalar_info_count = 107", "sh_scalar_info_count = 106", "sh_scalar_info_count should equal"),
+    ("shift_coeffs = {-3.5, ", "shift_coeffs = {", "coefficient dimensions"),
 ]
 
 
