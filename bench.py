@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch-cell and large-model fields")
+    ap.add_argument("--large-only", type=int, default=0, metavar="ATOMS",
+                    help="run only the large-model workload with this many atoms and print its fields "
+                         "(profiling of the large-graph kernels)")
     return ap.parse_args()
 
 
@@ -298,14 +301,14 @@ def batch_cells_run(torch, path, ncells=4096, reps=10):
             "tiles": {"basic_block": info["basic_block"], "force_block": info["force_block"]}}
 
 
-def large_model_run(torch, model_dir, reps=5):
+def large_model_run(torch, model_dir, reps=5, atoms=262144):
     """Large-model workload: Cu-Zr-Al body-5 L=4 K=4 rb10 rational-map model
     (5985 moments, 33,389 products) on 262,144 random-insertion atoms
     (0.06 A^-3, d_min 2.1 A, 50/35/15), FP32; static positions, one
     energy/force/virial evaluation per step."""
     from sus2sh import SUS2_SH, models, structures
     path = models.preset_model("l4k4", model_dir)
-    box, types, pos = structures.random_insertion(262144, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=77)
+    box, types, pos = structures.random_insertion(atoms, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=77)
     N = types.size
     dev = torch.device("cuda")
     pot = SUS2_SH(path, N, ["Cu", "Zr", "Al"])
@@ -326,8 +329,10 @@ def large_model_run(torch, model_dir, reps=5):
     ms = e0.elapsed_time(e1) / reps
     prof = pot.profile_read()
     flags = pot.sync()
+    info = pot.info()
     pot.close()
-    return {"workload": "262,144-atom Cu-Zr-Al l4k4 body-5 rational model, FP32", "atoms": N,
+    return {"workload": f"{N:,}-atom Cu-Zr-Al l4k4 body-5 rational model, FP32", "atoms": N,
+            "cg_kernel": {0: "row interpreter", 1: "straight-line", 2: "component-split"}.get(info["cg_kind"]),
             "ms_per_eval": ms, "atom_steps_per_s": N / (ms * 1e-3), "status_flags": flags,
             "stage_ms_per_eval": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"}}
 
@@ -392,6 +397,10 @@ def main():
     CELLS_RUN = tuple(args.cells)
     import numpy as np
     import torch
+    if args.large_only:
+        with tempfile.TemporaryDirectory() as d:
+            print(json.dumps({"large_model": large_model_run(torch, d, atoms=args.large_only)}), flush=True)
+        return
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:

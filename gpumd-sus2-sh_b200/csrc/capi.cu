@@ -25,9 +25,30 @@ namespace {
 
 thread_local std::string g_last_error;
 
-// Graphs up to this many saved products get a straight-line CG kernel; larger
-// ones (body-5 L=4 graphs have ~3e4) run the row interpreter.
-constexpr long long kCgJitMaxProducts = 12000;
+// Graphs up to this many saved products get one straight-line CG function
+// (above it ptxas spills: 7.5 KB at 5,475 products, 83 KB and a 4-minute
+// compile at 10,993); larger graphs get the component-split kernel, and
+// graphs that split into no small components run the row interpreter.
+constexpr long long kCgSingleMaxProducts = 3000;
+
+// The CG kernel source the engine builds for a model: the single straight-line
+// function, the component-split kernel (split: -1 auto, 0 never, 1 always), or
+// none (false; the row interpreter runs, *why says why).
+bool choose_cg_source(const HostModel& m, const Layered& lay, const std::vector<int>& basic_canon, int ncanon,
+                      bool use_float, int split, CgSource* out, std::string* why) {
+  long long terms = 0;
+  for (const Row& r : lay.rows) terms += static_cast<long long>(r.left.size());
+  const bool single_ok = terms <= kCgSingleMaxProducts;
+  if (split == 1 || (split < 0 && !single_ok)) {
+    if (generate_cg_split_source(m, lay, use_float, basic_canon, ncanon, out, why)) return true;
+  }
+  if (single_ok) {
+    *out = generate_cg_source(m, lay, use_float, basic_canon, ncanon);
+    return true;
+  }
+  if (why && why->empty()) *why = "graph above the single-function limit and the split kernel is disabled";
+  return false;
+}
 
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& m) : std::runtime_error(m) {}
@@ -514,17 +535,13 @@ struct Engine {
     prod_global = best_tile == 0;
     prod_tile = best_tile ? best_tile : 128;
     prod_smem = per_atom * prod_tile;
-    // straight-line CG kernel for graphs of moderate size
+    // model-specialised CG kernel (straight-line or component-split)
     if (opt.cg_jit) {
-      long long terms = 0;
-      for (const Row& r : lay.rows) terms += static_cast<long long>(r.left.size());
-      if (terms <= kCgJitMaxProducts) {
-        const auto t0 = std::chrono::steady_clock::now();
-        cg_src = generate_cg_source(model, lay, use_float, prog.basic_canon, prog.ncanon);
+      const auto t0 = std::chrono::steady_clock::now();
+      std::string why;
+      if (choose_cg_source(model, lay, prog.basic_canon, prog.ncanon, use_float, opt.cg_split, &cg_src, &why))
         cg_bin = compile_cg_source(cg_src);
-        cg_compile_ms =
-            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      }
+      cg_compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     if (num_atoms > 0) ensure_size(num_atoms);
   }
@@ -878,8 +895,9 @@ struct Engine {
     mark(ev, 2, s);
     if (!cg_bin.cubin.empty()) {
       std::string err;
-      if (!cg_mod.load(cg_bin, cg_src.kernel_name, &err) ||
-          !cg_mod.launch(s, N, pos4.p, Bbuf.p, Gbuf.p, d_shift.p, d_species.p, pe, pe_assign, &err))
+      if (!cg_mod.load(cg_bin, cg_src.kernel_name, &err, cg_src.smem_bytes) ||
+          !cg_mod.launch(s, N, pos4.p, Bbuf.p, Gbuf.p, d_shift.p, d_species.p, pe, pe_assign, &err, cg_src.block,
+                         cg_src.smem_bytes))
         throw CudaError(err);
     } else {
       launch_product<T>(s, N, program_dev(), pos4.p, reinterpret_cast<const T*>(Bbuf.p),
@@ -1251,7 +1269,7 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[31] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[34] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
@@ -1262,8 +1280,10 @@ int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
                      e.basic_block, e.force_block, e.edge_jit ? 1 : 0,
                      e.ejit_bin ? e.ejit_bin->basic_registers : -1, e.ejit_bin ? e.ejit_bin->force_registers : -1,
                      e.ejit_bin ? static_cast<int>(e.ejit_bin->compile_ms) : 0,
-                     e.gate ? static_cast<int>(e.model.gate.mode) : 0};
-  const int k = std::min(n, 31);
+                     e.gate ? static_cast<int>(e.model.gate.mode) : 0,
+                     e.cg_bin.cubin.empty() ? 0 : (e.cg_src.split ? 2 : 1),
+                     e.cg_mod.registers(), e.cg_mod.local_bytes()};
+  const int k = std::min(n, 34);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -1353,17 +1373,17 @@ int sus2sh_reduce(int N, const double* potential, const double* virial, double* 
   return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
 }
 
-int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text, size_t text_size) {
+int sus2sh_cg_kernel_info(const char* path, int use_float, int split, int* info, char* text, size_t text_size) {
   if (!path || !info) return SUS2SH_E_ARG;
   return guarded([&] {
     const sus2sh::HostModel m = sus2sh::load_model(path);
     const sus2sh::Layered lay = sus2sh::layer_products(m);
     const sus2sh::ProgramHost prog = sus2sh::compile_program(m, lay);
-    if (static_cast<long long>(m.products.size()) > sus2sh::kCgJitMaxProducts)
-      throw InputError("graph has more products than the straight-line CG kernel limit (" +
-                       std::to_string(sus2sh::kCgJitMaxProducts) + "); the row interpreter runs it");
     const auto t0 = std::chrono::steady_clock::now();
-    const sus2sh::CgSource src = sus2sh::generate_cg_source(m, lay, use_float != 0, prog.basic_canon, prog.ncanon);
+    sus2sh::CgSource src;
+    std::string why;
+    if (!sus2sh::choose_cg_source(m, lay, prog.basic_canon, prog.ncanon, use_float != 0, split, &src, &why))
+      throw InputError("no CG kernel for this graph (" + why + "); the row interpreter runs it");
     const sus2sh::CgBinary bin = sus2sh::compile_cg_source(src);
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     int spill = 0;
@@ -1379,6 +1399,11 @@ int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text
     info[2] = static_cast<int>(src.fp_terms);
     info[3] = static_cast<int>(ms);
     info[4] = static_cast<int>(bin.cubin.size());
+    info[5] = src.split ? 1 : 0;
+    info[6] = src.functions;
+    info[7] = src.components;
+    info[8] = src.block;
+    info[9] = static_cast<int>(src.smem_bytes);
     if (text && text_size) {
       const std::string& t = use_float < 0 ? src.code : bin.log;
       const size_t k = std::min(text_size - 1, t.size());

@@ -5,13 +5,19 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nvJitLink.h>
 #include <nvrtc.h>
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <set>
 #include <sstream>
 
@@ -204,14 +210,34 @@ CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_flo
   return out;
 }
 
-CgBinary compile_cg_source(const CgSource& src) {
+namespace {
+
+struct UnitResult {
+  std::vector<char> cubin;
+  std::string log;
+  std::string error;
+};
+
+// One NVRTC program for sm_100a (relocatable when rdc), ptxas report kept.
+UnitResult compile_unit(const std::string& code, bool rdc) {
+  UnitResult out;
   nvrtcProgram prog;
-  if (nvrtcCreateProgram(&prog, src.code.c_str(), "sus2sh_cg.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
-    throw InputError("NVRTC could not create the CG program.");
-  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--ptxas-options=--verbose",
-                        "--fmad=true"};
-  const nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
-  CgBinary out;
+  if (nvrtcCreateProgram(&prog, code.c_str(), "sus2sh_cg.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+    out.error = "NVRTC could not create the CG program.";
+    return out;
+  }
+  std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "--std=c++17", "--ptxas-options=--verbose",
+                                   "--fmad=true"};
+  if (rdc) opts.push_back("--relocatable-device-code=true");
+  // extra NVRTC options for tuning runs (whitespace separated), e.g.
+  // SUS2SH_NVRTC_OPTIONS="--ptxas-options=--device-function-maxrregcount=255"
+  std::vector<std::string> extra;
+  if (const char* env = std::getenv("SUS2SH_NVRTC_OPTIONS")) {
+    std::istringstream is(env);
+    for (std::string w; is >> w;) extra.push_back(w);
+  }
+  for (const std::string& w : extra) opts.push_back(w.c_str());
+  const nvrtcResult rc = nvrtcCompileProgram(prog, static_cast<int>(opts.size()), opts.data());
   size_t log_size = 0;
   nvrtcGetProgramLogSize(prog, &log_size);
   if (log_size > 1) {
@@ -220,16 +246,152 @@ CgBinary compile_cg_source(const CgSource& src) {
   }
   if (rc != NVRTC_SUCCESS) {
     nvrtcDestroyProgram(&prog);
-    throw InputError("NVRTC failed to compile the CG program: " + out.log.substr(0, 2000));
+    out.error = "NVRTC failed to compile the CG program: " + out.log.substr(0, 2000);
+    return out;
   }
   size_t n = 0;
   nvrtcGetCUBINSize(prog, &n);
   out.cubin.resize(n);
   nvrtcGetCUBIN(prog, out.cubin.data());
   nvrtcDestroyProgram(&prog);
-  const size_t p = out.log.find("Used ");
-  if (p != std::string::npos) out.registers = std::atoi(out.log.c_str() + p + 5);
   return out;
+}
+
+// nvJitLink 12.9, opened by path at first use.  The library is not linked:
+// a process that loaded an older libnvJitLink.so.12 first (PyTorch wheels
+// bundle one) would otherwise fail to resolve the 12.9 entry points.
+struct JitLinkApi {
+  decltype(&__nvJitLinkCreate_12_9) create = nullptr;
+  decltype(&__nvJitLinkDestroy_12_9) destroy = nullptr;
+  decltype(&__nvJitLinkAddData_12_9) add_data = nullptr;
+  decltype(&__nvJitLinkComplete_12_9) complete = nullptr;
+  decltype(&__nvJitLinkGetLinkedCubinSize_12_9) cubin_size = nullptr;
+  decltype(&__nvJitLinkGetLinkedCubin_12_9) cubin = nullptr;
+  decltype(&__nvJitLinkGetErrorLogSize_12_9) error_size = nullptr;
+  decltype(&__nvJitLinkGetErrorLog_12_9) error_log = nullptr;
+  bool ok = false;
+};
+
+const JitLinkApi& jitlink() {
+  static const JitLinkApi api = [] {
+    JitLinkApi a;
+    std::vector<std::string> paths;
+    if (const char* home = std::getenv("CUDA_HOME")) paths.push_back(std::string(home) + "/lib64/libnvJitLink.so.12");
+    paths.push_back("/usr/local/cuda/lib64/libnvJitLink.so.12");
+    paths.push_back("libnvJitLink.so.12");
+    for (const std::string& p : paths) {
+      void* h = dlopen(p.c_str(), RTLD_NOW | RTLD_LOCAL);
+      if (!h) continue;
+      a.create = reinterpret_cast<decltype(a.create)>(dlsym(h, "__nvJitLinkCreate_12_9"));
+      a.destroy = reinterpret_cast<decltype(a.destroy)>(dlsym(h, "__nvJitLinkDestroy_12_9"));
+      a.add_data = reinterpret_cast<decltype(a.add_data)>(dlsym(h, "__nvJitLinkAddData_12_9"));
+      a.complete = reinterpret_cast<decltype(a.complete)>(dlsym(h, "__nvJitLinkComplete_12_9"));
+      a.cubin_size = reinterpret_cast<decltype(a.cubin_size)>(dlsym(h, "__nvJitLinkGetLinkedCubinSize_12_9"));
+      a.cubin = reinterpret_cast<decltype(a.cubin)>(dlsym(h, "__nvJitLinkGetLinkedCubin_12_9"));
+      a.error_size = reinterpret_cast<decltype(a.error_size)>(dlsym(h, "__nvJitLinkGetErrorLogSize_12_9"));
+      a.error_log = reinterpret_cast<decltype(a.error_log)>(dlsym(h, "__nvJitLinkGetErrorLog_12_9"));
+      a.ok = a.create && a.destroy && a.add_data && a.complete && a.cubin_size && a.cubin && a.error_size &&
+             a.error_log;
+      if (a.ok) break;
+      dlclose(h);
+      a = JitLinkApi{};
+    }
+    return a;
+  }();
+  return api;
+}
+
+// Largest "Used N registers" in a ptxas report (-1 if none).
+int max_registers(const std::string& log) {
+  int best = -1;
+  for (size_t p = log.find("Used "); p != std::string::npos; p = log.find("Used ", p + 5))
+    best = std::max(best, std::atoi(log.c_str() + p + 5));
+  return best;
+}
+
+CgBinary build_binary(const CgSource& src) {
+  CgBinary out;
+  const JitLinkApi& jl = jitlink();
+  if (src.units.size() < 2 || !jl.ok) {
+    // one program (also the fallback when nvJitLink 12.9 is not available)
+    UnitResult u = compile_unit(src.code, false);
+    if (!u.error.empty()) throw InputError(u.error);
+    out.cubin = std::move(u.cubin);
+    out.log = std::move(u.log);
+    out.registers = max_registers(out.log);
+    return out;
+  }
+  // component-split kernel: the units compile in parallel as relocatable
+  // code and nvJitLink joins them
+  std::vector<UnitResult> res(src.units.size());
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nthreads = std::min(src.units.size(), std::min<size_t>(hw, 32));
+  std::vector<std::thread> pool;
+  std::mutex mu;
+  size_t next = 0;
+  for (size_t t = 0; t < nthreads; ++t)
+    pool.emplace_back([&] {
+      for (;;) {
+        size_t k;
+        {
+          std::lock_guard<std::mutex> lock(mu);
+          if (next >= src.units.size()) return;
+          k = next++;
+        }
+        res[k] = compile_unit(src.units[k], true);
+      }
+    });
+  for (std::thread& th : pool) th.join();
+  for (const UnitResult& u : res) {
+    if (!u.error.empty()) throw InputError(u.error);
+    out.log += u.log;
+  }
+  nvJitLinkHandle h = nullptr;
+  const char* lopts[] = {"-arch=sm_100a"};
+  if (jl.create(&h, 1, lopts) != NVJITLINK_SUCCESS) throw InputError("nvJitLink could not be created.");
+  auto link_error = [&](const char* what) {
+    size_t n = 0;
+    std::string log;
+    if (jl.error_size(h, &n) == NVJITLINK_SUCCESS && n > 1) {
+      log.resize(n);
+      jl.error_log(h, &log[0]);
+    }
+    jl.destroy(&h);
+    throw InputError(std::string(what) + " " + log.substr(0, 2000));
+  };
+  for (size_t k = 0; k < res.size(); ++k) {
+    const std::string name = "unit" + std::to_string(k);
+    if (jl.add_data(h, NVJITLINK_INPUT_CUBIN, res[k].cubin.data(), res[k].cubin.size(), name.c_str()) !=
+        NVJITLINK_SUCCESS)
+      link_error("nvJitLink rejected a CG unit:");
+  }
+  if (jl.complete(h) != NVJITLINK_SUCCESS) link_error("nvJitLink failed to link the CG kernel:");
+  size_t n = 0;
+  jl.cubin_size(h, &n);
+  out.cubin.resize(n);
+  jl.cubin(h, out.cubin.data());
+  jl.destroy(&h);
+  out.registers = max_registers(out.log);
+  return out;
+}
+
+}  // namespace
+
+CgBinary compile_cg_source(const CgSource& src) {
+  // binaries are cached per process: models of the same graph (or the same
+  // model loaded twice) compile once
+  static std::mutex mu;
+  static std::map<std::string, std::shared_ptr<const CgBinary>> cache;
+  const std::string key = src.kernel_name + ":" + std::to_string(src.code.size()) + ":" +
+                          std::to_string(fnv1a(src.code));
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return *it->second;
+  }
+  auto bin = std::make_shared<const CgBinary>(build_binary(src));
+  std::lock_guard<std::mutex> lock(mu);
+  return *cache.emplace(key, bin).first->second;
 }
 
 // ---------------------------------------------------------------------------
@@ -243,7 +405,7 @@ CgModule::~CgModule() {
   }
 }
 
-bool CgModule::load(const CgBinary& bin, const std::string& kernel_name, std::string* err) {
+bool CgModule::load(const CgBinary& bin, const std::string& kernel_name, std::string* err, size_t smem_bytes) {
   if (func_) return true;
   cudaFree(nullptr);  // make the primary context current on this thread
   auto load_data = entry<PFN_load>("cuModuleLoadData");
@@ -262,22 +424,35 @@ bool CgModule::load(const CgBinary& bin, const std::string& kernel_name, std::st
     if (err) *err = "cuModuleGetFunction failed for the CG kernel";
     return false;
   }
+  if (smem_bytes > 0) {
+    auto set_attr = entry<PFN_set_attr>("cuFuncSetAttribute");
+    if (!set_attr || set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem_bytes)) !=
+                         CUDA_SUCCESS) {
+      if (err) *err = "cuFuncSetAttribute failed for the CG kernel's shared memory";
+      return false;
+    }
+  }
+  if (auto get_attr = entry<PFN_get_attr>("cuFuncGetAttribute")) {
+    get_attr(&regs_, CU_FUNC_ATTRIBUTE_NUM_REGS, f);
+    get_attr(&local_, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, f);
+  }
   module_ = mod;
   func_ = f;
   return true;
 }
 
 bool CgModule::launch(void* stream, int N, const void* pos4, const void* B, void* G, const double* shift,
-                      const double* species, double* pe, int pe_assign, std::string* err) {
+                      const double* species, double* pe, int pe_assign, std::string* err, int block,
+                      size_t smem_bytes) {
   static PFN_launch launch_fn = entry<PFN_launch>("cuLaunchKernel");
   if (!launch_fn || !func_) {
     if (err) *err = "CG kernel not loaded";
     return false;
   }
   void* args[] = {&N, &pos4, &B, &G, &shift, &species, &pe, &pe_assign};
-  const unsigned grid = static_cast<unsigned>((N + 127) / 128);
-  if (launch_fn(static_cast<CUfunction>(func_), grid, 1, 1, 128, 1, 1, 0, static_cast<CUstream>(stream), args,
-                nullptr) != CUDA_SUCCESS) {
+  const unsigned grid = static_cast<unsigned>((N + block - 1) / block);
+  if (launch_fn(static_cast<CUfunction>(func_), grid, 1, 1, static_cast<unsigned>(block), 1, 1,
+                static_cast<unsigned>(smem_bytes), static_cast<CUstream>(stream), args, nullptr) != CUDA_SUCCESS) {
     if (err) *err = "cuLaunchKernel failed for the CG kernel";
     return false;
   }

@@ -19,9 +19,17 @@
 namespace sus2sh {
 
 struct CgSource {
-  std::string code;
+  std::string code;                // the whole program as one translation unit
+  std::vector<std::string> units;  // split kernels: the same program as separately
+                                   // compiled units (kernel first), linked by nvJitLink
   std::string kernel_name;
   long long fp_terms = 0;  // emitted multiply-add terms (size estimate)
+  // launch shape: threads per CTA (lane = atom) and dynamic shared memory
+  int block = 128;
+  size_t smem_bytes = 0;
+  bool split = false;      // component-split kernel (generate_cg_split_source)
+  int functions = 1;       // device functions in the program
+  int components = 0;      // independent components (split kernels)
 };
 
 // Emits the kernel source.  basic_canon[b] is the canonical [k*C + l*l+l+m]
@@ -29,13 +37,28 @@ struct CgSource {
 CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_float,
                             const std::vector<int>& basic_canon, int ncanon);
 
+// Component-split kernel for graphs too large for one straight-line
+// function: the local intermediates (those feeding terminal scalar rows only)
+// are grouped into the connected components of the terminal terms, each
+// evaluated by its own __noinline__ function with its values in registers;
+// basic moments, shared intermediates and all their adjoints live in
+// lane-private shared memory.  Same kernel parameters as
+// generate_cg_source.  Returns false with the reason in *why when the graph
+// does not split into components of at most 160 values or its shared-memory
+// slots do not fit.
+bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_float,
+                              const std::vector<int>& basic_canon, int ncanon, CgSource* out,
+                              std::string* why);
+
 struct CgBinary {
   std::vector<char> cubin;
   std::string log;
   int registers = -1;  // parsed from the ptxas report, -1 if unknown
 };
 
-// NVRTC compile for sm_100a; throws InputError with the log on failure.
+// NVRTC compile for sm_100a (split kernels: the units in parallel threads,
+// relocatable, then nvJitLink); cached per process by source.  Throws
+// InputError with the log on failure.
 CgBinary compile_cg_source(const CgSource& src);
 
 // Loaded module of a compiled kernel on the current device (driver API
@@ -46,16 +69,24 @@ class CgModule {
   ~CgModule();
   CgModule(const CgModule&) = delete;
   CgModule& operator=(const CgModule&) = delete;
-  // Loads the cubin into the current context once; returns false on error.
-  bool load(const CgBinary& bin, const std::string& kernel_name, std::string* err);
+  // Loads the cubin into the current context once (and raises the kernel's
+  // dynamic shared-memory limit to smem_bytes); returns false on error.
+  bool load(const CgBinary& bin, const std::string& kernel_name, std::string* err, size_t smem_bytes = 0);
   bool loaded() const { return func_ != nullptr; }
-  // Launches with params: N, pos4, B, G, shift, species, pe, pe_assign.
+  // Registers per thread and local memory (spill + stack) bytes per thread of
+  // the loaded kernel, call tree included (-1 before load).
+  int registers() const { return regs_; }
+  int local_bytes() const { return local_; }
+  // Launches with params: N, pos4, B, G, shift, species, pe, pe_assign, on
+  // ceil(N / block) CTAs of `block` threads with smem_bytes dynamic shared memory.
   bool launch(void* stream, int N, const void* pos4, const void* B, void* G, const double* shift,
-              const double* species, double* pe, int pe_assign, std::string* err);
+              const double* species, double* pe, int pe_assign, std::string* err, int block = 128,
+              size_t smem_bytes = 0);
 
  private:
   void* module_ = nullptr;
   void* func_ = nullptr;
+  int regs_ = -1, local_ = -1;
 };
 
 }  // namespace sus2sh

@@ -14,6 +14,7 @@ using PFN_launch = CUresult (*)(CUfunction, unsigned, unsigned, unsigned, unsign
                                 CUstream, void**, void**);
 using PFN_unload = CUresult (*)(CUmodule);
 using PFN_set_attr = CUresult (*)(CUfunction, CUfunction_attribute, int);
+using PFN_get_attr = CUresult (*)(int*, CUfunction_attribute, CUfunction);
 
 template <typename F>
 F entry(const char* name) {

@@ -55,7 +55,7 @@ def load() -> ctypes.CDLL:
         "sus2sh_param_grad_batch": (I, [P, I, I, P, P, P, P, P, P, P, P, P, P]),
         "sus2sh_profile_read": (I, [P, P, I]),
         "sus2sh_measure_fma_peak": (I, [I, P]),
-        "sus2sh_cg_kernel_info": (I, [S, I, P, P, ctypes.c_size_t]),
+        "sus2sh_cg_kernel_info": (I, [S, I, I, P, P, ctypes.c_size_t]),
         "sus2sh_zbl_pair": (I, [I, I, D, D, D, P, P]),
         "sus2sh_real_sh": (I, [I, D, D, D, P, P, P]),
         "sus2sh_edge_kernel_info": (I, [I, I, I, I, P, P, P, ctypes.c_char_p, ctypes.c_size_t]),

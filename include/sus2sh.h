@@ -184,7 +184,10 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * compiled with NVRTC at load (shape without an ahead-of-time build, or
  * sus2_sh_edge_jit=1) [27] [28] their registers per thread (basic, force)
  * [29] their compile time (ms) [30] two-layer gate mode (0 none,
- * 1 mu-body-linear-combo, 2 mu-scalar-full).  Returns the number written. */
+ * 1 mu-body-linear-combo, 2 mu-scalar-full) [31] CG kernel kind (0 row
+ * interpreter, 1 one straight-line function, 2 component-split) [32] [33]
+ * registers and local-memory bytes per thread of the loaded CG kernel, call
+ * tree included (-1 before the first evaluation).  Returns the number written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

@@ -45,11 +45,16 @@ int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* typ
 int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream);
 
 /* Generates and NVRTC-compiles (sm_100a, no GPU needed) the model-specialised
- * CG product kernel of a model file: info[0] registers per thread, [1] spill
- * store bytes, [2] emitted multiply-add terms, [3] generate+compile ms,
- * [4] cubin bytes.  text (if not NULL) receives the ptxas report.  Graphs
- * above the straight-line limit (12000 products) return SUS2SH_E_INPUT. */
-int sus2sh_cg_kernel_info(const char* path, int use_float, int* info, char* text, size_t text_size);
+ * CG product kernel the engine would build for a model file (split: -1 as the
+ * engine chooses, 0 never / 1 always the component-split kernel): info[0]
+ * registers per thread, [1] spill store bytes, [2] emitted multiply-add terms,
+ * [3] generate+compile ms, [4] cubin bytes, [5] 1 for a component-split
+ * kernel, [6] device functions, [7] components, [8] threads per CTA, [9]
+ * dynamic shared memory bytes.  text (if not NULL) receives the ptxas report
+ * (use_float < 0: the generated FP32 source instead).  Graphs that get no CG
+ * kernel (the engine runs the row interpreter) return SUS2SH_E_INPUT. */
+int sus2sh_cg_kernel_info(const char* path, int use_float, int split, int* info, char* text,
+                          size_t text_size);
 
 /* Compiles the per-edge kernels (k_basic, k_force, 128-thread CTAs) of one
  * model shape with NVRTC for sm_100a, as model load does for shapes without

@@ -1,29 +1,163 @@
-"""The model-specialised CG kernel is generated and NVRTC-compiled for sm_100a
-at model load (no GPU needed to compile)."""
+"""The model-specialised CG kernels are generated and NVRTC-compiled for sm_100a
+at model load (no GPU needed to compile).  Small graphs get one straight-line
+function; large graphs the component-split kernel.  The generated source of
+either is also compiled with the host C++ compiler and run on random basic
+moments, and its site energies and basic adjoints are compared with the FP64
+oracle's flat CG evaluation (oracle_cg_energy, the algorithm of
+src/force/sus2_sh.cu:4799-4846)."""
 import ctypes
+import os
+import re
+import subprocess
 
-from sus2sh import _lib
+import numpy as np
+import pytest
+
+import sus2sh_oracle as O
+from sus2sh import _lib, models
+
+FIELDS = ("regs", "spill", "terms", "ms", "cubin", "split", "functions", "components", "block", "smem")
 
 
-def _info(path, use_float):
+def _info(path, use_float, split=-1, text_size=8192):
     lib = _lib.load()
-    info = (ctypes.c_int * 5)()
-    txt = ctypes.create_string_buffer(8192)
-    rc = lib.sus2sh_cg_kernel_info(path.encode(), use_float, info, txt, 8192)
-    return rc, list(info), txt.value.decode()
+    info = (ctypes.c_int * len(FIELDS))()
+    txt = ctypes.create_string_buffer(text_size)
+    rc = lib.sus2sh_cg_kernel_info(path.encode(), use_float, split, info, txt, text_size)
+    return rc, dict(zip(FIELDS, list(info))), txt.value.decode()
 
 
 def test_l3k3_cg_kernel_compiles_without_spills(l3k3_path):
     rc, info, log = _info(l3k3_path, 1)
     assert rc == 0, log
-    regs, spill, terms, ms, cubin = info
-    assert 0 < regs <= 255 and spill == 0, log
+    assert info["split"] == 0 and info["functions"] == 1
+    assert 0 < info["regs"] <= 255 and info["spill"] == 0, log
     # 806 products: 606 forward terms + 200 fused terminal terms (x2) + 606 back terms (x2)
-    assert terms == 606 + 2 * 200 + 2 * 606
-    assert cubin > 0
+    assert info["terms"] == 606 + 2 * 200 + 2 * 606
+    assert info["cubin"] > 0
 
 
-def test_large_graph_stays_on_the_interpreter(l4k4_path):
+def test_large_graph_gets_the_split_kernel(l4k4_path):
+    # l4k4 body 5: 33,389 products in 116 (rank L, component M) components
     rc, info, log = _info(l4k4_path, 1)
+    assert rc == 0, _lib.load().sus2sh_last_error().decode()
+    assert info["split"] == 1 and info["components"] == 116
+    assert info["block"] == 128 and info["smem"] == 2 * 100 * 128 * 4
+    assert info["spill"] == 0, log
+
+
+def test_large_graph_without_split_runs_the_interpreter(l4k4_path):
+    rc, _, _ = _info(l4k4_path, 1, split=0)
     assert rc == -1
     assert "interpreter" in _lib.load().sus2sh_last_error().decode()
+
+
+# ---------------------------------------------------------------------------
+# host emulation of the generated CUDA source
+# ---------------------------------------------------------------------------
+_PRELUDE = r"""
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#define __device__
+#define __noinline__ __attribute__((noinline))
+#define __global__
+#define __launch_bounds__(...)
+#define __shared__
+#define __align__(n) __attribute__((aligned(n)))
+#define __syncthreads()
+struct EmuDim { unsigned x; };
+static EmuDim threadIdx, blockIdx, blockDim;
+template <class T> static inline T __ldg(const T* p) { return *p; }
+static inline long long __double_as_longlong(double d) { long long v; std::memcpy(&v, &d, 8); return v; }
+using std::fma;
+using std::fmaf;
+unsigned char smem_raw[232448] __attribute__((aligned(16)));
+"""
+
+_DRIVER = r"""
+extern "C" void run(int N, int block, const float* B, float* G, const int* type, const double* shift,
+                    const double* species, double* pe) {
+  D4* p4 = new D4[N];
+  for (int i = 0; i < N; ++i) {
+    long long t = type[i];
+    double w;
+    std::memcpy(&w, &t, 8);
+    p4[i] = D4{0, 0, 0, w};
+  }
+  blockDim.x = block;
+  for (int i = 0; i < N; ++i) {  // one lane at a time: every lane owns its shared-memory column
+    threadIdx.x = i % block;
+    blockIdx.x = i / block;
+    KERNEL(N, p4, B, G, shift, species, pe, 1);
+  }
+  delete[] p4;
+}
+"""
+
+
+def _emulate(path, split, tmp_path, N=45, seed=3):
+    rc, info, src = _info(path, -1, split=split, text_size=1 << 26)   # use_float < 0: FP32 source text
+    assert rc == 0, _lib.load().sus2sh_last_error().decode()
+    name = re.search(r"(sus2sh_cg\w+)\(int N", src).group(1)
+    block = info["block"]
+    canon = dict((int(b), int(c)) for b, c in re.findall(r"(?:sv\[|v)(\d+)(?: \* \d+\])? = __ldg\(B \+ (\d+) \* n", src))
+    cpp = tmp_path / "k.cpp"
+    cpp.write_text(_PRELUDE + src.replace('extern "C" __global__', "__global__") + _DRIVER.replace("KERNEL", name))
+    so = tmp_path / "k.so"
+    subprocess.check_call(["g++", "-O1", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)])
+    lib = ctypes.CDLL(str(so))
+    orc = O.Oracle(path)
+    m = orc.model
+    rng = np.random.default_rng(seed)
+    nb = m.alpha_basic_count
+    Bm = rng.normal(0.0, 1.0, (nb, N))
+    types = rng.integers(0, m.species_count, N).astype(np.int32)
+    pe0, G0 = orc.cg_energy(types, Bm)
+    ncanon = max(canon.values()) + 1
+    Bc = np.zeros((ncanon, N), np.float32)
+    for b, c in canon.items():
+        Bc[c] = Bm[b]
+    Gc = np.zeros((ncanon, N), np.float32)
+    pe = np.zeros(N)
+    shift = np.ascontiguousarray(m.shift_coeffs, dtype=np.float64)
+    species = np.ascontiguousarray(m.species_coeffs, dtype=np.float64)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    lib.run(N, block, P(Bc), P(Gc), P(types), P(shift), P(species), P(pe))
+    G = np.array([Gc[canon[b]] for b in range(nb)], dtype=np.float64)
+    scale = max(1.0, np.abs(pe0 - shift[types]).max())
+    return np.abs(pe - pe0).max() / scale, np.abs(G - G0).max() / np.abs(G0).max(), info
+
+
+@pytest.mark.parametrize("split", [0, 1])
+def test_generated_kernels_match_oracle_on_host(l3k3_path, tmp_path, split):
+    de, dg, info = _emulate(l3k3_path, split, tmp_path)
+    assert info["split"] == split
+    assert de < 1e-6 and dg < 1e-5, (de, dg)
+
+
+@pytest.fixture(scope="module")
+def body5_path(tmp_path_factory):
+    # l3k3 body 5: 5,475 products, above the single-function limit
+    p = str(tmp_path_factory.mktemp("models") / "l3k3b5.mtp")
+    return models.write_model(p, species=2, l_max=3, k_max=3, body_order=5, rb_size=8, seed=11)
+
+
+@pytest.fixture(scope="module")
+def body6_path(tmp_path_factory):
+    # l2k2 body 6: three layers, shared intermediates feed non-terminal rows
+    p = str(tmp_path_factory.mktemp("models") / "l2k2b6.mtp")
+    return models.write_model(p, species=2, l_max=2, k_max=2, body_order=6, rb_size=8, seed=12)
+
+
+def test_split_kernel_body5_matches_oracle_on_host(body5_path, tmp_path):
+    de, dg, info = _emulate(body5_path, -1, tmp_path)
+    assert info["split"] == 1 and info["components"] == 64
+    assert de < 1e-6 and dg < 1e-5, (de, dg)
+
+
+def test_split_kernel_body6_shared_intermediates_on_host(body6_path, tmp_path):
+    de, dg, info = _emulate(body6_path, 1, tmp_path)
+    assert info["split"] == 1
+    assert info["smem"] > 2 * 18 * info["block"] * 4   # 18 basics + shared intermediates
+    assert de < 1e-6 and dg < 1e-5, (de, dg)

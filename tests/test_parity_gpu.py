@@ -105,13 +105,36 @@ def test_open_boundaries(l3k3_path):
     compare(l3k3_path, mixed, types, pos + np.array([[0.0], [20.0], [0.0]]))
 
 
-def test_large_model_rational_three_species(l4k4_path):
-    # body-5 L=4 K=4 graph (product slots in HBM scratch).  The random model has
-    # site energies up to ~5e2 eV and force RMS ~4e2 eV/A, so the FP32 bars are
-    # relative: 1e-6 of the energy scale, 1e-5 of the force / virial RMS.
+@pytest.mark.parametrize("opts", [(), ("sus2_sh_cg_split=0",)], ids=["split_kernel", "row_interpreter"])
+def test_large_model_rational_three_species(l4k4_path, opts):
+    # body-5 L=4 K=4 graph: the component-split CG kernel (default for this
+    # size) and the row interpreter (product slots in HBM scratch).  The random
+    # model has site energies up to ~5e2 eV and force RMS ~4e2 eV/A, so the FP32
+    # bars are relative: 1e-6 of the energy scale, 1e-5 of the force / virial RMS.
     box, types, pos = structures.random_insertion(600, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=6)
-    compare(l4k4_path, box, types, pos, species=("Cu", "Zr", "Al"), relative=True)
-    compare(l4k4_path, box, types, pos, species=("Cu", "Zr", "Al"), fp64=True, relative=True)
+    compare(l4k4_path, box, types, pos, opts=opts, species=("Cu", "Zr", "Al"), relative=True)
+    compare(l4k4_path, box, types, pos, opts=opts, species=("Cu", "Zr", "Al"), fp64=True, relative=True)
+
+
+def test_large_model_uses_split_kernel(l4k4_path):
+    box, types, pos = structures.random_insertion(300, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=8)
+    pot = SUS2_SH(l4k4_path, types.size, ["Cu", "Zr", "Al"])
+    dev = torch.device("cuda")
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)
+    pot.compute(box, torch.as_tensor(types, device=dev), torch.as_tensor(pos.reshape(-1).copy(), device=dev),
+                z(types.size), z(3 * types.size), z(9 * types.size))
+    torch.cuda.synchronize()
+    info = pot.info()
+    pot.close()
+    assert info["cg_kind"] == 2 and 0 < info["cg_loaded_registers"] <= 255
+    assert info["cg_local_bytes"] <= 1024, info["cg_local_bytes"]
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_config0_split_kernel(l3k3_path, fp64):
+    # the component-split CG kernel forced on the l3k3 model (120 one-value components)
+    box, types, pos = structures.fcc(8, 8, 8, 3.8, (0.5, 0.5), 0.05, seed=1)
+    compare(l3k3_path, box, types, pos, opts=("sus2_sh_cg_split=1",), fp64=fp64)
 
 
 def test_reference_rounding_option(l3k3_path):
