@@ -83,6 +83,27 @@ struct DevBuf {
   }
 };
 
+// Derivative series of Chebyshev expansions: for every mu,
+// sum_n c[mu][n] T_n'(x) = sum_n d[mu][n] T_n(x) with d[mu][rb-1] = 0, by the
+// recurrence d_{n-1} = d_{n+1} + 2 n c_n (n = rb-1 .. 1) and d_0 halved.  The
+// force kernel evaluates R' from these instead of a dT_n recurrence.
+std::vector<double> chebyshev_derivative(const std::vector<double>& c, int kmu, int rb) {
+  std::vector<double> d(c.size(), 0.0);
+  for (int mu = 0; mu < kmu; ++mu) {
+    const double* cm = &c[static_cast<size_t>(mu) * rb];
+    double* dm = &d[static_cast<size_t>(mu) * rb];
+    double next2 = 0.0, next1 = 0.0;  // d_{n+1}, d_n while walking down
+    for (int n = rb - 1; n >= 1; --n) {
+      const double v = next2 + 2.0 * n * cm[n];  // d_{n-1}
+      dm[n - 1] = v;
+      next2 = next1;
+      next1 = v;
+    }
+    if (rb > 1) dm[0] *= 0.5;
+  }
+  return d;
+}
+
 // ---------------------------------------------------------------------------
 // CG program: the layered rows of the saved sh_products compiled to the
 // slot machine executed by k_product (see engine.cu for the row kinds).
@@ -291,6 +312,7 @@ struct Engine {
   bool use_float = true;
   RadialSetup rs{};
   std::vector<double> coef;        // [kmu][rb] unscaled
+  std::vector<double> dcoef;       // [kmu][rb] derivative series of coef (chebyshev_derivative)
   std::vector<double> pair_table;  // [S*S][stride]
 
   // model on device
@@ -356,6 +378,7 @@ struct Engine {
   // two-layer gate models
   bool gate = false;
   std::vector<double> gate_coef;  // [kmu][rb] first-layer radial coefficients
+  std::vector<double> gate_dcoef;  // their derivative series
   GateProgDev gprog{};
   DevBuf<int> d_g_basic, d_g_prod, d_g_qslot, d_g_qbody;
   DevBuf<double> d_g_coef, d_g_w, d_g_mix, d_g_add;
@@ -483,6 +506,8 @@ struct Engine {
     }
     if (pair_table.size() > static_cast<size_t>(kMaxPairTable))
       throw InputError("SUS2_SH radial pair table too large (species_count^2 * (2*radial_funcs+1) > 8192).");
+    dcoef = chebyshev_derivative(coef, kmu, rb);
+    if (gate) gate_dcoef = chebyshev_derivative(gate_coef, kmu, rb);
     // device uploads
     d_code.upload(prog.code);
     if (use_float) {
@@ -597,6 +622,7 @@ struct Engine {
       a.atom_cell = nullptr;
     }
     for (size_t k = 0; k < coef.size(); ++k) a.coef[k] = static_cast<T>(coef[k]);
+    for (size_t k = 0; k < dcoef.size(); ++k) a.dcoef[k] = static_cast<T>(dcoef[k]);
     return a;
   }
 
@@ -605,6 +631,7 @@ struct Engine {
   EdgeArgs<T> edge_args_gate() const {
     EdgeArgs<T> a = edge_args<T>();
     for (size_t k = 0; k < gate_coef.size(); ++k) a.coef[k] = static_cast<T>(gate_coef[k]);
+    for (size_t k = 0; k < gate_dcoef.size(); ++k) a.dcoef[k] = static_cast<T>(gate_dcoef[k]);
     return a;
   }
 

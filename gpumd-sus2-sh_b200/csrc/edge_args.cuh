@@ -37,6 +37,7 @@ struct EdgeArgs {
   const T* gate_deriv;       // [Kmu][N] dG/dh
   T* gate_adj;               // [Kmu][N] dE/dh accumulated by k_force (atomics)
   T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
+  T dcoef[kMaxCoef];         // d[mu][n]: sum_n c[mu][n] T_n'(xi) = sum_n d[mu][n] T_n(xi), d[mu][RB-1] = 0
 };
 
 }  // namespace sus2sh

@@ -42,7 +42,7 @@ __device__ __forceinline__ Edge<float> make_edge<float>(double dx, double dy, do
   e.uy = e.dy * e.rinv;
   e.uz = e.dz * e.rinv;
   // (r - rc) without FP32 cancellation near the cutoff
-  e.dr = static_cast<float>(r2 - rc2) / (e.r + static_cast<float>(rc));
+  e.dr = __fdividef(static_cast<float>(r2 - rc2), e.r + static_cast<float>(rc));
   return e;
 }
 

@@ -16,12 +16,13 @@
 #include "edge_common.cuh"
 #include "sh_math.cuh"
 
-// Minimum resident CTAs per SM of the FP32 edge kernels (register caps).
-// Measured on the 1.024M-atom l3k3 workload: k_force at 4 CTAs (128 registers,
-// 8 B spill) runs 1.55 ms vs 1.87 ms at its natural 167 registers; capping
-// k_basic below its natural 126 registers (5 CTAs) spills and loses.
+// Minimum resident CTAs per SM of the FP32 edge kernels (register caps, for
+// shapes with at most 64 basic moments).  Measured on the 1.024M-atom l3k3
+// workload: k_force at 4 CTAs (128 registers, 32 B spill) runs 1.38 ms vs
+// 1.54 ms at 3 CTAs; k_basic at 4 CTAs 0.71 ms vs 0.75 ms at its natural 140
+// registers.
 #ifndef SUS2_BASIC_MIN_BLOCKS
-#define SUS2_BASIC_MIN_BLOCKS 1
+#define SUS2_BASIC_MIN_BLOCKS 4
 #endif
 #ifndef SUS2_FORCE_MIN_BLOCKS
 #define SUS2_FORCE_MIN_BLOCKS 4
@@ -35,7 +36,11 @@ namespace edge {
 // GATE: two-layer gate models' main pass, every R_mu of neighbour j scaled by
 // the gate multiplier G_{j,mu} (gpu_sh_compute_basic_gate_main, sus2_sh.cu:4247-4314).
 template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
-__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK : 1) k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
+__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1) <= 64 &&
+                                                 SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1
+                                             ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK
+                                             : 1)
+    k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_tab = reinterpret_cast<T*>(smem_raw);
   load_pair_table(a, s_tab);
@@ -72,18 +77,21 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_BASIC_MIN_BLOCKS
 #pragma unroll
       for (int mu = 0; mu < KMU; ++mu) R[mu] *= a.gate_mult[static_cast<size_t>(mu) * a.N + j];
     }
-    T Y[C];
-    sh_values<L>(e.ux, e.uy, e.uz, Y);
+    T P[C];  // harmonic polynomials; their normalisation is applied once per atom below
+    sh_poly<L>(e.ux, e.uy, e.uz, P);
 #pragma unroll
     for (int k = 0; k < K; ++k)
 #pragma unroll
       for (int l = 0; l <= L; ++l)
 #pragma unroll
         for (int m = 0; m <= 2 * l; ++m)
-          acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], Y[l * l + m], acc[k * C + l * l + m]);
+          acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], P[l * l + m], acc[k * C + l * l + m]);
   }
 #pragma unroll
-  for (int b = 0; b < NB; ++b) B[static_cast<size_t>(b) * a.N + i] = acc[b];
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+      B[static_cast<size_t>(k * C + c) * a.N + i] = T(sh_poly_norm<L>(c)) * acc[k * C + c];
 }
 
 // ---------------------------------------------------------------------------
@@ -111,8 +119,13 @@ struct Scatter<double> {
 // sus2_sh.cu:6555-6693 with compute_sh_edge_derivative_gate_main_cached_grads
 // :6077-6121): R, R' scaled by G_{j,mu}, and dE/dh_{j,mu} += dG/dh_{j,mu}
 // R_mu sum_m g_{mu,m} Y_m accumulated on the neighbour.
+// The register cap applies to shapes whose adjoints fit it (K (L+1)^2 <= 64);
+// larger shapes keep up to 255 registers.  The same holds for k_basic.
 template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
-__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1 ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK : 1)
+__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1) <= 64 &&
+                                                 SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1
+                                             ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK
+                                             : 1)
     k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
             void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
             double sign) {
@@ -123,9 +136,14 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS
   if (i >= a.N) return;
   constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
   const T wscale = weight ? static_cast<T>(weight[i]) : T(1);
+  // adjoints scaled by the harmonic normalisation, so every edge works with
+  // the bare polynomials P_lm (Y_lm = c_lm P_lm)
   T g[NB];
 #pragma unroll
-  for (int b = 0; b < NB; ++b) g[b] = wscale * G[static_cast<size_t>(b) * a.N + i];
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+      g[k * C + c] = (wscale * T(sh_poly_norm<L>(c))) * G[static_cast<size_t>(k * C + c) * a.N + i];
   T fx = T(0), fy = T(0), fz = T(0);
   T w[9];
 #pragma unroll
@@ -151,47 +169,82 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && SUS2_FORCE_MIN_BLOCKS
     if (r2 >= rc2) continue;
     const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
     const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
-    T R[KMU], dR[KMU];
-    radial_values_ders<T, KMU, RB>(a, row, e, R, dR);
-    T Y[C];
-    sh_values<L>(e.ux, e.uy, e.uz, Y);
-    if constexpr (GATE) {
+    // R_mu = f s_mu, dR_mu = df s_mu + f fac sd_mu with f = s_pair (r-rc)^2,
+    // s_mu = sum_n c[mu][n] T_n, sd_mu = sum_n d[mu][n] T_n (derivative series);
+    // the common factors are applied after the contractions below
+    const T ps = row[2 * KMU];
+    const T f = ps * e.dr * e.dr;
+    const T df = T(2) * ps * e.dr;
+    const bool rational = a.rs.rational != 0;
+    T t[RB], fac = T(1);
+    if (a.rs.shared_xi) {
+      const T half_scal = T(0.5) * row[0];
+      T xi, dxi;
+      radial_map<T>(half_scal * (e.r - row[1]), rational, xi, dxi);
+      fac = half_scal * dxi;
+      chebyshev<RB>(xi, t);
+    }
+    T P[C];
+    sh_poly<L>(e.ux, e.uy, e.uz, P);
+    // Gt_lm = sum_k g_klm s_kl, Ht_lm = sum_k g_klm sd_kl; sG = P.Gt, sH = P.Ht;
+    // the radial sums of one l at a time
+    T Gt[C];
+    T sG = T(0), sH = T(0);
 #pragma unroll
-      for (int k = 0; k < K; ++k)
+    for (int l = 0; l <= L; ++l) {
+      T sk[K], sdk[K];
 #pragma unroll
-        for (int l = 0; l <= L; ++l) {
-          const int mu = k * (L + 1) + l;
+      for (int k = 0; k < K; ++k) {
+        const int mu = k * (L + 1) + l;
+        T scale = T(1);
+        if (!a.rs.shared_xi) {
+          const T half_scal = T(0.5) * row[2 * mu];
+          T xi, dxi;
+          radial_map<T>(half_scal * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+          scale = half_scal * dxi;
+          chebyshev<RB>(xi, t);
+        }
+        T v = T(0), d = T(0);
+#pragma unroll
+        for (int n = 0; n < RB; ++n) {
+          v = fma(a.coef[mu * RB + n], t[n], v);
+          if (n + 1 < RB) d = fma(a.dcoef[mu * RB + n], t[n], d);
+        }
+        sk[k] = v;
+        sdk[k] = scale * d;
+        if constexpr (GATE) {
           T p = T(0);
 #pragma unroll
-          for (int m = 0; m <= 2 * l; ++m) p = fma(g[k * C + l * l + m], Y[l * l + m], p);
+          for (int m = 0; m <= 2 * l; ++m) p = fma(g[k * C + l * l + m], P[l * l + m], p);
           const size_t at = static_cast<size_t>(mu) * a.N + j;
-          atomicAdd(a.gate_adj + at, p * R[mu] * a.gate_deriv[at]);
+          atomicAdd(a.gate_adj + at, p * (f * v) * a.gate_deriv[at]);
           const T gm = a.gate_mult[at];
-          R[mu] *= gm;
-          dR[mu] *= gm;
+          sk[k] *= gm;
+          sdk[k] *= gm;
         }
-    }
-    T Gy[C];
-    T s = T(0);
-#pragma unroll
-    for (int l = 0; l <= L; ++l)
+      }
 #pragma unroll
       for (int m = 0; m <= 2 * l; ++m) {
         T gv = T(0), hv = T(0);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          gv = fma(g[k * C + l * l + m], R[k * (L + 1) + l], gv);
-          hv = fma(g[k * C + l * l + m], dR[k * (L + 1) + l], hv);
+          gv = fma(g[k * C + l * l + m], sk[k], gv);
+          hv = fma(g[k * C + l * l + m], sdk[k], hv);
         }
-        Gy[l * l + m] = gv;
-        s = fma(hv, Y[l * l + m], s);
+        Gt[l * l + m] = gv;
+        sG = fma(gv, P[l * l + m], sG);
+        sH = fma(hv, P[l * l + m], sH);
       }
+    }
+    // radial part s = dE/dr along u; tangential part f (V - (u.V) u) / r
+    const T s = df * sG + (f * fac) * sH;
     T vx, vy, vz;
-    sh_grad_contract<L>(e.ux, e.uy, e.uz, Gy, vx, vy, vz);
+    sh_poly_grad_contract<L>(e.ux, e.uy, e.uz, Gt, vx, vy, vz);
     const T uv = e.ux * vx + e.uy * vy + e.uz * vz;
-    const T dEx = s * e.ux + (vx - uv * e.ux) * e.rinv;
-    const T dEy = s * e.uy + (vy - uv * e.uy) * e.rinv;
-    const T dEz = s * e.uz + (vz - uv * e.uz) * e.rinv;
+    const T ft = f * e.rinv;
+    const T dEx = s * e.ux + (vx - uv * e.ux) * ft;
+    const T dEy = s * e.uy + (vy - uv * e.uy) * ft;
+    const T dEz = s * e.uz + (vz - uv * e.uz) * ft;
     fx += dEx;
     fy += dEy;
     fz += dEz;

@@ -224,50 +224,80 @@ SUS2_HD void sh_grad_solid(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
   }
 }
 
-// Y[l*l+l+m] for l <= L at unit vector (x, y, z).
-template <int L, typename T>
-SUS2_HD void sh_values(T x, T y, T z, T* Y) {
-  if constexpr (L > 4) {
-    sh_values_solid<L>(x, y, z, Y);
-    return;
+// Normalisation c_i of the polynomial forms, Y_i = c_i P_i (flat index
+// i = l*l + l + m, L <= 4).  Models with L > 4 take every harmonic from the
+// solid-harmonic path, already normalised (c_i = 1).
+template <int L>
+SUS2_HD constexpr double sh_poly_norm(int i) {
+  if (L > 4) return 1.0;
+  switch (i) {
+    case 0: return YC::c00;
+    case 1: case 2: case 3: return YC::c1;
+    case 4: case 5: case 7: return YC::c2a;
+    case 6: return YC::c20;
+    case 8: return YC::c22;
+    case 9: case 15: return YC::c33;
+    case 10: return YC::c32;
+    case 11: case 13: return YC::c31;
+    case 12: return YC::c30;
+    case 14: return YC::c3p2;
+    case 16: return YC::c44m;
+    case 17: case 23: return YC::c43;
+    case 18: return YC::c42m;
+    case 19: case 21: return YC::c41;
+    case 20: return YC::c40;
+    case 22: return YC::c42;
+    case 24: return YC::c44;
+    default: return 1.0;
   }
-  Y[0] = T(YC::c00);
-  if (L < 1) return;
-  Y[1] = T(YC::c1) * y;
-  Y[2] = T(YC::c1) * z;
-  Y[3] = T(YC::c1) * x;
-  if (L < 2) return;
-  const T x2 = x * x, y2 = y * y, z2 = z * z;
-  Y[4] = T(YC::c2a) * x * y;
-  Y[5] = T(YC::c2a) * y * z;
-  Y[6] = T(YC::c20) * (T(2) * z2 - x2 - y2);
-  Y[7] = T(YC::c2a) * x * z;
-  Y[8] = T(YC::c22) * (x2 - y2);
-  if (L < 3) return;
-  const T a31 = T(4) * z2 - x2 - y2;
-  Y[9] = T(YC::c33) * y * (T(3) * x2 - y2);
-  Y[10] = T(YC::c32) * x * y * z;
-  Y[11] = T(YC::c31) * y * a31;
-  Y[12] = T(YC::c30) * z * (T(2) * z2 - T(3) * x2 - T(3) * y2);
-  Y[13] = T(YC::c31) * x * a31;
-  Y[14] = T(YC::c3p2) * z * (x2 - y2);
-  Y[15] = T(YC::c33) * x * (x2 - T(3) * y2);
-  if (L < 4) return;
-  const T r2 = x2 + y2;
-  Y[16] = T(YC::c44m) * x * y * (x2 - y2);
-  Y[17] = T(YC::c43) * y * z * (T(3) * x2 - y2);
-  Y[18] = T(YC::c42m) * x * y * (T(6) * z2 - r2);
-  Y[19] = T(YC::c41) * y * z * (T(4) * z2 - T(3) * r2);
-  Y[20] = T(YC::c40) * (T(8) * z2 * z2 - T(24) * z2 * r2 + T(3) * r2 * r2);
-  Y[21] = T(YC::c41) * x * z * (T(4) * z2 - T(3) * r2);
-  Y[22] = T(YC::c42) * (x2 - y2) * (T(6) * z2 - r2);
-  Y[23] = T(YC::c43) * x * z * (x2 - T(3) * y2);
-  Y[24] = T(YC::c44) * (x2 * x2 - T(6) * x2 * y2 + y2 * y2);
 }
 
-// V = sum_lm G[lm] * grad P_lm(u), P_lm the homogeneous polynomial of Y_lm.
+// P_i(x, y, z), the homogeneous polynomial of Y_i without its normalisation
+// (L <= 4; L > 4: the normalised solid-harmonic values).
 template <int L, typename T>
-SUS2_HD void sh_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
+SUS2_HD void sh_poly(T x, T y, T z, T* P) {
+  if constexpr (L > 4) {
+    sh_values_solid<L>(x, y, z, P);
+    return;
+  }
+  P[0] = T(1);
+  if (L < 1) return;
+  P[1] = y;
+  P[2] = z;
+  P[3] = x;
+  if (L < 2) return;
+  const T x2 = x * x, y2 = y * y, z2 = z * z;
+  P[4] = x * y;
+  P[5] = y * z;
+  P[6] = T(2) * z2 - x2 - y2;
+  P[7] = x * z;
+  P[8] = x2 - y2;
+  if (L < 3) return;
+  const T a31 = T(4) * z2 - x2 - y2;
+  P[9] = y * (T(3) * x2 - y2);
+  P[10] = x * y * z;
+  P[11] = y * a31;
+  P[12] = z * (T(2) * z2 - T(3) * x2 - T(3) * y2);
+  P[13] = x * a31;
+  P[14] = z * (x2 - y2);
+  P[15] = x * (x2 - T(3) * y2);
+  if (L < 4) return;
+  const T r2 = x2 + y2;
+  P[16] = x * y * (x2 - y2);
+  P[17] = y * z * (T(3) * x2 - y2);
+  P[18] = x * y * (T(6) * z2 - r2);
+  P[19] = y * z * (T(4) * z2 - T(3) * r2);
+  P[20] = T(8) * z2 * z2 - T(24) * z2 * r2 + T(3) * r2 * r2;
+  P[21] = x * z * (T(4) * z2 - T(3) * r2);
+  P[22] = (x2 - y2) * (T(6) * z2 - r2);
+  P[23] = x * z * (x2 - T(3) * y2);
+  P[24] = x2 * x2 - T(6) * x2 * y2 + y2 * y2;
+}
+
+// V = sum_i G[i] grad P_i (L <= 4; L > 4: gradients of the normalised solid
+// harmonics).
+template <int L, typename T>
+SUS2_HD void sh_poly_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
   if constexpr (L > 4) {
     sh_grad_solid<L>(x, y, z, G, vx, vy, vz);
     return;
@@ -276,34 +306,28 @@ SUS2_HD void sh_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
   vy = T(0);
   vz = T(0);
   if (L < 1) return;
-  {
-    const T c = T(YC::c1);
-    vx += c * G[3];
-    vy += c * G[1];
-    vz += c * G[2];
-  }
+  vx = G[3];
+  vy = G[1];
+  vz = G[2];
   if (L < 2) return;
   const T x2 = x * x, y2 = y * y, z2 = z * z;
   {
-    const T g4 = T(YC::c2a) * G[4], g5 = T(YC::c2a) * G[5], g6 = T(YC::c20) * G[6];
-    const T g7 = T(YC::c2a) * G[7], g8 = T(YC::c22) * G[8];
+    const T g4 = G[4], g5 = G[5], g6 = G[6], g7 = G[7], g8 = G[8];
     vx += g4 * y + g7 * z + T(2) * x * (g8 - g6);
     vy += g4 * x + g5 * z - T(2) * y * (g6 + g8);
     vz += g5 * y + g7 * x + T(4) * z * g6;
   }
   if (L < 3) return;
   {
-    const T g9 = T(YC::c33) * G[9], g10 = T(YC::c32) * G[10], g11 = T(YC::c31) * G[11];
-    const T g12 = T(YC::c30) * G[12], g13 = T(YC::c31) * G[13], g14 = T(YC::c3p2) * G[14];
-    const T g15 = T(YC::c33) * G[15];
+    const T g9 = G[9], g10 = G[10], g11 = G[11], g12 = G[12], g13 = G[13], g14 = G[14], g15 = G[15];
     const T xy = x * y, xz = x * z, yz = y * z;
-    // Y3-3 = y(3x^2-y^2): (6xy, 3x^2-3y^2, 0)
-    // Y3-2 = xyz: (yz, xz, xy)
-    // Y3-1 = y(4z^2-x^2-y^2): (-2xy, 4z^2-x^2-3y^2, 8yz)
-    // Y30 = z(2z^2-3x^2-3y^2): (-6xz, -6yz, 6z^2-3x^2-3y^2)
-    // Y31 = x(4z^2-x^2-y^2): (4z^2-3x^2-y^2, -2xy, 8xz)
-    // Y32 = z(x^2-y^2): (2xz, -2yz, x^2-y^2)
-    // Y33 = x(x^2-3y^2): (3x^2-3y^2, -6xy, 0)
+    // P9 = y(3x^2-y^2): (6xy, 3x^2-3y^2, 0)
+    // P10 = xyz: (yz, xz, xy)
+    // P11 = y(4z^2-x^2-y^2): (-2xy, 4z^2-x^2-3y^2, 8yz)
+    // P12 = z(2z^2-3x^2-3y^2): (-6xz, -6yz, 6z^2-3x^2-3y^2)
+    // P13 = x(4z^2-x^2-y^2): (4z^2-3x^2-y^2, -2xy, 8xz)
+    // P14 = z(x^2-y^2): (2xz, -2yz, x^2-y^2)
+    // P15 = x(x^2-3y^2): (3x^2-3y^2, -6xy, 0)
     vx += T(6) * xy * g9 + yz * g10 - T(2) * xy * g11 - T(6) * xz * g12 +
           (T(4) * z2 - T(3) * x2 - y2) * g13 + T(2) * xz * g14 + T(3) * (x2 - y2) * g15;
     vy += T(3) * (x2 - y2) * g9 + xz * g10 + (T(4) * z2 - x2 - T(3) * y2) * g11 -
@@ -313,48 +337,70 @@ SUS2_HD void sh_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
   }
   if (L < 4) return;
   {
-    const T g16 = T(YC::c44m) * G[16], g17 = T(YC::c43) * G[17], g18 = T(YC::c42m) * G[18];
-    const T g19 = T(YC::c41) * G[19], g20 = T(YC::c40) * G[20], g21 = T(YC::c41) * G[21];
-    const T g22 = T(YC::c42) * G[22], g23 = T(YC::c43) * G[23], g24 = T(YC::c44) * G[24];
-    const T xy = x * y, xz = x * z, yz = y * z, xyz = x * y * z, r2 = x2 + y2;
-    // Y4-4 = x^3 y - x y^3
+    const T g16 = G[16], g17 = G[17], g18 = G[18], g19 = G[19], g20 = G[20];
+    const T g21 = G[21], g22 = G[22], g23 = G[23], g24 = G[24];
+    const T xyz = x * y * z, r2 = x2 + y2;
+    // P16 = x^3 y - x y^3
     vx += g16 * (T(3) * x2 * y - y * y2);
     vy += g16 * (x * x2 - T(3) * x * y2);
-    // Y4-3 = 3x^2 yz - y^3 z
+    // P17 = 3x^2 yz - y^3 z
     vx += g17 * T(6) * xyz;
     vy += g17 * (T(3) * x2 * z - T(3) * y2 * z);
     vz += g17 * (T(3) * x2 * y - y * y2);
-    // Y4-2 = 6xyz^2 - x^3 y - x y^3
+    // P18 = 6xyz^2 - x^3 y - x y^3
     vx += g18 * (T(6) * y * z2 - T(3) * x2 * y - y * y2);
     vy += g18 * (T(6) * x * z2 - x * x2 - T(3) * x * y2);
     vz += g18 * T(12) * xyz;
-    // Y4-1 = 4yz^3 - 3x^2 yz - 3y^3 z
+    // P19 = 4yz^3 - 3x^2 yz - 3y^3 z
     vx += g19 * (-T(6) * xyz);
     vy += g19 * (T(4) * z * z2 - T(3) * x2 * z - T(9) * y2 * z);
     vz += g19 * (T(12) * y * z2 - T(3) * x2 * y - T(3) * y * y2);
-    // Y40 = 8z^4 - 24 z^2 r2 + 3 r2^2, r2 = x^2 + y^2
+    // P20 = 8z^4 - 24 z^2 r2 + 3 r2^2, r2 = x^2 + y^2
     const T a40 = T(12) * r2 - T(48) * z2;
     vx += g20 * a40 * x;
     vy += g20 * a40 * y;
     vz += g20 * (T(32) * z * z2 - T(48) * z * r2);
-    // Y41 = 4xz^3 - 3x^3 z - 3x y^2 z
+    // P21 = 4xz^3 - 3x^3 z - 3x y^2 z
     vx += g21 * (T(4) * z * z2 - T(9) * x2 * z - T(3) * y2 * z);
     vy += g21 * (-T(6) * xyz);
     vz += g21 * (T(12) * x * z2 - T(3) * x * x2 - T(3) * x * y2);
-    // Y42 = 6x^2 z^2 - 6y^2 z^2 - x^4 + y^4
+    // P22 = 6x^2 z^2 - 6y^2 z^2 - x^4 + y^4
     vx += g22 * (T(12) * x * z2 - T(4) * x * x2);
     vy += g22 * (T(4) * y * y2 - T(12) * y * z2);
     vz += g22 * (T(12) * (x2 - y2) * z);
-    // Y43 = x^3 z - 3x y^2 z
+    // P23 = x^3 z - 3x y^2 z
     vx += g23 * (T(3) * x2 * z - T(3) * y2 * z);
     vy += g23 * (-T(6) * xyz);
     vz += g23 * (x * x2 - T(3) * x * y2);
-    // Y44 = x^4 - 6x^2 y^2 + y^4
+    // P24 = x^4 - 6x^2 y^2 + y^4
     vx += g24 * (T(4) * x * x2 - T(12) * x * y2);
     vy += g24 * (T(4) * y * y2 - T(12) * x2 * y);
-    (void)xy;
-    (void)xz;
-    (void)yz;
+  }
+}
+
+// Y[l*l+l+m] for l <= L at unit vector (x, y, z).
+template <int L, typename T>
+SUS2_HD void sh_values(T x, T y, T z, T* Y) {
+  constexpr int C = (L + 1) * (L + 1);
+  sh_poly<L>(x, y, z, Y);
+  if constexpr (L <= 4) {
+#pragma unroll
+    for (int i = 0; i < C; ++i) Y[i] = T(sh_poly_norm<L>(i)) * Y[i];
+  }
+}
+
+// V = sum_lm G[lm] * grad P_lm(u), P_lm the homogeneous polynomial of Y_lm
+// (normalisation included).
+template <int L, typename T>
+SUS2_HD void sh_grad_contract(T x, T y, T z, const T* G, T& vx, T& vy, T& vz) {
+  if constexpr (L > 4) {
+    sh_grad_solid<L>(x, y, z, G, vx, vy, vz);
+  } else {
+    constexpr int C = (L + 1) * (L + 1);
+    T Gs[C];
+#pragma unroll
+    for (int i = 0; i < C; ++i) Gs[i] = T(sh_poly_norm<L>(i)) * G[i];
+    sh_poly_grad_contract<L>(x, y, z, Gs, vx, vy, vz);
   }
 }
 
