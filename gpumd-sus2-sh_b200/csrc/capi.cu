@@ -622,7 +622,8 @@ struct Engine {
       a.atom_cell = nullptr;
     }
     for (size_t k = 0; k < coef.size(); ++k) a.coef[k] = static_cast<T>(coef[k]);
-    for (size_t k = 0; k < dcoef.size(); ++k) a.dcoef[k] = static_cast<T>(dcoef[k]);
+    if (2 * coef.size() <= static_cast<size_t>(kMaxCoef))
+      for (size_t k = 0; k < dcoef.size(); ++k) a.coef[coef.size() + k] = static_cast<T>(dcoef[k]);
     return a;
   }
 
@@ -631,7 +632,8 @@ struct Engine {
   EdgeArgs<T> edge_args_gate() const {
     EdgeArgs<T> a = edge_args<T>();
     for (size_t k = 0; k < gate_coef.size(); ++k) a.coef[k] = static_cast<T>(gate_coef[k]);
-    for (size_t k = 0; k < gate_dcoef.size(); ++k) a.dcoef[k] = static_cast<T>(gate_dcoef[k]);
+    if (2 * gate_coef.size() <= static_cast<size_t>(kMaxCoef))
+      for (size_t k = 0; k < gate_dcoef.size(); ++k) a.coef[gate_coef.size() + k] = static_cast<T>(gate_dcoef[k]);
     return a;
   }
 

@@ -36,8 +36,12 @@ struct EdgeArgs {
   const T* gate_mult;        // [Kmu][N] G_{j,mu} = 1 + A tanh(a_j h_{j,mu})
   const T* gate_deriv;       // [Kmu][N] dG/dh
   T* gate_adj;               // [Kmu][N] dE/dh accumulated by k_force (atomics)
-  T coef[kMaxCoef];          // c[mu][n] (uniform across lanes)
-  T dcoef[kMaxCoef];         // d[mu][n]: sum_n c[mu][n] T_n'(xi) = sum_n d[mu][n] T_n(xi), d[mu][RB-1] = 0
+  // c[mu][n] (uniform across lanes), then, when 2 kmu rb <= kMaxCoef, the
+  // derivative series d[mu][n] at offset kmu rb:
+  // sum_n c[mu][n] T_n'(xi) = sum_n d[mu][n] T_n(xi), d[mu][rb-1] = 0.
+  // One array keeps the FP32 kernel parameters under 4 KB, where every
+  // coefficient is an immediate constant-bank operand.
+  T coef[kMaxCoef];
 };
 
 }  // namespace sus2sh

@@ -205,10 +205,21 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
           chebyshev<RB>(xi, t);
         }
         T v = T(0), d = T(0);
+        if constexpr (2 * KMU * RB <= kMaxCoef) {
+          // derivative series stored after the coefficients
 #pragma unroll
-        for (int n = 0; n < RB; ++n) {
-          v = fma(a.coef[mu * RB + n], t[n], v);
-          if (n + 1 < RB) d = fma(a.dcoef[mu * RB + n], t[n], d);
+          for (int n = 0; n < RB; ++n) {
+            v = fma(a.coef[mu * RB + n], t[n], v);
+            if (n + 1 < RB) d = fma(a.coef[KMU * RB + mu * RB + n], t[n], d);
+          }
+        } else {
+          T tt[RB], dt[RB];
+          chebyshev_d<RB>(t[RB > 1 ? 1 : 0], tt, dt);
+#pragma unroll
+          for (int n = 0; n < RB; ++n) {
+            v = fma(a.coef[mu * RB + n], t[n], v);
+            d = fma(a.coef[mu * RB + n], dt[n], d);
+          }
         }
         sk[k] = v;
         sdk[k] = scale * d;
