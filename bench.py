@@ -41,6 +41,8 @@ CELLS = (80, 80, 40)
 A = 3.8
 DT = 0.5
 TEMP = 200.0
+SKIN = 1.0  # Verlet skin (A)
+REBUILD = 10  # forced neighbour rebuild interval (steps)
 
 
 def parse_args():
@@ -50,7 +52,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
-    ap.add_argument("--fp64-steps", type=int, default=50)
+    ap.add_argument("--fp64-steps", type=int, default=-1,
+                    help="timed steps of the FP64-engine leg (default: the same as --steps, so both legs "
+                         "run under the same thermal and power conditions; 0 skips it)")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch-cell and large-model fields")
@@ -128,6 +132,21 @@ def edges_within(box, pos, rc):
     return int(counts.sum()) - pos.shape[1]  # minus self
 
 
+# DRAM bytes of one k_force launch (dram__bytes_read.sum + dram__bytes_write.sum)
+# from one ncu capture of the 524,288-atom l3k3 case (64x64x32 FCC cells, FP32,
+# 256-thread CTAs): 292.33 MB read + 43.09 MB written.  The traffic grows with
+# the atom count, so the bench scales it per atom.
+K_FORCE_DRAM_BYTES_PER_ATOM = (292.33e6 + 43.09e6) / 524288
+
+
+def k_force_algorithmic_bytes(nbasic, listed_per_atom):
+    """Bytes k_force must move per atom: adjoints G (4 nbasic), position and
+    species (32), neighbour count and list (4 + 4 per listed neighbour), the
+    FP32 scatter buffer (16) and the FP64 force (24, read + written) and
+    virial (72, read + written) it accumulates into."""
+    return 4 * nbasic + 32 + 4 + 4 * listed_per_atom + 16 + 2 * 24 + 2 * 72
+
+
 def flops_model(kmu, rb, C, Bb, P):
     """Counting rule for algorithmic work (FMA = 2 flops)."""
     per_edge_basic = kmu * (2 * rb + 4) + 6 * C + 2 * Bb
@@ -155,7 +174,7 @@ def make_workload(model_dir, rank):
 def run_md(torch, path, box, types, pos, vel, masses, steps, warmup, fp64, world, clocks=None):
     from sus2sh import SUS2_SH
     from sus2sh.md import NVE
-    opts = ["Cu", "Zr", "sus2_sh_skin=1.0", "sus2_sh_rebuild_interval=10"] + (["sus2_float=0"] if fp64 else [])
+    opts = ["Cu", "Zr", f"sus2_sh_skin={SKIN}", f"sus2_sh_rebuild_interval={REBUILD}"] + (["sus2_float=0"] if fp64 else [])
     pot = SUS2_SH(path, types.size, opts)
     md = NVE(pot, box, types, pos, vel, masses, dt_fs=DT)
     md.initial_force()
@@ -390,6 +409,8 @@ def reference_arm(args):
 
 def main():
     args = parse_args()
+    if args.fp64_steps < 0:
+        args.fp64_steps = args.steps
     if args.impl == "reference":
         reference_arm(args)
         return
@@ -446,7 +467,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded 80x80x40 FCC Cu-Zr 64/36, MB velocities 200 K; seeded random l3k3 model)",
                 "config": {"workload": "1.024M-atom l3k3 Cu-Zr NVE MD, FP32 engine", "atoms_per_gpu": N,
-                           "dt_fs": DT, "skin_A": 1.0, "rebuild_every": 10, "rc_A": pot.rc,
+                           "dt_fs": DT, "skin_A": SKIN, "rebuild_every": REBUILD, "rc_A": pot.rc,
                            "model": "SUS2-SH L3 K3 body4 rb8 (248 moments, 806 products)",
                            "l2": "inputs larger than L2 (positions+neighbour list+moments > 126 MB)",
                            "parallelism": f"replicas x{world}"},
@@ -459,7 +480,12 @@ def main():
                 "stage_ms_per_step": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"},
                 "roofline": {"kernel": "k_force (adjoint force/virial)", "bound": "fp32",
                              "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                             "frac": achieved / fp32_peak if fp32_peak > 0 else None, "traffic": None,
+                             "frac": achieved / fp32_peak if fp32_peak > 0 else None,
+                             "traffic": K_FORCE_DRAM_BYTES_PER_ATOM * N,
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_force on the "
+                                               "524,288-atom case, scaled per atom",
+                             "algorithmic_bytes": k_force_algorithmic_bytes(
+                                 info["basics"], edges_within(box, pos, pot.rc + SKIN) / N) * N,
                              "peak_source": "measured FP32 FMA-chain microbenchmark on this GPU (burst)",
                              "flops_per_edge": ff, "edges_per_launch": edges,
                              "launch_ms": force_ms_launch,

@@ -767,7 +767,8 @@ struct Engine {
       std::memcpy(last_h, h, sizeof(last_h));
       for (int k = 0; k < 3; ++k) last_pbc[k] = pbc[k] ? 1 : 0;
       if (ncells + 1 > cells_alloc) {
-        cell_count.resize(ncells + 1);
+        // counts plus one scan block sum per 1024 cells
+        cell_count.resize(ncells + 1 + (ncells + 1023) / 1024);
         cell_start.resize(ncells + 1);
         cells_alloc = ncells + 1;
       }
@@ -789,7 +790,7 @@ struct Engine {
       ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
       launch_build(s, N, 1, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p, cell_start.p,
                    cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nullptr, ncount.p, 0, 1, d_status.p);
-      launches += 6;
+      launches += 8;
       Status st{};
       ck(cudaMemcpyAsync(&st, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
       ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
@@ -799,7 +800,7 @@ struct Engine {
     launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
                  cell_start.p, cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
                  d_status.p);
-    launches += 6;
+    launches += 8;
     ck(cudaGetLastError(), "neighbour build launch");
     have_ref = true;
     force_next = false;

@@ -20,8 +20,9 @@ __device__ __forceinline__ int type_of(const double4& p) {
 // ---------------------------------------------------------------------------
 template <typename T>
 struct Edge {
-  T r, rinv, ux, uy, uz, dr;  // dr = r - rc (computed from r^2 - rc^2 in FP64)
+  T r, rinv, ux, uy, uz, dr;  // dr = r - rc (formed in FP64)
   T dx, dy, dz;
+  double rd;                  // r in FP64: the radial argument scal (r - shift) / 2 is formed from it
 };
 
 template <typename T>
@@ -34,15 +35,20 @@ __device__ __forceinline__ Edge<float> make_edge<float>(double dx, double dy, do
   Edge<float> e;
   const float r2f = static_cast<float>(r2);
   e.rinv = rsqrtf(r2f);
-  e.r = r2f * e.rinv;
+  const float r32 = r2f * e.rinv;
+  // one Newton step on the FP64 r^2 gives r to FP64 accuracy: the radial
+  // argument and (r - rc) near the cutoff are formed from it in FP64
+  e.rd = fma(r2 - static_cast<double>(r32) * static_cast<double>(r32), 0.5 * static_cast<double>(e.rinv),
+             static_cast<double>(r32));
+  e.r = static_cast<float>(e.rd);
   e.dx = static_cast<float>(dx);
   e.dy = static_cast<float>(dy);
   e.dz = static_cast<float>(dz);
   e.ux = e.dx * e.rinv;
   e.uy = e.dy * e.rinv;
   e.uz = e.dz * e.rinv;
-  // (r - rc) without FP32 cancellation near the cutoff
-  e.dr = __fdividef(static_cast<float>(r2 - rc2), e.r + static_cast<float>(rc));
+  e.dr = static_cast<float>(e.rd - rc);
+  (void)rc2;
   return e;
 }
 
@@ -51,6 +57,7 @@ __device__ __forceinline__ Edge<double> make_edge<double>(double dx, double dy, 
                                                           double rc, double rc2) {
   Edge<double> e;
   e.r = sqrt(r2);
+  e.rd = e.r;
   e.rinv = 1.0 / e.r;
   e.dx = dx;
   e.dy = dy;
@@ -71,7 +78,7 @@ __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __r
   const bool rational = a.rs.rational != 0;
   if (a.rs.shared_xi) {
     T xi, dxi;
-    radial_map<T>(T(0.5) * row[0] * (e.r - row[1]), rational, xi, dxi);
+    radial_map<T>(T(0.5) * row[0] * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
     T t[RB];
     chebyshev<RB>(xi, t);
 #pragma unroll
@@ -85,7 +92,8 @@ __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __r
 #pragma unroll
     for (int mu = 0; mu < KMU; ++mu) {
       T xi, dxi;
-      radial_map<T>(T(0.5) * row[2 * mu] * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+      radial_map<T>(T(0.5) * row[2 * mu] * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational,
+                    xi, dxi);
       T t[RB];
       chebyshev<RB>(xi, t);
       T s = T(0);
@@ -106,7 +114,7 @@ __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T
   if (a.rs.shared_xi) {
     const T half_scal = T(0.5) * row[0];
     T xi, dxi;
-    radial_map<T>(half_scal * (e.r - row[1]), rational, xi, dxi);
+    radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
     const T g = f * half_scal * dxi;  // f * d xi / dr
     T t[RB], dt[RB];
     chebyshev_d<RB>(xi, t, dt);
@@ -126,7 +134,7 @@ __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T
     for (int mu = 0; mu < KMU; ++mu) {
       const T half_scal = T(0.5) * row[2 * mu];
       T xi, dxi;
-      radial_map<T>(half_scal * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+      radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi, dxi);
       T t[RB], dt[RB];
       chebyshev_d<RB>(xi, t, dt);
       T s = T(0), sd = T(0);

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
     if (a.rs.shared_xi) {
       const T half_scal = T(0.5) * row[0];
       T xi, dxi;
-      radial_map<T>(half_scal * (e.r - row[1]), rational, xi, dxi);
+      radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
       fac = half_scal * dxi;
       chebyshev<RB>(xi, t);
     }
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
         if (!a.rs.shared_xi) {
           const T half_scal = T(0.5) * row[2 * mu];
           T xi, dxi;
-          radial_map<T>(half_scal * (e.r - row[2 * mu + 1]), rational, xi, dxi);
+          radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi, dxi);
           scale = half_scal * dxi;
           chebyshev<RB>(xi, t);
         }

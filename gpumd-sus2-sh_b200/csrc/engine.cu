@@ -3,7 +3,7 @@
 // Kernel map (reference stage in brackets, src/force/sus2_sh.cu):
 //   k_pack        positions -> unwrapped double4 + species, displacement max
 //   k_decide      rebuild flag (skin/2 displacement rule or host-forced)
-//   k_bin/k_scan/k_scatter/k_sort_cells/k_fill
+//   k_bin/k_scan_*/k_scatter/k_sort_cells/k_fill
 //                 cell-list Verlet list with explicit image codes
 //                 [build_neighbor_list :9547-9618, image kernels :7668-7769]
 //   k_basic       B[k,l,m] = sum_j R_kl(r_ij) Y_lm(r_ij)      [gpu_sh_compute_basic :3486-3550]
@@ -114,30 +114,72 @@ __global__ void k_bin(int N, const Status* __restrict__ st, const BoxGeom* __res
   atom_rank[i] = atomicAdd(&cell_count[cell], 1);
 }
 
-// Exclusive scan of cell counts, one block.
-__global__ void k_scan(const Status* __restrict__ st, const int* __restrict__ cnt,
-                       int* __restrict__ start, int ncells) {
-  if (!st->rebuilt) return;
-  __shared__ int part[1024];
-  const int t = threadIdx.x, nt = blockDim.x;
-  const int chunk = (ncells + nt - 1) / nt;
-  const int b0 = t * chunk, b1 = min(ncells, b0 + chunk);
-  int sum = 0;
-  for (int c = b0; c < b1; ++c) sum += cnt[c];
-  part[t] = sum;
+// Exclusive scan of the cell counts in three passes: per-block sums of 1024
+// cells, a scan of the block sums (one block, looping when there are more
+// than 1024 of them), and the per-block scans with their offsets.
+constexpr int kScanTile = 1024;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
   __syncthreads();
-  for (int o = 1; o < nt; o <<= 1) {
-    int v = t >= o ? part[t - o] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
+  if (warp == 0) {
+    int w = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    warp_sums[lane] = w;  // inclusive prefix of the warp sums
   }
-  int run = part[t] - sum;
-  for (int c = b0; c < b1; ++c) {
-    start[c] = run;
-    run += cnt[c];
+  __syncthreads();
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  const int before = warp > 0 ? warp_sums[warp - 1] : 0;
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanTile) k_scan_sums(const Status* __restrict__ st, const int* __restrict__ cnt,
+                                                         int ncells, int* __restrict__ block_sums) {
+  if (!st->rebuilt) return;
+  __shared__ int warp_sums[32];
+  const int c = blockIdx.x * kScanTile + threadIdx.x;
+  int total;
+  block_exclusive_scan(c < ncells ? cnt[c] : 0, warp_sums, total);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanTile) k_scan_top(const Status* __restrict__ st, int nblocks,
+                                                        int* __restrict__ block_sums) {
+  if (!st->rebuilt) return;
+  __shared__ int warp_sums[32];
+  int carry = 0;
+  for (int b0 = 0; b0 < nblocks; b0 += kScanTile) {
+    const int b = b0 + threadIdx.x;
+    const int v = b < nblocks ? block_sums[b] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, warp_sums, total);
+    if (b < nblocks) block_sums[b] = carry + ex;
+    carry += total;
   }
-  if (t == nt - 1) start[ncells] = part[t];
+}
+
+__global__ void __launch_bounds__(kScanTile) k_scan_apply(const Status* __restrict__ st, const int* __restrict__ cnt,
+                                                          int ncells, const int* __restrict__ block_sums,
+                                                          int* __restrict__ start) {
+  if (!st->rebuilt) return;
+  __shared__ int warp_sums[32];
+  const int c = blockIdx.x * kScanTile + threadIdx.x;
+  const int v = c < ncells ? cnt[c] : 0;
+  int total;
+  const int ex = block_exclusive_scan(v, warp_sums, total);
+  const int s0 = block_sums[blockIdx.x] + ex;
+  if (c < ncells) start[c] = s0;
+  if (c == ncells - 1) start[ncells] = s0 + v;
 }
 
 __global__ void k_scatter(int N, const Status* __restrict__ st, const int* __restrict__ start,
@@ -532,7 +574,12 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
   k_decide<<<1, 1, 0, s>>>(st, force, half_skin2);
   cudaMemsetAsync(cell_count, 0, sizeof(int) * (ncells + 1), s);
   k_bin<<<blocks_for(N, 256), 256, 0, s>>>(N, st, geom_dev, pos4, ref4, cell_count, atom_cell, atom_rank);
-  k_scan<<<1, 1024, 0, s>>>(st, cell_count, cell_start, ncells);
+  // block sums live in the spare tail of cell_count (sized by the caller)
+  const int nblocks = blocks_for(ncells, kScanTile);
+  int* block_sums = cell_count + ncells + 1;
+  k_scan_sums<<<nblocks, kScanTile, 0, s>>>(st, cell_count, ncells, block_sums);
+  k_scan_top<<<1, kScanTile, 0, s>>>(st, nblocks, block_sums);
+  k_scan_apply<<<nblocks, kScanTile, 0, s>>>(st, cell_count, ncells, block_sums, cell_start);
   k_scatter<<<blocks_for(N, 256), 256, 0, s>>>(N, st, cell_start, atom_cell, atom_rank, cell_atoms);
   k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, cell_start, cell_atoms);
   k_fill<<<blocks_for(N, 128), 128, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms,

@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(128)
           const int pr = a.rs.shared_xi ? 0 : mu;
           const T half_scal = T(0.5) * row[2 * pr];
           T xi, dxi;
-          radial_map<T>(half_scal * (e.r - row[2 * pr + 1]), rational, xi, dxi);
+          radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * pr + 1])), rational, xi, dxi);
           T t[RB], dt[RB];
           chebyshev_d<RB>(xi, t, dt);
           const T p1 = ps * fc * (A - Cm);
