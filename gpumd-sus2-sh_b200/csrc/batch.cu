@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(128)
   const double* h = cell_h + 9 * c;
   const int rx = cell_reach[3 * c], ry = cell_reach[3 * c + 1], rz = cell_reach[3 * c + 2];
   const bool ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
+  if (ortho) return;  // orthorhombic cells: k_batch_fill_ortho
   const double cut = sqrt(cutoff2);
   const double4 pi = pos4[i];
   int k = 0;
@@ -142,6 +143,121 @@ __global__ void __launch_bounds__(128)
   ncount[i] = k;
   atomicMax(&st->max_count, k);
   if (k > cap && !count_only) st->overflow = 1;
+}
+
+// Orthorhombic cells, one CTA per cell: the cell's positions are staged in
+// shared memory (FP32, relative to its first atom) and every thread tests its
+// atom against them; per axis only the images that can come within the
+// cutoff are visited (computed from the displacement, at most `reach` each
+// way).  An FP32 pre-test with a 1e-3 A margin admits a superset of the pairs;
+// each admitted pair gets the exact FP64 test of k_batch_fill, so the lists
+// (and their order: j ascending, then tz, ty, tx ascending) are the same.
+constexpr int kFillTile = 256;
+
+__global__ void __launch_bounds__(128)
+    k_batch_fill_ortho(int N, const int* __restrict__ off, const double4* __restrict__ pos4,
+                       const double* __restrict__ cell_h, const int* __restrict__ cell_reach, double cutoff2,
+                       int* __restrict__ nbr, int* __restrict__ ncount, int cap, int count_only, Status* st) {
+  __shared__ float4 sp[kFillTile];
+  const int c = blockIdx.x;
+  const double* h = cell_h + 9 * c;
+  const bool ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
+  const int a0 = off[c], a1 = off[c + 1];
+  if (!ortho || a1 <= a0) return;  // uniform across the block
+  const double4 o = pos4[a0];
+  const float L[3] = {static_cast<float>(h[0]), static_cast<float>(h[4]), static_cast<float>(h[8])};
+  const float iL[3] = {1.0f / L[0], 1.0f / L[1], 1.0f / L[2]};
+  const int r[3] = {cell_reach[3 * c], cell_reach[3 * c + 1], cell_reach[3 * c + 2]};
+  const float cutm = static_cast<float>(sqrt(cutoff2)) + 1.0e-3f;
+  const float cutm2 = cutm * cutm;
+  for (int base = a0; base < a1; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const bool act = i < a1;
+    double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    if (act) {
+      pi = pos4[i];
+      fx = static_cast<float>(pi.x - o.x);
+      fy = static_cast<float>(pi.y - o.y);
+      fz = static_cast<float>(pi.z - o.z);
+    }
+    int k = 0;
+    for (int t0 = a0; t0 < a1; t0 += kFillTile) {
+      const int tn = min(kFillTile, a1 - t0);
+      __syncthreads();  // the previous tile is consumed
+      for (int q = threadIdx.x; q < tn; q += blockDim.x) {
+        const double4 p = pos4[t0 + q];
+        sp[q] = make_float4(static_cast<float>(p.x - o.x), static_cast<float>(p.y - o.y),
+                            static_cast<float>(p.z - o.z), 0.0f);
+      }
+      __syncthreads();
+      if (!act) continue;
+      // candidates in groups of 8: the nearest-image distances of a group are
+      // independent (instruction-level parallelism); most of a large cell's
+      // candidates are farther than the cutoff in every image and stop there
+      for (int q0 = 0; q0 < tn; q0 += 8) {
+        unsigned near = 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const float4 pj = sp[min(q0 + u, tn - 1)];
+          float m2 = 0.0f;
+          const float d[3] = {pj.x - fx, pj.y - fy, pj.z - fz};
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const float t = r[a] > 0 ? rintf(d[a] * iL[a]) : 0.0f;
+            const float e = d[a] - t * L[a];
+            m2 = fmaf(e, e, m2);
+          }
+          if (q0 + u < tn && m2 < cutm2) near |= 1u << u;
+        }
+        while (near) {
+          const int u = __ffs(near) - 1;
+          near &= near - 1;
+          const int q = q0 + u;
+          const int j = t0 + q;
+          const float4 pj = sp[q];
+          const float d0[3] = {pj.x - fx, pj.y - fy, pj.z - fz};
+          int lo[3], hi[3];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            lo[a] = max(-r[a], static_cast<int>(ceilf((-cutm - d0[a]) * iL[a])));
+            hi[a] = min(r[a], static_cast<int>(floorf((cutm - d0[a]) * iL[a])));
+          }
+          for (int tz = lo[2]; tz <= hi[2]; ++tz) {
+            const float ez = d0[2] + tz * L[2];
+            const float ez2 = ez * ez;
+            if (ez2 >= cutm2) continue;
+            for (int ty = lo[1]; ty <= hi[1]; ++ty) {
+              const float ey = d0[1] + ty * L[1];
+              const float eyz2 = ey * ey + ez2;
+              if (eyz2 >= cutm2) continue;
+              for (int tx = lo[0]; tx <= hi[0]; ++tx) {
+                const float ex = d0[0] + tx * L[0];
+                if (ex * ex + eyz2 >= cutm2) continue;
+                if (j == i && tx == 0 && ty == 0 && tz == 0) continue;
+                const double4 pjd = pos4[j];
+                const double dx = (pjd.x - pi.x) + tx * h[0] + ty * h[1] + tz * h[2];
+                const double dy = (pjd.y - pi.y) + tx * h[3] + ty * h[4] + tz * h[5];
+                const double dz = (pjd.z - pi.z) + tx * h[6] + ty * h[7] + tz * h[8];
+                if (dx * dx + dy * dy + dz * dz < cutoff2) {
+                  if (!count_only && k < cap) {
+                    const int code = (tx + 2) * 25 + (ty + 2) * 5 + (tz + 2);
+                    nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
+                  }
+                  ++k;
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    if (act) {
+      ncount[i] = k;
+      atomicMax(&st->max_count, k);
+      if (k > cap && !count_only) st->overflow = 1;
+    }
+  }
 }
 
 // One block per cell: sum of site energies and of per-atom virials.
@@ -192,9 +308,11 @@ void launch_batch_pack(cudaStream_t s, int N, int ncells, const int* off, const 
                                               atom_cell, pos4, st);
 }
 
-void launch_batch_fill(cudaStream_t s, int N, const int* off, const int* atom_cell, const double4* pos4,
+void launch_batch_fill(cudaStream_t s, int N, int ncells, const int* off, const int* atom_cell, const double4* pos4,
                        const double* cell_h, const int* cell_reach, double cutoff2, int* nbr, int* ncount, int cap,
                        int count_only, Status* st) {
+  k_batch_fill_ortho<<<ncells, 128, 0, s>>>(N, off, pos4, cell_h, cell_reach, cutoff2, nbr, ncount, cap, count_only,
+                                            st);
   k_batch_fill<<<blocks(N, 128), 128, 0, s>>>(N, off, atom_cell, pos4, cell_h, cell_reach, cutoff2, nbr, ncount,
                                               cap, count_only, st);
 }

@@ -738,18 +738,18 @@ struct Engine {
     const double cutoff2 = list_cutoff * list_cutoff;
     if (cap == 0) {
       ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
-      launch_batch_fill(s, N, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nullptr, ncount.p, 0, 1,
-                        d_status.p);
+      launch_batch_fill(s, N, ncells, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nullptr,
+                        ncount.p, 0, 1, d_status.p);
       Status st{};
       ck(cudaMemcpyAsync(&st, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
       ck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
       if (st.thin_cell) throw InputError("sus2sh batch: a periodic cell is thinner than half the cutoff.");
       grow_capacity(st.max_count);
-      launches += 1;
+      launches += 2;
     }
-    launch_batch_fill(s, N, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nbr.p, ncount.p, cap, 0,
-                      d_status.p);
-    launches += 1;
+    launch_batch_fill(s, N, ncells, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nbr.p, ncount.p,
+                      cap, 0, d_status.p);
+    launches += 2;
     ck(cudaGetLastError(), "batch neighbour build launch");
   }
 

@@ -143,7 +143,7 @@ void launch_batch_geometry(cudaStream_t s, int ncells, const double* cell_h, con
 void launch_batch_pack(cudaStream_t s, int N, int ncells, const int* off, const double* x, const int* type,
                        const double* cell_h, const double* cell_hinv, const int* cell_pbc, int species,
                        int* atom_cell, double4* pos4, Status* st);
-void launch_batch_fill(cudaStream_t s, int N, const int* off, const int* atom_cell, const double4* pos4,
+void launch_batch_fill(cudaStream_t s, int N, int ncells, const int* off, const int* atom_cell, const double4* pos4,
                        const double* cell_h, const int* cell_reach, double cutoff2, int* nbr, int* ncount,
                        int cap, int count_only, Status* st);
 void launch_cell_reduce(cudaStream_t s, int ncells, int N, const int* off, const double* pe, const double* virial,

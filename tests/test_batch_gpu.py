@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 import sus2sh_oracle as O  # noqa: E402
-from sus2sh import SUS2_SH, structures  # noqa: E402
+from sus2sh import SUS2_SH, Box, structures  # noqa: E402
 
 
 @pytest.fixture(scope="module")
@@ -52,6 +52,36 @@ def test_batch_matches_oracle_cell_by_cell(l3k3_path, batch, fp64):
         assert np.sqrt(((w[:, a:b] - w0) ** 2).mean()) < frms_tol
         assert abs(ce[c] - pe0.sum()) < etol * (b - a)
         assert np.abs(cw[c] - w0.sum(axis=1)).max() < frms_tol * (b - a)
+    pot.close()
+
+
+def test_batch_mixed_triclinic_cells(l3k3_path):
+    # every other cell sheared (xy and xz tilts): triclinic cells take the
+    # general per-atom image scan, orthorhombic ones the shared-memory scan
+    off, H, boxes, types, pos = structures.cell_batch(8, 40, 300, seed=77)
+    H = H.copy()
+    pos = pos.copy()
+    tboxes = []
+    for c, box in enumerate(boxes):
+        a, b = off[c], off[c + 1]
+        h = box.cpu_h.reshape(3, 3).copy()
+        if c % 2:
+            frac = np.linalg.solve(h, pos[:, a:b])
+            h[0, 1] = 0.12 * h[1, 1]
+            h[0, 2] = -0.08 * h[2, 2]
+            pos[:, a:b] = h @ frac
+        H[c] = h.reshape(-1)
+        tboxes.append(Box(h.reshape(-1), box.pbc))
+    dev = torch.device("cuda")
+    pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr"])
+    pe, f, w, ce, cw = _run(pot, off, H, types, pos, dev)
+    orc = O.Oracle(l3k3_path)
+    for c, box in enumerate(tboxes):
+        a, b = off[c], off[c + 1]
+        pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types[a:b], pos[:, a:b])
+        assert np.abs(pe[a:b] - pe0).max() < 1e-6, c
+        assert np.sqrt(((f[:, a:b] - f0) ** 2).mean()) < 1e-5, c
+        assert np.sqrt(((w[:, a:b] - w0) ** 2).mean()) < 1e-5, c
     pot.close()
 
 
