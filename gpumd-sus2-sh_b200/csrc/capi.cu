@@ -391,6 +391,11 @@ struct Engine {
   CgSource cg_src;
   CgBinary cg_bin;
   CgModule cg_mod;
+  // forward-over-reverse product kernel of the parameter gradients (first use)
+  bool pg_tried = false;
+  CgSource pg_src;
+  CgBinary pg_bin;
+  CgModule pg_mod;
   double cg_compile_ms = 0.0;
 
   ~Engine() {
@@ -982,27 +987,60 @@ struct Engine {
   template <typename T>
   void param_grad_impl(cudaStream_t s, const double* ew, const double* fw, double* grad_w, double* grad_c) {
     if (gate) throw InputError("SUS2_SH parameter gradients do not cover two-layer gate models.");
+    if (!pg_tried) {
+      // model-specialised forward-over-reverse product kernel, built at the
+      // first gradient call for graphs of the straight-line size
+      pg_tried = true;
+      long long terms = 0;
+      for (const Row& r : lay.rows) terms += static_cast<long long>(r.left.size());
+      if (opt.cg_jit && terms <= kCgSingleMaxProducts) {
+        pg_src = generate_pg_source(model, lay, use_float, prog.basic_canon, prog.ncanon);
+        pg_bin = compile_cg_source(pg_src);
+      }
+    }
+    const bool generated = !pg_bin.cubin.empty();
     const size_t nb = static_cast<size_t>(prog.ncanon) * N;
-    const size_t work = 4ull * model.moments * N;
-    pg_buf.resize((4 * nb + work) * sizeof(T));
+    // generated kernel: per-atom scalar terms [scalar][N] and 64 partial sums
+    // (doubles) per scalar; interpreter: its [4 M][N] scratch
+    const size_t ns = static_cast<size_t>(std::max(model.scalar_count, 1));
+    // the partial sums start on a 256-byte boundary (FP64 loads and stores)
+    const size_t partial_at = ((4 * nb + ns * N) * sizeof(T) + 255) / 256 * 256 / sizeof(T);
+    const size_t total = generated ? partial_at + (ns * 64 * sizeof(double)) / sizeof(T)
+                                   : 4 * nb + 4ull * model.moments * N;
+    pg_buf.resize(total * sizeof(T));
     T* base = reinterpret_cast<T*>(pg_buf.p);
-    FlatProgram fp{};
-    fp.nprod = static_cast<int>(model.products.size());
-    fp.nbasic = prog.nbasic;
-    fp.ncanon = prog.ncanon;
-    fp.nscalar = model.scalar_count;
-    fp.left = d_fl.p;
-    fp.right = d_fr.p;
-    fp.target = d_ft.p;
-    fp.coeff = d_fc.p;
-    fp.basic_canon = d_basic_canon.p;
-    fp.scalar_map = d_smap.p;
-    fp.scalar_w = d_sw.p;
-    if (launch_param_grad<T>(s, edge_args<T>(), fp, model.moments, d_species.p, ew, fw, base, base + nb,
-                             base + 4 * nb, base + 2 * nb, base + 3 * nb, grad_w, grad_c) != 0)
+    T *B = base, *Bd = base + nb, *Galpha = base + 2 * nb, *Gbeta = base + 3 * nb, *X = base + 4 * nb;
+    const EdgeArgs<T> a = edge_args<T>();
+    if (launch_pg_basic<T>(s, a, fw, B, Bd, grad_c) != 0)
       throw InputError("SUS2_SH parameter gradients are built ahead of time for the common shapes only; "
                        "this model shape (sh_l_max, sh_k_max, radial_basis_size) has none.");
-    launches += 3;
+    if (generated) {
+      std::string err;
+      int n = N;
+      const void* p4 = pos4.p;
+      const void* sp = d_species.p;
+      void* args[] = {&n, &p4, &B, &Bd, &sp, &ew, &Galpha, &Gbeta, &X};
+      if (!pg_mod.load(pg_bin, pg_src.kernel_name, &err) ||
+          !pg_mod.launch_args(s, static_cast<unsigned>((N + 127) / 128), 128, 0, args, &err))
+        throw CudaError(err);
+      launch_pg_reduce<T>(s, model.scalar_count, N, X, reinterpret_cast<double*>(base + partial_at), grad_w);
+    } else {
+      FlatProgram fp{};
+      fp.nprod = static_cast<int>(model.products.size());
+      fp.nbasic = prog.nbasic;
+      fp.ncanon = prog.ncanon;
+      fp.nscalar = model.scalar_count;
+      fp.left = d_fl.p;
+      fp.right = d_fr.p;
+      fp.target = d_ft.p;
+      fp.coeff = d_fc.p;
+      fp.basic_canon = d_basic_canon.p;
+      fp.scalar_map = d_smap.p;
+      fp.scalar_w = d_sw.p;
+      launch_pg_product<T>(s, N, fp, model.moments, pos4.p, d_species.p, ew, B, Bd, X, Galpha, Gbeta, grad_w);
+    }
+    launch_pg_radial<T>(s, a, fw, Galpha, Gbeta, grad_c);
+    launches += generated ? 5 : 3;
   }
 
   void finish(cudaStream_t s) {
@@ -1412,8 +1450,12 @@ int sus2sh_cg_kernel_info(const char* path, int use_float, int split, int* info,
     const auto t0 = std::chrono::steady_clock::now();
     sus2sh::CgSource src;
     std::string why;
-    if (!sus2sh::choose_cg_source(m, lay, prog.basic_canon, prog.ncanon, use_float != 0, split, &src, &why))
+    if (split == 2) {
+      src = sus2sh::generate_pg_source(m, lay, use_float != 0, prog.basic_canon, prog.ncanon);
+    } else if (!sus2sh::choose_cg_source(m, lay, prog.basic_canon, prog.ncanon, use_float != 0, split, &src,
+                                         &why)) {
       throw InputError("no CG kernel for this graph (" + why + "); the row interpreter runs it");
+    }
     const sus2sh::CgBinary bin = sus2sh::compile_cg_source(src);
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     int spill = 0;

@@ -210,6 +210,196 @@ CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_flo
   return out;
 }
 
+// Forward-over-reverse CG product for the parameter gradients: every moment
+// carries its value v and tangent w (the derivative along the position
+// perturbation of the force-matching term), every adjoint its value a and
+// tangent b.  Same row schedule as generate_cg_source; every scalar is kept
+// (a weight of zero still has a gradient).  Per atom the kernel writes
+// contrib[s] = c_t (ew M_s - dM_s) for the reduction of dL/dw_s, and the
+// basic adjoints alpha = c_t (ew a - b), beta = c_t a for the radial pass.
+CgSource generate_pg_source(const HostModel& m, const Layered& lay, bool use_float,
+                            const std::vector<int>& basic_canon, int ncanon) {
+  const int M = m.moments, Bb = m.basic_count;
+  const char* T = use_float ? "float" : "double";
+  const char* FMA = use_float ? "fmaf" : "fma";
+  const std::string zero = use_float ? "0.0f" : "0.0";
+  std::vector<int> row_of(M, -1);
+  for (size_t r = 0; r < lay.rows.size(); ++r) row_of[lay.rows[r].target] = static_cast<int>(r);
+  std::vector<double> weight(M, 0.0);
+  std::vector<char> is_scalar(M, 0);
+  std::vector<std::vector<int>> scalars_of(M);
+  for (int s = 0; s < m.scalar_count; ++s) {
+    weight[m.moment_mapping[s]] += m.moment_coeffs[s];
+    is_scalar[m.moment_mapping[s]] = 1;
+    scalars_of[m.moment_mapping[s]].push_back(s);
+  }
+  std::vector<char> live(M, 0);
+  for (int r = static_cast<int>(lay.rows.size()) - 1; r >= 0; --r) {
+    const Row& row = lay.rows[r];
+    if (is_scalar[row.target]) live[row.target] = 1;
+    if (!live[row.target]) continue;
+    for (size_t t = 0; t < row.left.size(); ++t) live[row.left[t]] = live[row.right[t]] = 1;
+  }
+  std::vector<std::vector<int>> consumers(M);
+  for (const Row& row : lay.rows) {
+    if (!live[row.target]) continue;
+    std::set<int> ops(row.left.begin(), row.left.end());
+    ops.insert(row.right.begin(), row.right.end());
+    for (int o : ops) consumers[o].push_back(row.target);
+  }
+  std::vector<int> pending(M, 0);
+  for (int x = 0; x < M; ++x) pending[x] = static_cast<int>(consumers[x].size());
+  std::vector<char> terminal(M, 0);
+  for (const Row& row : lay.rows)
+    if (live[row.target] && consumers[row.target].empty()) terminal[row.target] = 1;
+
+  std::ostringstream body;
+  long long terms = 0;
+  std::vector<char> emitted(M, 0);
+  for (int b = 0; b < Bb; ++b) emitted[b] = 1;
+  auto v = [](int x) { return "v" + std::to_string(x); };
+  auto w = [](int x) { return "w" + std::to_string(x); };
+  auto a = [](int x) { return "a" + std::to_string(x); };
+  auto bt = [](int x) { return "b" + std::to_string(x); };
+  auto contrib = [&](std::ostringstream& o, int x, const std::string& val, const std::string& tan) {
+    for (int s : scalars_of[x])
+      o << "  contrib[" << s << " * n + i] = (" << T << ")(ct * (ak * (double)" << val << " - (double)" << tan
+        << "));\n";
+  };
+
+  std::function<void(int)> ensure = [&](int x) {
+    if (emitted[x]) return;
+    const Row& row = lay.rows[row_of[x]];
+    for (size_t t = 0; t < row.left.size(); ++t) {
+      ensure(row.left[t]);
+      ensure(row.right[t]);
+    }
+    body << "  " << T << " " << v(x) << " = " << zero << ", " << w(x) << " = " << zero << ";\n";
+    for (size_t t = 0; t < row.left.size(); ++t) {
+      const int l = row.left[t], r = row.right[t];
+      const std::string c = lit(row.coeff[t], use_float);
+      body << "  { const " << T << " cl = " << c << " * " << v(l) << ";\n"
+           << "    " << v(x) << " = " << FMA << "(cl, " << v(r) << ", " << v(x) << ");\n"
+           << "    " << w(x) << " = " << FMA << "(cl, " << w(r) << ", " << FMA << "(" << c << " * " << w(l) << ", "
+           << v(r) << ", " << w(x) << ")); }\n";
+    }
+    terms += 3 * static_cast<long long>(row.left.size());
+    body << "  " << T << " " << a(x) << " = " << (weight[x] != 0.0 ? lit(weight[x], use_float) : zero) << ", "
+         << bt(x) << " = " << zero << ";\n";
+    contrib(body, x, v(x), w(x));
+    emitted[x] = 1;
+  };
+
+  std::function<void(int)> back = [&](int x) {
+    const Row& row = lay.rows[row_of[x]];
+    for (size_t t = 0; t < row.left.size(); ++t) {
+      const int l = row.left[t], r = row.right[t];
+      const std::string c = lit(row.coeff[t], use_float);
+      body << "  { const " << T << " q = " << c << " * " << a(x) << ", qd = " << c << " * " << bt(x) << ";\n"
+           << "    " << bt(l) << " = " << FMA << "(qd, " << v(r) << ", " << FMA << "(q, " << w(r) << ", " << bt(l)
+           << "));\n"
+           << "    " << bt(r) << " = " << FMA << "(qd, " << v(l) << ", " << FMA << "(q, " << w(l) << ", " << bt(r)
+           << "));\n"
+           << "    " << a(l) << " = " << FMA << "(q, " << v(r) << ", " << a(l) << ");\n"
+           << "    " << a(r) << " = " << FMA << "(q, " << v(l) << ", " << a(r) << "); }\n";
+    }
+    terms += 6 * static_cast<long long>(row.left.size());
+    std::set<int> ops(row.left.begin(), row.left.end());
+    ops.insert(row.right.begin(), row.right.end());
+    for (int o : ops) {
+      if (o < Bb) continue;
+      if (--pending[o] == 0) back(o);
+    }
+  };
+
+  std::vector<int> term_rows;
+  std::vector<int> order(M, 0);
+  for (size_t r = 0; r < lay.rows.size(); ++r) order[lay.rows[r].target] = static_cast<int>(r) + 1;
+  for (const Row& row : lay.rows)
+    if (terminal[row.target]) term_rows.push_back(row.target);
+  auto key = [&](int t) {
+    const Row& row = lay.rows[row_of[t]];
+    int k = 0;
+    for (size_t i = 0; i < row.left.size(); ++i) k = std::max({k, order[row.left[i]], order[row.right[i]]});
+    return k;
+  };
+  std::stable_sort(term_rows.begin(), term_rows.end(), [&](int x, int y) { return key(x) < key(y); });
+  for (int t : term_rows) {
+    const Row& row = lay.rows[row_of[t]];
+    for (size_t i = 0; i < row.left.size(); ++i) {
+      ensure(row.left[i]);
+      ensure(row.right[i]);
+    }
+    const double wt = weight[t];
+    body << "  {\n    " << T << " t = " << zero << ", td = " << zero << ";\n";
+    for (size_t i = 0; i < row.left.size(); ++i) {
+      const int l = row.left[i], r = row.right[i];
+      const std::string c = lit(row.coeff[i], use_float);
+      body << "    { const " << T << " cl = " << c << " * " << v(l) << ";\n"
+           << "      t = " << FMA << "(cl, " << v(r) << ", t);\n"
+           << "      td = " << FMA << "(cl, " << w(r) << ", " << FMA << "(" << c << " * " << w(l) << ", " << v(r)
+           << ", td)); }\n";
+      if (wt != 0.0) {
+        const std::string p = lit(row.coeff[i] * wt, use_float);
+        body << "    " << a(l) << " = " << FMA << "(" << p << ", " << v(r) << ", " << a(l) << ");\n"
+             << "    " << a(r) << " = " << FMA << "(" << p << ", " << v(l) << ", " << a(r) << ");\n"
+             << "    " << bt(l) << " = " << FMA << "(" << p << ", " << w(r) << ", " << bt(l) << ");\n"
+             << "    " << bt(r) << " = " << FMA << "(" << p << ", " << w(l) << ", " << bt(r) << ");\n";
+      }
+    }
+    std::ostringstream cb;
+    contrib(cb, t, "t", "td");
+    body << cb.str() << "  }\n";
+    terms += static_cast<long long>(row.left.size()) * (wt != 0.0 ? 7 : 3);
+    std::set<int> ops(row.left.begin(), row.left.end());
+    ops.insert(row.right.begin(), row.right.end());
+    for (int o : ops) {
+      if (o < Bb) continue;
+      if (--pending[o] == 0) back(o);
+    }
+  }
+
+  std::ostringstream src;
+  const std::string tag = std::to_string(fnv1a(body.str()) ^ (use_float ? 0x9e37ull : 0x79b9ull));
+  CgSource out;
+  out.kernel_name = "sus2sh_pg_" + tag;
+  src << "// generated SUS2-SH forward-over-reverse CG product kernel (" << (use_float ? "FP32" : "FP64") << ")\n"
+      << "struct D4 { double x, y, z, w; };\n"
+      << "extern \"C\" __global__ void __launch_bounds__(128) " << out.kernel_name
+      << "(int N, const D4* __restrict__ pos4, const " << T << "* __restrict__ B, const " << T
+      << "* __restrict__ Bd, const double* __restrict__ species, const double* __restrict__ ew, " << T
+      << "* __restrict__ Galpha, " << T << "* __restrict__ Gbeta, " << T << "* __restrict__ contrib) {\n"
+      << "  const int i = blockIdx.x * blockDim.x + threadIdx.x;\n"
+      << "  if (i >= N) return;\n"
+      << "  const size_t n = (size_t)N;\n"
+      << "  const double ct = species[(int)__double_as_longlong(pos4[i].w)];\n"
+      << "  const double ak = ew ? ew[i] : 0.0;\n";
+  for (int b = 0; b < Bb; ++b) {
+    src << "  const " << T << " " << v(b) << " = __ldg(B + " << basic_canon[b] << " * n + i), " << w(b)
+        << " = __ldg(Bd + " << basic_canon[b] << " * n + i);\n";
+    src << "  " << T << " " << a(b) << " = " << (weight[b] != 0.0 ? lit(weight[b], use_float) : zero) << ", "
+        << bt(b) << " = " << zero << ";\n";
+    contrib(src, b, v(b), w(b));
+  }
+  src << body.str();
+  src << "  const " << T << " sc = (" << T << ")ct, sa = (" << T << ")(ct * ak);\n";
+  std::vector<int> canon_basic(ncanon, -1);
+  for (int b = 0; b < Bb; ++b) canon_basic[basic_canon[b]] = b;
+  for (int c = 0; c < ncanon; ++c) {
+    if (canon_basic[c] >= 0) {
+      const int b = canon_basic[c];
+      src << "  Galpha[" << c << " * n + i] = " << FMA << "(sa, " << a(b) << ", -sc * " << bt(b) << ");\n"
+          << "  Gbeta[" << c << " * n + i] = sc * " << a(b) << ";\n";
+    } else {
+      src << "  Galpha[" << c << " * n + i] = (" << T << ")0;\n  Gbeta[" << c << " * n + i] = (" << T << ")0;\n";
+    }
+  }
+  src << "}\n";
+  out.code = src.str();
+  out.fp_terms = terms;
+  return out;
+}
+
 namespace {
 
 struct UnitResult {
@@ -438,6 +628,21 @@ bool CgModule::load(const CgBinary& bin, const std::string& kernel_name, std::st
   }
   module_ = mod;
   func_ = f;
+  return true;
+}
+
+bool CgModule::launch_args(void* stream, unsigned grid, unsigned block, size_t smem_bytes, void** args,
+                           std::string* err) {
+  static PFN_launch launch_fn = entry<PFN_launch>("cuLaunchKernel");
+  if (!launch_fn || !func_) {
+    if (err) *err = "CG kernel not loaded";
+    return false;
+  }
+  if (launch_fn(static_cast<CUfunction>(func_), grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem_bytes),
+                static_cast<CUstream>(stream), args, nullptr) != CUDA_SUCCESS) {
+    if (err) *err = "cuLaunchKernel failed for a generated kernel";
+    return false;
+  }
   return true;
 }
 

@@ -50,6 +50,14 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
                               const std::vector<int>& basic_canon, int ncanon, CgSource* out,
                               std::string* why);
 
+// Forward-over-reverse (dual-number) version of generate_cg_source for the
+// parameter gradients.  Kernel parameters: N, pos4, B, Bd (basic tangents),
+// species, ew (dL/dE_i, may be NULL), Galpha, Gbeta ([K*C][N] outputs:
+// c_t (ew a - b) and c_t a) and contrib ([scalar_count][N]:
+// c_t (ew M_s - dM_s), summed over atoms into dL/dw_s by the caller).
+CgSource generate_pg_source(const HostModel& m, const Layered& lay, bool use_float,
+                            const std::vector<int>& basic_canon, int ncanon);
+
 struct CgBinary {
   std::vector<char> cubin;
   std::string log;
@@ -77,6 +85,8 @@ class CgModule {
   // the loaded kernel, call tree included (-1 before load).
   int registers() const { return regs_; }
   int local_bytes() const { return local_; }
+  // Launches with an explicit parameter array.
+  bool launch_args(void* stream, unsigned grid, unsigned block, size_t smem_bytes, void** args, std::string* err);
   // Launches with params: N, pos4, B, G, shift, species, pe, pe_assign, on
   // ceil(N / block) CTAs of `block` threads with smem_bytes dynamic shared memory.
   bool launch(void* stream, int N, const void* pos4, const void* B, void* G, const double* shift,

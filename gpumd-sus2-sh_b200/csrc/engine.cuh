@@ -66,12 +66,26 @@ struct FlatProgram {
 };
 
 // Parameter gradients (param_grad.cu): weights ew = dL/dE_i (N, may be NULL)
-// and fw = dL/dF_i (3N SoA, may be NULL); grad_w [nscalar] and grad_c
-// [kmu*rb] are assigned.  B, Bd, Galpha, Gbeta: [K*C][N]; work: [4 M][N].
+// and fw = dL/dF_i (3N SoA, may be NULL).  Passes: launch_pg_basic (B and its
+// tangent Bd, zeroes grad_c), then the product pass -- the generated
+// forward-over-reverse kernel followed by launch_pg_reduce over its
+// [nscalar][N] per-atom terms, or the flat interpreter launch_pg_product
+// (scratch work [4 M][N]) -- then launch_pg_radial (grad_c [kmu*rb],
+// accumulated).  grad_w [nscalar] is assigned.  B, Bd, Galpha, Gbeta:
+// [K*C][N].  The edge passes return -1 for shapes without an ahead-of-time
+// build.
 template <typename T>
-int launch_param_grad(cudaStream_t s, const EdgeArgs<T>& a, const FlatProgram& p, int M,
-                      const double* species_coeffs, const double* ew, const double* fw, T* B, T* Bd, T* work,
-                      T* Galpha, T* Gbeta, double* grad_w, double* grad_c);
+int launch_pg_basic(cudaStream_t s, const EdgeArgs<T>& a, const double* fw, T* B, T* Bd, double* grad_c);
+template <typename T>
+void launch_pg_product(cudaStream_t s, int N, const FlatProgram& p, int M, const double4* pos4,
+                       const double* species_coeffs, const double* ew, const T* B, const T* Bd, T* work, T* Galpha,
+                       T* Gbeta, double* grad_w);
+// partial: nscalar * 64 doubles of scratch.
+template <typename T>
+void launch_pg_reduce(cudaStream_t s, int nscalar, int N, const T* contrib, double* partial, double* grad_w);
+template <typename T>
+int launch_pg_radial(cudaStream_t s, const EdgeArgs<T>& a, const double* fw, const T* Galpha, const T* Gbeta,
+                     double* grad_c);
 
 // Program tables of a handle, for kernels outside the handle's own path.
 struct CgView {

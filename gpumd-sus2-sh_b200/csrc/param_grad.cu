@@ -231,6 +231,15 @@ __global__ void __launch_bounds__(128)
       const T fc = e.dr * e.dr, dfc = T(2) * e.dr;
       T Y[C], Yd[C];
       harmonics_and_tangent<T, L>(e, tx, ty, tz, ud, Y, Yd);
+      // radial basis of the pair: once per edge when every mu shares (scal, shift)
+      T t0[RB], dt0[RB], xr0 = T(0);
+      if (a.rs.shared_xi) {
+        const T half_scal = T(0.5) * row[0];
+        T xi, dxi;
+        radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
+        chebyshev_d<RB>(xi, t0, dt0);
+        xr0 = fc * half_scal * dxi;
+      }
 #pragma unroll
       for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -243,22 +252,46 @@ __global__ void __launch_bounds__(128)
             Bm = fma(be[k * C + l * l + m], Y[l * l + m], Bm);
             Cm = fma(be[k * C + l * l + m], Yd[l * l + m], Cm);
           }
-          const int pr = a.rs.shared_xi ? 0 : mu;
-          const T half_scal = T(0.5) * row[2 * pr];
-          T xi, dxi;
-          radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * pr + 1])), rational, xi, dxi);
-          T t[RB], dt[RB];
-          chebyshev_d<RB>(xi, t, dt);
+          T t[RB], dt[RB], xr;  // xr = fc * d xi / dr
+          if (a.rs.shared_xi) {
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+              t[q] = t0[q];
+              dt[q] = dt0[q];
+            }
+            xr = xr0;
+          } else {
+            const T half_scal = T(0.5) * row[2 * mu];
+            T xi, dxi;
+            radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi,
+                          dxi);
+            chebyshev_d<RB>(xi, t, dt);
+            xr = fc * half_scal * dxi;
+          }
           const T p1 = ps * fc * (A - Cm);
           const T p2 = ps * ud * Bm;
-          const T xr = fc * half_scal * dxi;  // fc * d xi / dr
 #pragma unroll
           for (int q = 0; q < RB; ++q) acc[mu * RB + q] += p1 * t[q] - p2 * (dfc * t[q] + xr * dt[q]);
         }
     }
   }
+  // warp sums -> per-warp rows in shared memory -> one FP64 atomic per
+  // coefficient per CTA (the CTA has at most 4 warps)
+  __shared__ double part[4][KMU * RB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-  for (int q = 0; q < KMU * RB; ++q) warp_add(grad_c + q, static_cast<double>(acc[q]));
+  for (int q = 0; q < KMU * RB; ++q) {
+    double v = static_cast<double>(acc[q]);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) part[warp][q] = v;
+  }
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int q = threadIdx.x; q < KMU * RB; q += blockDim.x) {
+    double v = 0.0;
+    for (int w = 0; w < nw; ++w) v += part[w][q];
+    if (v != 0.0) atomicAdd(grad_c + q, v);
+  }
 }
 
 inline int blocks(int n, int b) { return (n + b - 1) / b; }
@@ -273,13 +306,42 @@ inline int blocks(int n, int b) { return (n + b - 1) / b; }
   X(2, 2, 8)              \
   X(1, 1, 4)
 
+// dL/dw_s = sum_k contrib[s][k] (the generated product kernel writes the
+// per-atom terms), in two deterministic stages: kPgChunks blocks per scalar
+// write partial sums, then one thread per scalar adds them in order.
+constexpr int kPgChunks = 64;
+
 template <typename T>
-int launch_param_grad(cudaStream_t s, const EdgeArgs<T>& a, const FlatProgram& p, int M,
-                      const double* species_coeffs, const double* ew, const double* fw, T* B, T* Bd, T* work,
-                      T* Galpha, T* Gbeta, double* grad_w, double* grad_c) {
+__global__ void __launch_bounds__(256) k_pg_reduce(int N, const T* __restrict__ contrib, double* __restrict__ partial) {
+  const int s = blockIdx.y, chunk = blockIdx.x;
+  const T* row = contrib + static_cast<size_t>(s) * N;
+  const int per = (N + kPgChunks - 1) / kPgChunks;
+  const int k0 = chunk * per, k1 = min(N, k0 + per);
+  double v = 0.0;
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) v += static_cast<double>(row[k]);
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    partial[static_cast<size_t>(s) * kPgChunks + chunk] = t;
+  }
+}
+
+__global__ void k_pg_reduce_final(int nscalar, const double* __restrict__ partial, double* __restrict__ grad_w) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nscalar) return;
+  double t = 0.0;
+  for (int c = 0; c < kPgChunks; ++c) t += partial[static_cast<size_t>(s) * kPgChunks + c];
+  grad_w[s] = t;
+}
+
+template <typename T>
+int launch_pg_basic(cudaStream_t s, const EdgeArgs<T>& a, const double* fw, T* B, T* Bd, double* grad_c) {
   const size_t sm = sizeof(T) * static_cast<size_t>(a.rs.species) * a.rs.species * a.rs.pair_stride;
   const int grid = blocks(a.N, 128);
-  cudaMemsetAsync(grad_w, 0, sizeof(double) * (p.nscalar > 0 ? p.nscalar : 1), s);
   cudaMemsetAsync(grad_c, 0, sizeof(double) * a.rs.kmu * a.rs.rb, s);
   bool ok = false;
 #define SUS2_PG_BASIC(L, K, RB)                                                     \
@@ -289,9 +351,31 @@ int launch_param_grad(cudaStream_t s, const EdgeArgs<T>& a, const FlatProgram& p
   }
   SUS2_PG_SHAPES(SUS2_PG_BASIC)
 #undef SUS2_PG_BASIC
-  if (!ok) return -1;
-  k_pg_product<T><<<grid, 128, 0, s>>>(a.N, M, p, a.pos4, species_coeffs, ew, B, Bd, work, Galpha, Gbeta, grad_w);
-  ok = false;
+  return ok ? 0 : -1;
+}
+
+template <typename T>
+void launch_pg_product(cudaStream_t s, int N, const FlatProgram& p, int M, const double4* pos4,
+                       const double* species_coeffs, const double* ew, const T* B, const T* Bd, T* work, T* Galpha,
+                       T* Gbeta, double* grad_w) {
+  cudaMemsetAsync(grad_w, 0, sizeof(double) * (p.nscalar > 0 ? p.nscalar : 1), s);
+  k_pg_product<T><<<blocks(N, 128), 128, 0, s>>>(N, M, p, pos4, species_coeffs, ew, B, Bd, work, Galpha, Gbeta,
+                                                 grad_w);
+}
+
+template <typename T>
+void launch_pg_reduce(cudaStream_t s, int nscalar, int N, const T* contrib, double* partial, double* grad_w) {
+  if (nscalar <= 0) return;
+  k_pg_reduce<T><<<dim3(kPgChunks, nscalar), 256, 0, s>>>(N, contrib, partial);
+  k_pg_reduce_final<<<blocks(nscalar, 128), 128, 0, s>>>(nscalar, partial, grad_w);
+}
+
+template <typename T>
+int launch_pg_radial(cudaStream_t s, const EdgeArgs<T>& a, const double* fw, const T* Galpha, const T* Gbeta,
+                     double* grad_c) {
+  const size_t sm = sizeof(T) * static_cast<size_t>(a.rs.species) * a.rs.species * a.rs.pair_stride;
+  const int grid = blocks(a.N, 128);
+  bool ok = false;
 #define SUS2_PG_RADIAL(L, K, RB)                                                    \
   if (!ok && a.l_max == L && a.k_max == K && a.rs.rb == RB) {                       \
     k_pg_radial<T, L, K, RB><<<grid, 128, sm, s>>>(a, fw, Galpha, Gbeta, grad_c);   \
@@ -302,11 +386,14 @@ int launch_param_grad(cudaStream_t s, const EdgeArgs<T>& a, const FlatProgram& p
   return ok ? 0 : -1;
 }
 
-template int launch_param_grad<float>(cudaStream_t, const EdgeArgs<float>&, const FlatProgram&, int, const double*,
-                                      const double*, const double*, float*, float*, float*, float*, float*, double*,
-                                      double*);
-template int launch_param_grad<double>(cudaStream_t, const EdgeArgs<double>&, const FlatProgram&, int,
-                                       const double*, const double*, const double*, double*, double*, double*,
-                                       double*, double*, double*, double*);
+#define SUS2_PG_INSTANTIATE(T)                                                                                      \
+  template int launch_pg_basic<T>(cudaStream_t, const EdgeArgs<T>&, const double*, T*, T*, double*);               \
+  template void launch_pg_product<T>(cudaStream_t, int, const FlatProgram&, int, const double4*, const double*,     \
+                                     const double*, const T*, const T*, T*, T*, T*, double*);                        \
+  template void launch_pg_reduce<T>(cudaStream_t, int, int, const T*, double*, double*);                            \
+  template int launch_pg_radial<T>(cudaStream_t, const EdgeArgs<T>&, const double*, const T*, const T*, double*);
+SUS2_PG_INSTANTIATE(float)
+SUS2_PG_INSTANTIATE(double)
+#undef SUS2_PG_INSTANTIATE
 
 }  // namespace sus2sh

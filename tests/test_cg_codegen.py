@@ -161,3 +161,92 @@ def test_split_kernel_body6_shared_intermediates_on_host(body6_path, tmp_path):
     assert info["split"] == 1
     assert info["smem"] > 2 * 18 * info["block"] * 4   # 18 basics + shared intermediates
     assert de < 1e-6 and dg < 1e-5, (de, dg)
+
+
+# ---------------------------------------------------------------------------
+# forward-over-reverse product kernel of the parameter gradients
+# ---------------------------------------------------------------------------
+_PG_DRIVER = r"""
+extern "C" void run_pg(int N, int block, const float* B, const float* Bd, const int* type, const double* species,
+                       const double* ew, float* Ga, float* Gb, float* contrib) {
+  D4* p4 = new D4[N];
+  for (int i = 0; i < N; ++i) {
+    long long t = type[i];
+    double w;
+    std::memcpy(&w, &t, 8);
+    p4[i] = D4{0, 0, 0, w};
+  }
+  blockDim.x = block;
+  for (int i = 0; i < N; ++i) {
+    threadIdx.x = i % block;
+    blockIdx.x = i / block;
+    KERNEL(N, p4, B, Bd, species, ew, Ga, Gb, contrib);
+  }
+  delete[] p4;
+}
+"""
+
+
+def _flat_dual(m, types, Bm, Bdm, ew):
+    """Flat products in file order with dual numbers (the interpreter's
+    algorithm): returns alpha, beta per basic and contrib per scalar."""
+    N = Bm.shape[1]
+    M = m.alpha_moments_count
+    nb = m.alpha_basic_count
+    Mv = np.zeros((M, N)); Md = np.zeros((M, N))
+    Mv[:nb] = Bm; Md[:nb] = Bdm
+    for (l, r, t, c) in m.products:
+        Md[t] += c * (Md[l] * Mv[r] + Mv[l] * Md[r])
+        Mv[t] += c * Mv[l] * Mv[r]
+    ct = np.asarray(m.species_coeffs)[types]
+    gv = np.zeros((M, N)); gd = np.zeros((M, N))
+    contrib = np.zeros((m.alpha_scalar_moments, N))
+    for s, (mm, w) in enumerate(zip(m.alpha_moment_mapping, m.moment_coeffs)):
+        gv[mm] += ct * w
+        contrib[s] = ct * (ew * Mv[mm] - Md[mm])
+    for (l, r, t, c) in reversed(m.products):
+        gt, gdt = c * gv[t], c * gd[t]
+        gd[l] += gdt * Mv[r] + gt * Md[r]
+        gd[r] += gdt * Mv[l] + gt * Md[l]
+        gv[l] += gt * Mv[r]
+        gv[r] += gt * Mv[l]
+    return ew * gv[:nb] - gd[:nb], gv[:nb], contrib
+
+
+def test_param_grad_product_kernel_matches_flat_duals_on_host(l3k3_path, tmp_path):
+    rc, info, src = _info(l3k3_path, -1, split=2, text_size=1 << 26)
+    assert rc == 0, _lib.load().sus2sh_last_error().decode()
+    name = re.search(r"(sus2sh_pg_\w+)\(int N", src).group(1)
+    canon = dict((int(b), int(c)) for b, c in re.findall(r"v(\d+) = __ldg\(B \+ (\d+) \* n \+ i\)", src))
+    cpp = tmp_path / "pg.cpp"
+    cpp.write_text(_PRELUDE + src.replace('extern "C" __global__', "__global__") + _PG_DRIVER.replace("KERNEL", name))
+    so = tmp_path / "pg.so"
+    subprocess.check_call(["g++", "-O1", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)])
+    lib = ctypes.CDLL(str(so))
+    m = O.Oracle(l3k3_path).model
+    N = 37
+    rng = np.random.default_rng(9)
+    nb = m.alpha_basic_count
+    Bm = rng.normal(0.0, 1.0, (nb, N))
+    Bdm = rng.normal(0.0, 0.3, (nb, N))
+    types = rng.integers(0, m.species_count, N).astype(np.int32)
+    ew = rng.normal(0.0, 1.0, N)
+    al0, be0, co0 = _flat_dual(m, types, Bm, Bdm, ew)
+    ncanon = max(canon.values()) + 1
+    Bc = np.zeros((ncanon, N), np.float32)
+    Bdc = np.zeros((ncanon, N), np.float32)
+    for b, c in canon.items():
+        Bc[c] = Bm[b]
+        Bdc[c] = Bdm[b]
+    Ga = np.zeros((ncanon, N), np.float32)
+    Gb = np.zeros((ncanon, N), np.float32)
+    co = np.zeros((m.alpha_scalar_moments, N), np.float32)
+    species = np.ascontiguousarray(m.species_coeffs, dtype=np.float64)
+    ewc = np.ascontiguousarray(ew)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    lib.run_pg(N, 128, P(Bc), P(Bdc), P(types), P(species), P(ewc), P(Ga), P(Gb), P(co))
+    al = np.array([Ga[canon[b]] for b in range(nb)], dtype=np.float64)
+    be = np.array([Gb[canon[b]] for b in range(nb)], dtype=np.float64)
+    rel = lambda x, y: np.abs(x - y).max() / max(np.abs(y).max(), 1e-30)
+    assert rel(al, al0) < 2e-5 and rel(be, be0) < 2e-5, (rel(al, al0), rel(be, be0))
+    assert rel(co.astype(np.float64), co0) < 2e-5, rel(co.astype(np.float64), co0)
