@@ -70,6 +70,25 @@ def test_param_grad_matches_finite_differences(setup, fp64):
     pot.close()
 
 
+@pytest.mark.parametrize("fp64", [True, False])
+def test_generated_and_interpreted_products_agree(setup, fp64):
+    # the model-specialised forward-over-reverse product kernel (default) and
+    # the flat-product interpreter (sus2_sh_cg_jit=0, used for graphs above the
+    # straight-line size) give the same gradients
+    path, cells, targets = setup
+    opts = ["Cu", "Zr"] + (["sus2_float=0"] if fp64 else [])
+    pot = SUS2_SH(path, cells[0][1].size, opts)
+    L1, gw1, gc1 = loss_and_grad(pot, cells, targets)
+    pot.close()
+    pot = SUS2_SH(path, cells[0][1].size, opts + ["sus2_sh_cg_jit=0"])
+    L2, gw2, gc2 = loss_and_grad(pot, cells, targets)
+    pot.close()
+    tol = 1e-10 if fp64 else 2e-5
+    assert abs(L1 - L2) <= tol * max(1.0, abs(L2))
+    assert np.abs(gw1 - gw2).max() <= tol * np.abs(gw2).max()
+    assert np.abs(gc1 - gc2).max() <= tol * np.abs(gc2).max()
+
+
 def test_energy_only_gradient_is_moment_sum(setup):
     # with force_weight = 0 and unit energy weights, dL/dw_s = sum_i c_t M_i[s]:
     # compare against the oracle's moments through the linear structure of E
