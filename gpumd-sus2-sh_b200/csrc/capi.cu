@@ -336,6 +336,11 @@ struct Engine {
   int calls_since_build = 0;
   DevBuf<double4> pos4, ref4;
   DevBuf<int> nbr, ncount, cell_count, cell_start, cell_atoms, atom_cell, atom_rank;
+  // in-cutoff sub-list of the current positions, written by the basic-moment
+  // kernel and walked by the force kernel (cut_valid: written since the last
+  // change of positions or list)
+  DevBuf<int> cut_nbr, cut_count;
+  bool cut_valid = false;
   DevBuf<unsigned char> Bbuf, Gbuf, scratch, ftmp;
   DevBuf<Status> d_status;
   Status* h_status = nullptr;  // pinned
@@ -603,6 +608,9 @@ struct Engine {
     }
     cap = 0;
     nbr.release();
+    cut_nbr.release();
+    cut_count.resize(N);
+    cut_valid = false;
     have_ref = false;
     force_next = true;
   }
@@ -618,6 +626,9 @@ struct Engine {
     a.pos4 = pos4.p;
     a.nbr = nbr.p;
     a.ncount = ncount.p;
+    a.cut_nbr = cut_nbr.p;
+    a.cut_count = cut_count.p;
+    a.use_cut = 0;
     a.pair_table = use_float ? static_cast<const void*>(d_pair_f.p) : static_cast<const void*>(d_pair_d.p);
     if (batch_active) {
       a.shift = reinterpret_cast<const double(*)[3]>(d_cell_shift.p);
@@ -721,6 +732,7 @@ struct Engine {
   // can be captured in a CUDA graph.
   void prepare_batch(cudaStream_t s, int n, int ncells, const int* off, const double* cell_h, const int* cell_pbc,
                      const int* type, const double* x) {
+    cut_valid = false;  // new positions
     if (ncells <= 0) throw InputError("sus2sh batch: ncells must be positive.");
     ensure_size(n);
     last_stream = s;
@@ -760,6 +772,7 @@ struct Engine {
 
   // Positions -> pos4, conditional neighbour build.
   void prepare(cudaStream_t s, int n, const double* h, const int* pbc, const int* type, const double* x) {
+    cut_valid = false;  // new positions
     ensure_size(n);
     last_stream = s;
     batch_active = false;
@@ -818,6 +831,8 @@ struct Engine {
     if (c <= cap) return;
     cap = c;
     nbr.resize(static_cast<size_t>(cap) * N);
+    cut_nbr.resize(static_cast<size_t>(cap) * N);
+    cut_valid = false;
   }
 
   ZblTables zbl_tables() const {
@@ -846,15 +861,19 @@ struct Engine {
       if (!ejit_mod.load(*ejit_bin, &err) ||
           !ejit_mod.launch_basic(s, a.N, 128, edge_smem<T>(), &a, out, gated, &err))
         throw CudaError(err);
+      cut_valid = true;
       return;
     }
     if (launch_basic<T>(s, a, reinterpret_cast<T*>(out), gated ? 128 : block, gated) != 0)
       throw InputError("SUS2_SH basic kernel shape not compiled.");
+    cut_valid = true;
   }
 
   template <typename T>
-  void run_force(cudaStream_t s, const EdgeArgs<T>& a, const void* G, bool gated, const double* weight,
+  void run_force(cudaStream_t s, const EdgeArgs<T>& a_in, const void* G, bool gated, const double* weight,
                  double* force, double* virial, double sign, int block) {
+    EdgeArgs<T> a = a_in;
+    a.use_cut = cut_valid ? 1 : 0;
     if (edge_jit) {
       std::string err;
       if (!ejit_mod.load(*ejit_bin, &err) ||
@@ -892,8 +911,10 @@ struct Engine {
     float best_b = 1e30f, best_f = 1e30f;
     for (int block : {64, 128, 256}) {
       const float tb = time_it([&] { launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block, false); });
+      EdgeArgs<T> af = a;
+      af.use_cut = 1;  // the basic launches above wrote the in-cutoff sub-list
       const float tf = time_it([&] {
-        launch_force<T>(s, a, reinterpret_cast<const T*>(Gbuf.p), nullptr, ftmp.p, f_scratch.p, w_scratch.p, 1.0,
+        launch_force<T>(s, af, reinterpret_cast<const T*>(Gbuf.p), nullptr, ftmp.p, f_scratch.p, w_scratch.p, 1.0,
                         block);
       });
       launches += 4;

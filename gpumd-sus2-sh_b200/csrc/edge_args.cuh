@@ -29,6 +29,12 @@ struct EdgeArgs {
   const double4* pos4;
   const int* nbr;
   const int* ncount;
+  // in-cutoff sub-list [cap][N] / counts [N]: k_basic writes it (when
+  // cut_nbr is set) in the order of the full list, k_force then walks only
+  // those pairs (when use_cut is set) instead of testing every listed pair
+  int* cut_nbr;
+  int* cut_count;
+  int use_cut;
   const void* pair_table;   // T[S*S][pair_stride]
   const double (*shift)[3];  // image vectors [cells][125][3] (one box: BoxGeom::shift)
   const int* atom_cell;      // cell of each atom in a batch of boxes, NULL for one box

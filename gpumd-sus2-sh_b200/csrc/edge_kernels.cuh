@@ -57,6 +57,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
   const int cnt = min(a.ncount[i], a.cap);
   const double rc = a.rs.rc, rc2 = rc * rc;
   NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
+  int* const cut = a.cut_nbr ? a.cut_nbr + i : nullptr;
+  int ncut = 0;
   for (int n = 0; n < cnt; ++n) {
     int w;
     double4 pj;
@@ -68,6 +70,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
     const double dz = pj.z - pi.z + sz;
     const double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 >= rc2) continue;
+    if (cut) cut[static_cast<size_t>(ncut++) * a.N] = w;
     const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
     const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
     T R[KMU];
@@ -87,6 +90,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
         for (int m = 0; m <= 2 * l; ++m)
           acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], P[l * l + m], acc[k * C + l * l + m]);
   }
+  if (cut) a.cut_count[i] = ncut;
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -152,9 +156,13 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
   const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
   const int S = a.rs.species;
   const int row_i = type_of(pi) * S;
-  const int cnt = min(a.ncount[i], a.cap);
+  // the in-cutoff sub-list written by k_basic when available (every pair in
+  // it passes the test below, so no lane idles on a listed pair outside rc),
+  // else the full list
+  const bool sub = a.use_cut != 0;
+  const int cnt = sub ? a.cut_count[i] : min(a.ncount[i], a.cap);
   const double rc = a.rs.rc, rc2 = rc * rc;
-  NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
+  NeighborStream ns(sub ? a.cut_nbr : a.nbr, a.pos4, a.N, i, cnt);
   for (int n = 0; n < cnt; ++n) {
     int wd;
     double4 pj;
