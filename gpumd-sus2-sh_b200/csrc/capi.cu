@@ -31,6 +31,11 @@ thread_local std::string g_last_error;
 // graphs that split into no small components run the row interpreter.
 constexpr long long kCgSingleMaxProducts = 3000;
 
+// Margin (A) of the inner neighbour list the basic-moment kernel walks: the
+// listed pairs within rc + margin, refiltered from the full list whenever an
+// atom has moved more than margin / 2 since the last build.
+constexpr double kInnerMargin = 0.2;
+
 // The CG kernel source the engine builds for a model: the single straight-line
 // function, the component-split kernel (split: -1 auto, 0 never, 1 always), or
 // none (false; the row interpreter runs, *why says why).
@@ -341,6 +346,10 @@ struct Engine {
   // change of positions or list)
   DevBuf<int> cut_nbr, cut_count;
   bool cut_valid = false;
+  // inner list: listed pairs within rc + kInnerMargin (single boxes with a
+  // skin above the margin), walked by the basic-moment kernel
+  DevBuf<int> inner_nbr, inner_count;
+  bool inner_valid = false;
   DevBuf<unsigned char> Bbuf, Gbuf, scratch, ftmp;
   DevBuf<Status> d_status;
   Status* h_status = nullptr;  // pinned
@@ -611,6 +620,9 @@ struct Engine {
     cut_nbr.release();
     cut_count.resize(N);
     cut_valid = false;
+    inner_nbr.release();
+    inner_count.resize(N);
+    inner_valid = false;
     have_ref = false;
     force_next = true;
   }
@@ -629,6 +641,8 @@ struct Engine {
     a.cut_nbr = cut_nbr.p;
     a.cut_count = cut_count.p;
     a.use_cut = 0;
+    a.inner_nbr = inner_valid ? inner_nbr.p : nullptr;
+    a.inner_count = inner_count.p;
     a.pair_table = use_float ? static_cast<const void*>(d_pair_f.p) : static_cast<const void*>(d_pair_d.p);
     if (batch_active) {
       a.shift = reinterpret_cast<const double(*)[3]>(d_cell_shift.p);
@@ -732,6 +746,7 @@ struct Engine {
   // can be captured in a CUDA graph.
   void prepare_batch(cudaStream_t s, int n, int ncells, const int* off, const double* cell_h, const int* cell_pbc,
                      const int* type, const double* x) {
+    inner_valid = false;  // the batch list holds only pairs within rc
     cut_valid = false;  // new positions
     if (ncells <= 0) throw InputError("sus2sh batch: ncells must be positive.");
     ensure_size(n);
@@ -815,10 +830,19 @@ struct Engine {
       grow_capacity(st.max_count);
       force = true;
     }
+    const bool use_inner = opt.skin > kInnerMargin;
+    const double inner = model.rc + kInnerMargin;
     launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
                  cell_start.p, cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
                  d_status.p);
     launches += 8;
+    inner_valid = false;
+    if (use_inner) {
+      launch_inner(s, N, d_status.p, static_cast<float>(0.25 * kInnerMargin * kInnerMargin), inner * inner, pos4.p,
+                   nbr.p, ncount.p, cap, d_geom.p, inner_nbr.p, inner_count.p);
+      launches += 1;
+      inner_valid = true;
+    }
     ck(cudaGetLastError(), "neighbour build launch");
     have_ref = true;
     force_next = false;
@@ -832,6 +856,7 @@ struct Engine {
     cap = c;
     nbr.resize(static_cast<size_t>(cap) * N);
     cut_nbr.resize(static_cast<size_t>(cap) * N);
+    inner_nbr.resize(static_cast<size_t>(cap) * N);
     cut_valid = false;
   }
 

@@ -35,6 +35,10 @@ struct EdgeArgs {
   int* cut_nbr;
   int* cut_count;
   int use_cut;
+  // inner list (pairs within rc + a margin, list order) walked by k_basic
+  // instead of nbr / ncount when set
+  const int* inner_nbr;
+  const int* inner_count;
   const void* pair_table;   // T[S*S][pair_stride]
   const double (*shift)[3];  // image vectors [cells][125][3] (one box: BoxGeom::shift)
   const int* atom_cell;      // cell of each atom in a batch of boxes, NULL for one box

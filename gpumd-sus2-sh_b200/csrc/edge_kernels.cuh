@@ -54,9 +54,11 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
   const double(*cell_shift)[3] = a.shift + (a.atom_cell ? 125 * a.atom_cell[i] : 0);
   const int S = a.rs.species;
   const int row_i = type_of(pi) * S;
-  const int cnt = min(a.ncount[i], a.cap);
+  // the inner list (pairs within rc + margin) when the engine keeps one
+  const bool inner = a.inner_nbr != nullptr;
+  const int cnt = inner ? a.inner_count[i] : min(a.ncount[i], a.cap);
   const double rc = a.rs.rc, rc2 = rc * rc;
-  NeighborStream ns(a.nbr, a.pos4, a.N, i, cnt);
+  NeighborStream ns(inner ? a.inner_nbr : a.nbr, a.pos4, a.N, i, cnt);
   int* const cut = a.cut_nbr ? a.cut_nbr + i : nullptr;
   int ncut = 0;
   for (int n = 0; n < cnt; ++n) {

@@ -271,6 +271,31 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
   if (!count_only) pos4[i] = p;
 }
 
+// Inner list: the listed pairs within rc + margin, in list order, for the
+// basic-moment kernel.  Rebuilt at every full build and on every call whose
+// largest displacement since that build exceeds margin / 2 (so it holds every
+// pair within rc); otherwise it returns at once.
+__global__ void k_inner(int N, const Status* __restrict__ st, float half_margin2, double inner2,
+                        const double4* __restrict__ pos4, const int* __restrict__ nbr,
+                        const int* __restrict__ ncount, int cap, const BoxGeom* __restrict__ g,
+                        int* __restrict__ inner_nbr, int* __restrict__ inner_count) {
+  if (!st->rebuilt && !(__uint_as_float(st->maxdisp2_bits) > half_margin2)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double4 pi = pos4[i];
+  const int cnt = min(ncount[i], cap);
+  int k = 0;
+  for (int n = 0; n < cnt; ++n) {
+    const int w = __ldg(nbr + static_cast<size_t>(n) * N + i);
+    const double4 pj = pos4[w & 0xFFFFFF];
+    double sx, sy, sz;
+    image_shift(g->shift, static_cast<unsigned>(w) >> 24, sx, sy, sz);
+    const double dx = pj.x - pi.x + sx, dy = pj.y - pi.y + sy, dz = pj.z - pi.z + sz;
+    if (dx * dx + dy * dy + dz * dz < inner2) inner_nbr[static_cast<size_t>(k++) * N + i] = w;
+  }
+  inner_count[i] = k;
+}
+
 template <typename T>
 __global__ void k_finalize(int N, const void* __restrict__ ftmp, double* __restrict__ force,
                            double sign);
@@ -584,6 +609,13 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
   k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, cell_start, cell_atoms);
   k_fill<<<blocks_for(N, 128), 128, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms,
                                              atom_cell, nbr, ncount, pos4, cap, count_only);
+}
+
+void launch_inner(cudaStream_t s, int N, const Status* st, float half_margin2, double inner2, const double4* pos4,
+                  const int* nbr, const int* ncount, int cap, const BoxGeom* geom_dev, int* inner_nbr,
+                  int* inner_count) {
+  k_inner<<<blocks_for(N, 128), 128, 0, s>>>(N, st, half_margin2, inner2, pos4, nbr, ncount, cap, geom_dev,
+                                              inner_nbr, inner_count);
 }
 
 // Compiled (L, K, RB) shapes of the edge kernels.

@@ -99,6 +99,12 @@ struct CgView {
 // ---- launchers (engine.cu) ----------------------------------------------
 void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const double4* ref4,
                  double4* pos4, const BoxGeom* geom_dev, int have_ref, int species, Status* st);
+// Inner list of the listed pairs within sqrt(inner2) (k_inner); runs when the
+// list was rebuilt in this call or the largest displacement since the build
+// exceeds sqrt(half_margin2).
+void launch_inner(cudaStream_t s, int N, const Status* st, float half_margin2, double inner2, const double4* pos4,
+                  const int* nbr, const int* ncount, int cap, const BoxGeom* geom_dev, int* inner_nbr,
+                  int* inner_count);
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
                   const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
                   int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
