@@ -134,17 +134,17 @@ def edges_within(box, pos, rc):
 
 # DRAM bytes of one k_force launch (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the 524,288-atom l3k3 case (64x64x32 FCC cells, FP32,
-# 256-thread CTAs): 292.33 MB read + 43.09 MB written.  The traffic grows with
-# the atom count, so the bench scales it per atom.
-K_FORCE_DRAM_BYTES_PER_ATOM = (292.33e6 + 43.09e6) / 524288
+# 64-thread CTAs, walking the in-cutoff sub-list): 267.18 MB read + 40.97 MB
+# written.  The traffic grows with the atom count, so the bench scales it per atom.
+K_FORCE_DRAM_BYTES_PER_ATOM = (267.18e6 + 40.97e6) / 524288
 
 
-def k_force_algorithmic_bytes(nbasic, listed_per_atom):
+def k_force_algorithmic_bytes(nbasic, cut_per_atom):
     """Bytes k_force must move per atom: adjoints G (4 nbasic), position and
-    species (32), neighbour count and list (4 + 4 per listed neighbour), the
-    FP32 scatter buffer (16) and the FP64 force (24, read + written) and
-    virial (72, read + written) it accumulates into."""
-    return 4 * nbasic + 32 + 4 + 4 * listed_per_atom + 16 + 2 * 24 + 2 * 72
+    species (32), the in-cutoff neighbour count and list it walks (4 + 4 per
+    pair inside rc), the FP32 scatter buffer (16) and the FP64 force (24,
+    read + written) and virial (72, read + written) it accumulates into."""
+    return 4 * nbasic + 32 + 4 + 4 * cut_per_atom + 16 + 2 * 24 + 2 * 72
 
 
 def flops_model(kmu, rb, C, Bb, P):
@@ -484,8 +484,7 @@ def main():
                              "traffic": K_FORCE_DRAM_BYTES_PER_ATOM * N,
                              "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_force on the "
                                                "524,288-atom case, scaled per atom",
-                             "algorithmic_bytes": k_force_algorithmic_bytes(
-                                 info["basics"], edges_within(box, pos, pot.rc + SKIN) / N) * N,
+                             "algorithmic_bytes": k_force_algorithmic_bytes(info["basics"], edges / N) * N,
                              "peak_source": "measured FP32 FMA-chain microbenchmark on this GPU (burst)",
                              "flops_per_edge": ff, "edges_per_launch": edges,
                              "launch_ms": force_ms_launch,
