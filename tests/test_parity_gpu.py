@@ -105,6 +105,45 @@ def test_open_boundaries(l3k3_path):
     compare(l3k3_path, mixed, types, pos + np.array([[0.0], [20.0], [0.0]]))
 
 
+def per_mu_radial_model(src, dst):
+    """Copy of model ``src`` whose radial functions each get their own (scal,
+    shift) per species pair, so no radial argument is shared between them
+    (scal_coeffs holds, per radial function, S*S scales then S*S shifts)."""
+    import re
+    text = open(src).read()
+    S = int(re.search(r"species_count = (\d+)", text).group(1))
+    m = re.search(r"scal_coeffs = \{([^}]*)\}", text)
+    n = len(m.group(1).split(","))
+    vals = []
+    for mu in range(n // (2 * S * S)):
+        vals += [0.8 + 0.07 * mu + 0.1 * p for p in range(S * S)]
+        vals += [2.9 + 0.11 * mu - 0.05 * p for p in range(S * S)]
+    text = text[:m.start(1)] + ", ".join(repr(v) for v in vals) + text[m.end(1):]
+    with open(dst, "w") as fh:
+        fh.write(text)
+    return dst
+
+
+def test_per_function_radial_arguments(l3k3_path, tmp_path):
+    # every radial function with its own (scal, shift): the per-function
+    # radial map of the moment and force kernels (the preset models share one
+    # radial argument between all functions of a pair)
+    path = per_mu_radial_model(l3k3_path, str(tmp_path / "per_mu.mtp"))
+    box, types, pos = structures.fcc(6, 6, 6, 3.8, (0.6, 0.4), 0.08, seed=21)
+    pe0, f0, w0 = O.Oracle(path).efs(box.cpu_h, box.pbc, types, pos)
+    pe, f, w = engine_efs(path, box, types, pos)
+    # this model's site energies are larger than the preset's; single FP32
+    # site energies reach about 1.4e-6 eV, so, as for the hot MD frame, the
+    # energy bar is per atom of the system, with an RMS and a 5x max bar per site
+    de = pe - pe0
+    assert abs(de.sum()) / de.size < E_TOL32, de.sum()
+    assert np.sqrt((de ** 2).mean()) < E_TOL32, np.sqrt((de ** 2).mean())
+    assert np.abs(de).max() < 5 * E_TOL32, np.abs(de).max()
+    assert np.sqrt(((f - f0) ** 2).mean()) < F_RMS32
+    assert np.sqrt(((w - w0) ** 2).mean()) < W_RMS32
+    compare(path, box, types, pos, fp64=True)
+
+
 @pytest.mark.parametrize("opts", [(), ("sus2_sh_cg_split=0",)], ids=["split_kernel", "row_interpreter"])
 def test_large_model_rational_three_species(l4k4_path, opts):
     # body-5 L=4 K=4 graph: the component-split CG kernel (default for this
