@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <map>
 #include <memory>
 #include <random>
@@ -398,7 +399,10 @@ struct Engine {
   DevBuf<double> d_g_coef, d_g_w, d_g_mix, d_g_add;
   DevBuf<char> Bg, Gg, gslots, gmult, gderiv, gadj;
   // edge kernels built with NVRTC at load (shapes without an ahead-of-time build)
-  bool edge_jit = false;
+  // edge kernels: 0 ahead-of-time build, 1 NVRTC build of the shape (shapes
+  // without an ahead-of-time build, sus2_sh_edge_jit=1, FP64 and gate models),
+  // 2 NVRTC build specialised to this FP32 model's radial coefficients
+  int edge_jit = 0;
   std::shared_ptr<const EdgeJitBinary> ejit_bin;
   EdgeJitModule ejit_mod;
   // model-specialised CG kernel (NVRTC); empty cubin -> interpreter
@@ -459,11 +463,7 @@ struct Engine {
     profile = opt.profile;
     lay = layer_products(model);
     prog = compile_program(model, lay);
-    // shapes without an ahead-of-time build (or sus2_sh_edge_jit=1) get their
-    // edge kernels from NVRTC now
-    edge_jit = opt.edge_jit || !shape_supported(model.l_max, model.k_max, model.rb_size);
     gate = model.gate.enabled;
-    if (edge_jit) ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
     list_cutoff = model.rc;
     if (model.zbl_enabled) {
       // atomic numbers from the model, else from the element symbols after the
@@ -527,6 +527,27 @@ struct Engine {
       throw InputError("SUS2_SH radial pair table too large (species_count^2 * (2*radial_funcs+1) > 8192).");
     dcoef = chebyshev_derivative(coef, kmu, rb);
     if (gate) gate_dcoef = chebyshev_derivative(gate_coef, kmu, rb);
+    // edge kernels from NVRTC now: specialised to the model (FP32, non-gate),
+    // or for the shape when it has no ahead-of-time build (or on request)
+    if (opt.edge_jit) {
+      edge_jit = 1;
+    } else if (use_float && !gate && opt.model_edges) {
+      edge_jit = 2;
+    } else if (!shape_supported(model.l_max, model.k_max, model.rb_size)) {
+      edge_jit = 1;
+    }
+    std::future<std::shared_ptr<const EdgeJitBinary>> model_edges;
+    if (edge_jit == 2) {
+      // built on host threads while the CG kernel below compiles
+      std::vector<float> table(kMaxCoef);
+      table.resize(fill_coef(coef, dcoef, table.data()));
+      model_edges = std::async(std::launch::async, [l = model.l_max, k = model.k_max, rb = model.rb_size, table,
+                                                    shared_xi = rs.shared_xi != 0, rational = rs.rational != 0] {
+        return compile_model_edge_kernels(l, k, rb, table, shared_xi, rational);
+      });
+    } else if (edge_jit == 1) {
+      ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
+    }
     // device uploads
     d_code.upload(prog.code);
     if (use_float) {
@@ -587,6 +608,7 @@ struct Engine {
         cg_bin = compile_cg_source(cg_src);
       cg_compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
+    if (model_edges.valid()) ejit_bin = model_edges.get();
     if (num_atoms > 0) ensure_size(num_atoms);
   }
 
@@ -651,19 +673,25 @@ struct Engine {
       a.shift = d_geom.p->shift;
       a.atom_cell = nullptr;
     }
-    for (size_t k = 0; k < coef.size(); ++k) a.coef[k] = static_cast<T>(coef[k]);
-    if (2 * coef.size() <= static_cast<size_t>(kMaxCoef))
-      for (size_t k = 0; k < dcoef.size(); ++k) a.coef[coef.size() + k] = static_cast<T>(dcoef[k]);
+    fill_coef(coef, dcoef, a.coef);
     return a;
+  }
+
+  // The edge kernels' coefficient table: c[mu][n], then the derivative series
+  // when both fit kMaxCoef.  Returns the entries written.
+  template <typename T>
+  static size_t fill_coef(const std::vector<double>& c, const std::vector<double>& d, T* out) {
+    for (size_t k = 0; k < c.size(); ++k) out[k] = static_cast<T>(c[k]);
+    if (2 * c.size() > static_cast<size_t>(kMaxCoef)) return c.size();
+    for (size_t k = 0; k < d.size(); ++k) out[c.size() + k] = static_cast<T>(d[k]);
+    return c.size() + d.size();
   }
 
   // EdgeArgs of the gate's first layer: same pair tables, gate coefficients.
   template <typename T>
   EdgeArgs<T> edge_args_gate() const {
     EdgeArgs<T> a = edge_args<T>();
-    for (size_t k = 0; k < gate_coef.size(); ++k) a.coef[k] = static_cast<T>(gate_coef[k]);
-    if (2 * gate_coef.size() <= static_cast<size_t>(kMaxCoef))
-      for (size_t k = 0; k < gate_dcoef.size(); ++k) a.coef[gate_coef.size() + k] = static_cast<T>(gate_dcoef[k]);
+    fill_coef(gate_coef, gate_dcoef, a.coef);
     return a;
   }
 
@@ -878,13 +906,22 @@ struct Engine {
     return sizeof(T) * static_cast<size_t>(rs.species) * rs.species * rs.pair_stride;
   }
 
+  // CTA size of an NVRTC launch: the requested one when the module has it
+  // (the model-specialised build has 64, 128 and 256), else its first.
+  int jit_block(int block, bool gated) const {
+    if (gated) return 128;
+    for (int b : ejit_bin->blocks)
+      if (b == block) return block;
+    return ejit_bin->blocks.front();
+  }
+
   // k_basic / k_force through the ahead-of-time build or the NVRTC module.
   template <typename T>
   void run_basic(cudaStream_t s, const EdgeArgs<T>& a, void* out, bool gated, int block) {
     if (edge_jit) {
       std::string err;
       if (!ejit_mod.load(*ejit_bin, &err) ||
-          !ejit_mod.launch_basic(s, a.N, 128, edge_smem<T>(), &a, out, gated, &err))
+          !ejit_mod.launch_basic(s, a.N, jit_block(block, gated), edge_smem<T>(), &a, out, gated, &err))
         throw CudaError(err);
       cut_valid = true;
       return;
@@ -902,8 +939,8 @@ struct Engine {
     if (edge_jit) {
       std::string err;
       if (!ejit_mod.load(*ejit_bin, &err) ||
-          !ejit_mod.launch_force(s, a.N, 128, edge_smem<T>(), &a, G, weight, ftmp.p, force, virial, sign, gated,
-                                 &err))
+          !ejit_mod.launch_force(s, a.N, jit_block(block, gated), edge_smem<T>(), &a, G, weight, ftmp.p, force,
+                                 virial, sign, gated, &err))
         throw CudaError(err);
       return;
     }
@@ -915,7 +952,7 @@ struct Engine {
   template <typename T>
   void autotune(cudaStream_t s, const EdgeArgs<T>& a) {
     tuned = true;
-    if (!opt.autotune || sizeof(T) != 4 || edge_jit || gate) return;
+    if (!opt.autotune || sizeof(T) != 4 || edge_jit == 1 || gate) return;
     DevBuf<double> f_scratch, w_scratch;
     f_scratch.resize(3ull * N);
     w_scratch.resize(9ull * N);
@@ -935,12 +972,10 @@ struct Engine {
     };
     float best_b = 1e30f, best_f = 1e30f;
     for (int block : {64, 128, 256}) {
-      const float tb = time_it([&] { launch_basic<T>(s, a, reinterpret_cast<T*>(Bbuf.p), block, false); });
-      EdgeArgs<T> af = a;
-      af.use_cut = 1;  // the basic launches above wrote the in-cutoff sub-list
+      const float tb = time_it([&] { run_basic<T>(s, a, Bbuf.p, false, block); });
       const float tf = time_it([&] {
-        launch_force<T>(s, af, reinterpret_cast<const T*>(Gbuf.p), nullptr, ftmp.p, f_scratch.p, w_scratch.p, 1.0,
-                        block);
+        // the basic launches above wrote the in-cutoff sub-list
+        run_force<T>(s, a, Gbuf.p, false, nullptr, f_scratch.p, w_scratch.p, 1.0, block);
       });
       launches += 4;
       if (tb < best_b) {
@@ -1391,7 +1426,7 @@ int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
                      e.use_float ? 1 : 0, e.cap, e.h_status ? e.h_status->builds : 0,
                      static_cast<int>(e.launches & 0x7fffffff), e.rs.shared_xi, e.prod_global ? 1 : 0,
                      e.cg_bin.cubin.empty() ? 0 : 1, e.cg_bin.registers, static_cast<int>(e.cg_compile_ms),
-                     e.basic_block, e.force_block, e.edge_jit ? 1 : 0,
+                     e.basic_block, e.force_block, e.edge_jit,
                      e.ejit_bin ? e.ejit_bin->basic_registers : -1, e.ejit_bin ? e.ejit_bin->force_registers : -1,
                      e.ejit_bin ? static_cast<int>(e.ejit_bin->compile_ms) : 0,
                      e.gate ? static_cast<int>(e.model.gate.mode) : 0,
@@ -1555,6 +1590,38 @@ int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_r
     if (basic_registers) *basic_registers = bin->basic_registers;
     if (force_registers) *force_registers = bin->force_registers;
     if (compile_ms) *compile_ms = bin->compile_ms;
+    if (log && log_len) {
+      std::strncpy(log, bin->log.c_str(), log_len - 1);
+      log[log_len - 1] = '\0';
+    }
+  });
+}
+
+int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t log_len) {
+  if (!path || !info) return SUS2SH_E_ARG;
+  return guarded([&] {
+    const sus2sh::HostModel m = sus2sh::load_model(path);
+    const std::vector<double> dc = sus2sh::chebyshev_derivative(m.radial_coeffs, m.radial_funcs, m.rb_size);
+    std::vector<float> table(sus2sh::kMaxCoef);
+    table.resize(sus2sh::Engine::fill_coef(m.radial_coeffs, dc, table.data()));
+    // one radial argument per pair when every function of every pair has the
+    // (scal, shift) of the pair's first function (as the engine finds at load)
+    const int S = m.species_count, kmu = m.radial_funcs;
+    bool shared = true;
+    for (int p = 0; p < S * S; ++p)
+      for (int mu = 0; mu < kmu; ++mu)
+        shared = shared && m.scal_coeffs[2 * mu * S * S + p] == m.scal_coeffs[p] &&
+                 m.scal_coeffs[2 * mu * S * S + S * S + p] == m.scal_coeffs[S * S + p];
+    const auto bin = sus2sh::compile_model_edge_kernels(m.l_max, m.k_max, m.rb_size, table, shared,
+                                                        m.radial_map == sus2sh::RadialMap::Rational);
+    info[0] = bin->basic_registers;
+    info[1] = bin->force_registers;
+    info[2] = static_cast<int>(bin->compile_ms);
+    info[3] = static_cast<int>(bin->global_bytes);
+    info[4] = static_cast<int>(table.size());
+    size_t bytes = 0;
+    for (const auto& c : bin->cubins) bytes += c.size();
+    info[5] = static_cast<int>(bytes);
     if (log && log_len) {
       std::strncpy(log, bin->log.c_str(), log_len - 1);
       log[log_len - 1] = '\0';

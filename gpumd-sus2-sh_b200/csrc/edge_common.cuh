@@ -11,6 +11,23 @@ namespace edge {
 
 constexpr int kCenterCode = 62;  // image (0,0,0) in base-5 codes
 
+// Radial coefficient X (c[mu][n], then the derivative series), whether all
+// radial functions of a pair share one radial argument, and whether the
+// radial map is the rational one: from the kernel parameters, or, in a build
+// specialised to one model, compiled in (model_coef() table and the
+// SUS2_MODEL_SHARED_XI / SUS2_MODEL_RATIONAL constants), so every coefficient
+// of an unrolled loop is an immediate operand and the per-edge tests of the
+// radial setup disappear.
+#ifdef SUS2_MODEL_COEF
+#define SUS2_COEF(a, X) (::sus2sh::edge::model_coef(X))
+#define SUS2_SHARED_XI(a) (SUS2_MODEL_SHARED_XI != 0)
+#define SUS2_RATIONAL(a) (SUS2_MODEL_RATIONAL != 0)
+#else
+#define SUS2_COEF(a, X) ((a).coef[X])
+#define SUS2_SHARED_XI(a) ((a).rs.shared_xi != 0)
+#define SUS2_RATIONAL(a) ((a).rs.rational != 0)
+#endif
+
 __device__ __forceinline__ int type_of(const double4& p) {
   return static_cast<int>(__double_as_longlong(p.w));
 }
@@ -75,8 +92,8 @@ template <typename T, int KMU, int RB>
 __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __restrict__ row,
                                               const Edge<T>& e, T* R) {
   const T f = row[2 * KMU] * e.dr * e.dr;
-  const bool rational = a.rs.rational != 0;
-  if (a.rs.shared_xi) {
+  const bool rational = SUS2_RATIONAL(a);
+  if (SUS2_SHARED_XI(a)) {
     T xi, dxi;
     radial_map<T>(T(0.5) * row[0] * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
     T t[RB];
@@ -85,7 +102,7 @@ __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __r
     for (int mu = 0; mu < KMU; ++mu) {
       T s = T(0);
 #pragma unroll
-      for (int n = 0; n < RB; ++n) s = fma(a.coef[mu * RB + n], t[n], s);
+      for (int n = 0; n < RB; ++n) s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
       R[mu] = f * s;
     }
   } else {
@@ -98,7 +115,7 @@ __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __r
       chebyshev<RB>(xi, t);
       T s = T(0);
 #pragma unroll
-      for (int n = 0; n < RB; ++n) s = fma(a.coef[mu * RB + n], t[n], s);
+      for (int n = 0; n < RB; ++n) s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
       R[mu] = f * s;
     }
   }
@@ -110,8 +127,8 @@ __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T
   const T ps = row[2 * KMU];
   const T f = ps * e.dr * e.dr;
   const T df = T(2) * ps * e.dr;
-  const bool rational = a.rs.rational != 0;
-  if (a.rs.shared_xi) {
+  const bool rational = SUS2_RATIONAL(a);
+  if (SUS2_SHARED_XI(a)) {
     const T half_scal = T(0.5) * row[0];
     T xi, dxi;
     radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
@@ -123,8 +140,8 @@ __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T
       T s = T(0), sd = T(0);
 #pragma unroll
       for (int n = 0; n < RB; ++n) {
-        s = fma(a.coef[mu * RB + n], t[n], s);
-        sd = fma(a.coef[mu * RB + n], dt[n], sd);
+        s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
+        sd = fma(SUS2_COEF(a, mu * RB + n), dt[n], sd);
       }
       R[mu] = f * s;
       dR[mu] = df * s + g * sd;
@@ -140,8 +157,8 @@ __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T
       T s = T(0), sd = T(0);
 #pragma unroll
       for (int n = 0; n < RB; ++n) {
-        s = fma(a.coef[mu * RB + n], t[n], s);
-        sd = fma(a.coef[mu * RB + n], dt[n], sd);
+        s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
+        sd = fma(SUS2_COEF(a, mu * RB + n), dt[n], sd);
       }
       R[mu] = f * s;
       dR[mu] = df * s + f * half_scal * dxi * sd;

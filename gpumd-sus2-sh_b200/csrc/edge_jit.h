@@ -1,8 +1,12 @@
 // Per-edge kernels (k_basic, k_force of edge_kernels.cuh) compiled with NVRTC
-// for sm_100a when the model is loaded, for any shape the model format allows
-// (sh_l_max <= 6, radial_funcs_count <= 48, radial_basis_size <= 16).  The
-// ahead-of-time library covers the common shapes; this covers the rest with
-// the same kernel templates, so every model the reference loads runs.
+// for sm_100a when the model is loaded:
+//  * for any shape the model format allows (sh_l_max <= 6, radial_funcs_count
+//    <= 48, radial_basis_size <= 16): the ahead-of-time library covers the
+//    common shapes, this covers the rest with the same kernel templates, so
+//    every model the reference loads runs;
+//  * specialised to one FP32 model: the radial coefficients and their
+//    derivative series compiled in, so each is an immediate operand of its
+//    multiply-add instead of a constant load per edge.
 #pragma once
 
 #include <memory>
@@ -12,11 +16,15 @@
 namespace sus2sh {
 
 struct EdgeJitBinary {
-  std::vector<char> cubin;
-  std::string basic_name, force_name;  // lowered (mangled) kernel names
-  std::string basic_gate_name, force_gate_name;  // GATE variants (gate models only)
-  std::string log;                     // NVRTC + ptxas report
-  int basic_registers = -1, force_registers = -1;
+  std::vector<std::vector<char>> cubins;              // one per NVRTC program
+  std::vector<int> blocks;                            // CTA sizes compiled
+  std::vector<std::string> basic_names, force_names;  // lowered (mangled) names, one per CTA size
+  std::vector<int> basic_cubin, force_cubin;          // the cubin holding each of them
+  std::string basic_gate_name, force_gate_name;       // GATE variants (gate models only, 128 threads, cubin 0)
+  std::string log;                                    // NVRTC + ptxas report
+  int basic_registers = -1, force_registers = -1;     // of the first CTA size
+  long long global_bytes = -1;                        // module data in global memory ("bytes gmem")
+  bool model_coef = false;                            // coefficients compiled in
   double compile_ms = 0.0;
 };
 
@@ -26,6 +34,16 @@ struct EdgeJitBinary {
 std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block,
                                                           bool gate);
 
+// FP32 k_basic / k_force of one model at 64, 128 and 256 threads per CTA,
+// with `coef` (the kernels' coefficient table: c[mu][n], then the derivative
+// series when it fits, as EdgeArgs::coef holds them), whether the radial
+// functions of a pair share one argument, and the radial map compiled in:
+// six NVRTC programs built on parallel host threads.  Cached per process by
+// shape, table and radial setup.
+std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k_max, int rb,
+                                                                const std::vector<float>& coef, bool shared_xi,
+                                                                bool rational);
+
 // Module of one compiled shape, loaded into the current context.
 class EdgeJitModule {
  public:
@@ -34,8 +52,9 @@ class EdgeJitModule {
   EdgeJitModule(const EdgeJitModule&) = delete;
   EdgeJitModule& operator=(const EdgeJitModule&) = delete;
   bool load(const EdgeJitBinary& bin, std::string* err);
-  bool loaded() const { return basic_ != nullptr; }
-  // args: pointer to the host EdgeArgs<T> passed by value to the kernel.
+  bool loaded() const { return !modules_.empty(); }
+  // args: pointer to the host EdgeArgs<T> passed by value to the kernel;
+  // block: a CTA size the binary was compiled for (gate variants: 128).
   bool launch_basic(void* stream, int N, int block, size_t smem, const void* args, void* B, bool gate,
                     std::string* err);
   bool launch_force(void* stream, int N, int block, size_t smem, const void* args, const void* G,
@@ -43,14 +62,17 @@ class EdgeJitModule {
                     std::string* err);
 
  private:
-  bool set_smem(void* fn, size_t smem, int* have, std::string* err);
-  void* module_ = nullptr;
-  void* basic_ = nullptr;
-  void* force_ = nullptr;
-  void* basic_gate_ = nullptr;
-  void* force_gate_ = nullptr;
-  int basic_smem_ = 48 * 1024, force_smem_ = 48 * 1024, basic_gate_smem_ = 48 * 1024,
-      force_gate_smem_ = 48 * 1024;
+  struct Fn {
+    void* fn = nullptr;
+    int smem = 48 * 1024;  // dynamic shared memory the function is opted into
+  };
+  Fn* find(bool force, bool gate, int block);
+  bool set_smem(Fn& f, size_t smem, std::string* err);
+  bool launch(Fn* f, const char* what, void* stream, int N, int block, size_t smem, void** params, std::string* err);
+  std::vector<void*> modules_;
+  std::vector<int> blocks_;
+  std::vector<Fn> basic_, force_;
+  Fn basic_gate_, force_gate_;
 };
 
 }  // namespace sus2sh

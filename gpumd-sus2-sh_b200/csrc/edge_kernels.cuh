@@ -185,9 +185,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
     const T ps = row[2 * KMU];
     const T f = ps * e.dr * e.dr;
     const T df = T(2) * ps * e.dr;
-    const bool rational = a.rs.rational != 0;
+    const bool rational = SUS2_RATIONAL(a);
     T t[RB], fac = T(1);
-    if (a.rs.shared_xi) {
+    if (SUS2_SHARED_XI(a)) {
       const T half_scal = T(0.5) * row[0];
       T xi, dxi;
       radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
       for (int k = 0; k < K; ++k) {
         const int mu = k * (L + 1) + l;
         T scale = T(1);
-        if (!a.rs.shared_xi) {
+        if (!SUS2_SHARED_XI(a)) {
           const T half_scal = T(0.5) * row[2 * mu];
           T xi, dxi;
           radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi, dxi);
@@ -219,16 +219,16 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
           // derivative series stored after the coefficients
 #pragma unroll
           for (int n = 0; n < RB; ++n) {
-            v = fma(a.coef[mu * RB + n], t[n], v);
-            if (n + 1 < RB) d = fma(a.coef[KMU * RB + mu * RB + n], t[n], d);
+            v = fma(SUS2_COEF(a, mu * RB + n), t[n], v);
+            if (n + 1 < RB) d = fma(SUS2_COEF(a, KMU * RB + mu * RB + n), t[n], d);
           }
         } else {
           T tt[RB], dt[RB];
           chebyshev_d<RB>(t[RB > 1 ? 1 : 0], tt, dt);
 #pragma unroll
           for (int n = 0; n < RB; ++n) {
-            v = fma(a.coef[mu * RB + n], t[n], v);
-            d = fma(a.coef[mu * RB + n], dt[n], d);
+            v = fma(SUS2_COEF(a, mu * RB + n), t[n], v);
+            d = fma(SUS2_COEF(a, mu * RB + n), dt[n], d);
           }
         }
         sk[k] = v;

@@ -139,6 +139,8 @@ struct Options {
   bool autotune = true;             // sus2_sh_autotune=0 keeps 128-thread edge-kernel CTAs
   bool edge_jit = false;            // sus2_sh_edge_jit=1 compiles the edge kernels at load even
                                     // for a shape built ahead of time
+  bool model_edges = true;          // sus2_sh_model_edges=0 keeps the FP32 edge kernels that read
+                                    // the radial coefficients from their parameters
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

@@ -18,6 +18,7 @@ EXPORTS = (
     "sus2sh_write_synthetic_model", "sus2sh_standard_graph_counts", "sus2sh_md_kick_drift",
     "sus2sh_md_kick", "sus2sh_reduce", "sus2sh_random_insertion", "sus2sh_measure_fma_peak",
     "sus2sh_cg_kernel_info", "sus2sh_zbl_pair", "sus2sh_real_sh", "sus2sh_edge_kernel_info",
+    "sus2sh_model_edge_kernel_info",
 )
 
 _lib = None
@@ -59,6 +60,7 @@ def load() -> ctypes.CDLL:
         "sus2sh_zbl_pair": (I, [I, I, D, D, D, P, P]),
         "sus2sh_real_sh": (I, [I, D, D, D, P, P, P]),
         "sus2sh_edge_kernel_info": (I, [I, I, I, I, P, P, P, ctypes.c_char_p, ctypes.c_size_t]),
+        "sus2sh_model_edge_kernel_info": (I, [S, P, ctypes.c_char_p, ctypes.c_size_t]),
         "sus2sh_write_synthetic_model": (I, [S, I, I, I, I, P, I, I, D, D, I, P, D, D, D, D,
                                              ctypes.c_ulonglong]),
         "sus2sh_standard_graph_counts": (I, [I, I, I, P, I, P]),

@@ -181,8 +181,11 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * [23] its NVRTC compile time (ms) [24] CTA size of the basic-moment kernel
  * [25] CTA size of the force kernel (both picked by the tile autotuner at the
  * first evaluation; option sus2_sh_autotune=0 keeps 128) [26] edge kernels
- * compiled with NVRTC at load (shape without an ahead-of-time build, or
- * sus2_sh_edge_jit=1) [27] [28] their registers per thread (basic, force)
+ * compiled with NVRTC at load: 0 no (ahead-of-time build), 1 for the shape
+ * (shape without an ahead-of-time build, FP64 or gate model; or
+ * sus2_sh_edge_jit=1), 2 specialised to the model's radial coefficients (FP32
+ * non-gate models; sus2_sh_model_edges=0 turns it off) [27] [28] their
+ * registers per thread (basic, force; first CTA size)
  * [29] their compile time (ms) [30] two-layer gate mode (0 none,
  * 1 mu-body-linear-combo, 2 mu-scalar-full) [31] CG kernel kind (0 row
  * interpreter, 1 one straight-line function, 2 component-split) [32] [33]

@@ -65,6 +65,17 @@ int sus2sh_cg_kernel_info(const char* path, int use_float, int split, int* info,
 int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_registers, int* force_registers,
                             double* compile_ms, char* log, size_t log_len);
 
+/* Compiles, as FP32 model load does (option sus2_sh_model_edges, on by
+ * default), the per-edge kernels specialised to the radial coefficients of a
+ * model file (k_basic, k_force at 64, 128 and 256 threads per CTA; each
+ * coefficient and derivative-series coefficient an immediate operand).
+ * info[0] k_basic and [1] k_force registers per thread (64-thread CTAs),
+ * [2] compile ms, [3] bytes of module data in global memory (as for the
+ * shape's build without the table: every coefficient folded into the
+ * instructions), [4] coefficient-table entries, [5] cubin bytes.  log (if not NULL) receives the ptxas report.  Needs no
+ * GPU.  No reference counterpart. */
+int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t log_len);
+
 /* The engine's real spherical harmonics, evaluated on the host in FP64: Y at
  * the unit vector (x, y, z) for every l <= l_max (l_max <= 6, flat index
  * l*l + l + m) and, when G and V are non-NULL, V = sum_lm G[lm] grad P_lm

@@ -2,7 +2,8 @@
 on the reference's solid-harmonic path, and uncommon (L, K, rb) shapes): the
 edge kernels come from NVRTC at load, the results must match the FP64 oracle
 like the precompiled shapes do.  Forcing the NVRTC build on a precompiled
-shape must reproduce the ahead-of-time kernels."""
+shape must reproduce the ahead-of-time kernels, and so must the FP32 build
+specialised to a model's radial coefficients (the default for FP32 models)."""
 import ctypes
 import os
 
@@ -51,7 +52,8 @@ def test_nvrtc_shapes_match_oracle(model_dir, name, fp64):
     box, types, pos = structures.fcc(4, 4, 4, 3.8, (0.5, 0.5), 0.1, seed=70)
     pot = SUS2_SH(path, types.size, ["Cu", "Zr"] + (["sus2_float=0"] if fp64 else []))
     info = pot.info()
-    assert info["edge_jit"] == 1 and info["edge_jit_force_registers"] > 0
+    # FP32: the build specialised to the model; FP64: the build of the shape
+    assert info["edge_jit"] == (1 if fp64 else 2) and info["edge_jit_force_registers"] > 0
     pe, f, w = _efs(pot, box, types, pos)
     pot.close()
     pe0, f0, w0 = O.Oracle(path).efs(box.cpu_h, box.pbc, types, pos)
@@ -68,7 +70,7 @@ def test_nvrtc_shapes_match_oracle(model_dir, name, fp64):
 @pytest.mark.parametrize("fp64", [False, True])
 def test_forced_nvrtc_build_reproduces_precompiled_kernels(l3k3_path, fp64):
     box, types, pos = structures.fcc(5, 5, 5, 3.8, (0.5, 0.5), 0.1, seed=71)
-    opts = ["Cu", "Zr", "sus2_sh_autotune=0"] + (["sus2_float=0"] if fp64 else [])
+    opts = ["Cu", "Zr", "sus2_sh_autotune=0", "sus2_sh_model_edges=0"] + (["sus2_float=0"] if fp64 else [])
     a = SUS2_SH(l3k3_path, types.size, opts)
     assert a.info()["edge_jit"] == 0
     ra = _efs(a, box, types, pos)
@@ -80,6 +82,39 @@ def test_forced_nvrtc_build_reproduces_precompiled_kernels(l3k3_path, fp64):
     tol = 1e-12 if fp64 else 1e-6
     for x, y in zip(ra, rb):
         assert np.abs(x - y).max() <= tol * max(1.0, np.abs(x).max())
+
+
+@pytest.mark.parametrize("autotune", [0, 1])
+def test_model_specialised_kernels_reproduce_parameter_kernels(l3k3_path, autotune):
+    # the same FP32 arithmetic with each radial coefficient an immediate
+    # operand instead of a kernel-parameter load; with the tile autotuner on,
+    # every CTA size of the specialised build may be picked
+    box, types, pos = structures.fcc(6, 6, 6, 3.8, (0.64, 0.36), 0.08, seed=74)
+    opts = ["Cu", "Zr", f"sus2_sh_autotune={autotune}"]
+    a = SUS2_SH(l3k3_path, types.size, opts + ["sus2_sh_model_edges=0"])
+    ra = _efs(a, box, types, pos)
+    assert a.info()["edge_jit"] == 0
+    a.close()
+    b = SUS2_SH(l3k3_path, types.size, opts)
+    rb = _efs(b, box, types, pos)
+    info = b.info()
+    b.close()
+    assert info["edge_jit"] == 2 and info["force_block"] in (64, 128, 256)
+    for x, y in zip(ra, rb):
+        assert np.abs(x - y).max() <= 1e-6 * max(1.0, np.abs(x).max())
+
+
+def test_model_specialised_kernels_large_model(l4k4_path):
+    # L=4 K=4 rb=10 rational three-species model through the specialised build
+    box, types, pos = structures.random_insertion(400, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=75)
+    pot = SUS2_SH(l4k4_path, types.size, ["Cu", "Zr", "Al"])
+    assert pot.info()["edge_jit"] == 2
+    pe, f, w = _efs(pot, box, types, pos)
+    pot.close()
+    pe0, f0, w0 = O.Oracle(l4k4_path).efs(box.cpu_h, box.pbc, types, pos)
+    assert np.abs(pe - pe0).max() < 5e-6 * max(1.0, np.abs(pe0).max())
+    assert np.sqrt(((f - f0) ** 2).mean()) < 1e-5 * max(1.0, np.sqrt((f0 ** 2).mean()))
+    assert np.sqrt(((w - w0) ** 2).mean()) < 1e-5 * max(1.0, np.sqrt((w0 ** 2).mean()))
 
 
 def test_nvrtc_shape_in_a_batch_of_cells(model_dir):

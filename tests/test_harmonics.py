@@ -84,6 +84,30 @@ def test_edge_kernels_compile_with_nvrtc(shape):
     assert "sm_100a" in log.value.decode()
 
 
+@pytest.mark.parametrize("name", ["l3k3", "l4k4"])
+def test_model_specialised_edge_kernels_fold_the_coefficients(model_dir, name):
+    # the FP32 edge kernels built for one model: every radial coefficient
+    # (and derivative-series coefficient) becomes an instruction operand, so
+    # the module holds no table in memory and the registers stay within the
+    # caps of the parameter-reading build
+    from sus2sh import models
+    lib = _lib.load()
+    path = models.preset_model(name, model_dir)
+    info = (ctypes.c_int * 6)()
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = lib.sus2sh_model_edge_kernel_info(path.encode(), ctypes.cast(info, ctypes.c_void_p), log, 1 << 16)
+    assert rc == 0, lib.sus2sh_last_error().decode()
+    basic_regs, force_regs, ms, gmem, entries, cubin = list(info)
+    kmu_rb = {"l3k3": 12 * 8, "l4k4": 20 * 10}[name]
+    assert entries == 2 * kmu_rb  # coefficients, then the derivative series
+    assert 0 <= gmem < 4 * entries  # no table in global memory
+    assert 0 < basic_regs <= 255 and 0 < force_regs <= 255
+    if name == "l3k3":
+        assert basic_regs <= 128 and force_regs <= 128
+    assert log.value.decode().count("Compiling entry function") == 6
+    assert cubin > 0
+
+
 def test_edge_kernel_shape_limits():
     lib = _lib.load()
     assert lib.sus2sh_edge_kernel_info(1, 7, 1, 8, None, None, None, None, 0) != 0
