@@ -134,9 +134,10 @@ def edges_within(box, pos, rc):
 
 # DRAM bytes of one k_force launch (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the 524,288-atom l3k3 case (64x64x32 FCC cells, FP32,
-# 64-thread CTAs, walking the in-cutoff sub-list): 267.18 MB read + 40.97 MB
-# written.  The traffic grows with the atom count, so the bench scales it per atom.
-K_FORCE_DRAM_BYTES_PER_ATOM = (267.18e6 + 40.97e6) / 524288
+# the build specialised to the model, 128-thread CTAs, walking the in-cutoff
+# sub-list): 267.20 MB read + 39.99 MB written.  The traffic grows with the atom
+# count, so the bench scales it per atom.
+K_FORCE_DRAM_BYTES_PER_ATOM = (267.20e6 + 39.99e6) / 524288
 
 
 def k_force_algorithmic_bytes(nbasic, cut_per_atom):
@@ -478,7 +479,10 @@ def main():
                 "accuracy": {"force_rms_fp32_vs_fp64_eV_per_A": frms, "max_abs_dE_per_atom_eV": de,
                              "abs_dE_total_per_atom_eV": de_total},
                 "stage_ms_per_step": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"},
-                "roofline": {"kernel": "k_force (adjoint force/virial)", "bound": "fp32",
+                "roofline": {"kernel": "k_force (adjoint force/virial; "
+                                       + {0: "ahead-of-time build", 1: "NVRTC build of the shape",
+                                          2: "NVRTC build specialised to the model"}.get(info["edge_jit"], "?")
+                                       + f", {info['force_block']}-thread CTAs)", "bound": "fp32",
                              "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                              "frac": achieved / fp32_peak if fp32_peak > 0 else None,
                              "traffic": K_FORCE_DRAM_BYTES_PER_ATOM * N,
