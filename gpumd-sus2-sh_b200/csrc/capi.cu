@@ -19,6 +19,7 @@
 #include <memory>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace sus2sh {
@@ -358,9 +359,12 @@ struct Engine {
   size_t prod_smem = 0;
   int prod_tile = 32;
   bool prod_global = false;
-  // host-buffer path
+  // host-buffer path: the site energies go to the host on a second stream
+  // while the forces are computed (created at the first such call)
   DevBuf<double> io_pos, io_pe, io_f, io_vir, io_red;
   DevBuf<int> io_type;
+  cudaStream_t io_side = nullptr;
+  cudaEvent_t io_pe_ready = nullptr, io_pe_copied = nullptr;
   // forward state
   int fwd_N = 0;
   // stage profiler (CUDA events on the caller's stream; the reference's
@@ -417,6 +421,12 @@ struct Engine {
   double cg_compile_ms = 0.0;
 
   ~Engine() {
+    if (io_side) {
+      cudaStreamSynchronize(io_side);
+      cudaStreamDestroy(io_side);
+      cudaEventDestroy(io_pe_ready);
+      cudaEventDestroy(io_pe_copied);
+    }
     if (h_geom) cudaFreeHost(h_geom);
     if (h_status) cudaFreeHost(h_status);
     for (auto& v : {&ev_used, &ev_free})
@@ -1129,15 +1139,21 @@ struct Engine {
     ck(cudaGetLastError(), "kernel launch");
   }
 
+  // One energy/force/virial evaluation.  between(s), when given, is called on
+  // the host between the energy and the force passes (the site energies are
+  // final on stream s from that point).
+  template <typename Between = std::nullptr_t>
   void compute(cudaStream_t s, int n, const double* h, const int* pbc, const int* type, const double* x,
-               double* pe, double* f, double* vir) {
+               double* pe, double* f, double* vir, Between between = nullptr) {
     EvSet* ev = ev_begin(s);
     prepare(s, n, h, pbc, type, x);
     if (use_float) {
       forward_impl<float>(s, pe, 0, ev);
+      if constexpr (!std::is_same_v<Between, std::nullptr_t>) between(s);
       backward_impl<float>(s, nullptr, f, vir, 1.0, ev);
     } else {
       forward_impl<double>(s, pe, 0, ev);
+      if constexpr (!std::is_same_v<Between, std::nullptr_t>) between(s);
       backward_impl<double>(s, nullptr, f, vir, 1.0, ev);
     }
     finish(s);
@@ -1382,11 +1398,22 @@ int sus2sh_compute_host(sus2sh_handle* h, int N, const double box_h[9], const in
     ck(cudaMemsetAsync(e.io_pe.p, 0, sizeof(double) * N, s), "memset");
     ck(cudaMemsetAsync(e.io_f.p, 0, sizeof(double) * 3 * N, s), "memset");
     ck(cudaMemsetAsync(e.io_vir.p, 0, sizeof(double) * 9 * N, s), "memset");
-    e.compute(s, N, box_h, pbc, e.io_type.p, e.io_pos.p, e.io_pe.p, e.io_f.p, e.io_vir.p);
+    if (!e.io_side) {
+      ck(cudaStreamCreateWithFlags(&e.io_side, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreateWithFlags(&e.io_pe_ready, cudaEventDisableTiming), "cudaEventCreate");
+      ck(cudaEventCreateWithFlags(&e.io_pe_copied, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    // the site energies leave on the side stream while the force pass runs
+    e.compute(s, N, box_h, pbc, e.io_type.p, e.io_pos.p, e.io_pe.p, e.io_f.p, e.io_vir.p, [&](cudaStream_t cs) {
+      ck(cudaEventRecord(e.io_pe_ready, cs), "cudaEventRecord");
+      ck(cudaStreamWaitEvent(e.io_side, e.io_pe_ready, 0), "cudaStreamWaitEvent");
+      ck(cudaMemcpyAsync(potential, e.io_pe.p, sizeof(double) * N, cudaMemcpyDeviceToHost, e.io_side), "D2H");
+      ck(cudaEventRecord(e.io_pe_copied, e.io_side), "cudaEventRecord");
+    });
     sus2sh::launch_reduce(s, N, e.io_pe.p, e.io_vir.p, e.io_red.p);
     e.launches += 1;
-    ck(cudaMemcpyAsync(potential, e.io_pe.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s), "D2H");
     ck(cudaMemcpyAsync(force, e.io_f.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s), "D2H");
+    ck(cudaStreamWaitEvent(s, e.io_pe_copied, 0), "cudaStreamWaitEvent");
     if (virial_total) {
       double red[10];
       ck(cudaMemcpyAsync(red, e.io_red.p, sizeof(red), cudaMemcpyDeviceToHost, s), "D2H");
