@@ -297,6 +297,8 @@ int make_geometry(const double* h, const int* pbc, double cutoff, int N, BoxGeom
       throw InputError("SUS2_SH periodic box is thinner than half the neighbour cutoff (rc + skin).");
     g.reach[d] = r;
   }
+  for (int r = 0; r < 3; ++r)
+    for (int d = 0; d < 3; ++d) g.cellvec[3 * r + d] = h[3 * r + d] / g.ncell[d];
   for (int tx = -2; tx <= 2; ++tx)
     for (int ty = -2; ty <= 2; ++ty)
       for (int tz = -2; tz <= 2; ++tz) {
@@ -343,6 +345,7 @@ struct Engine {
   int calls_since_build = 0;
   DevBuf<double4> pos4, ref4;
   DevBuf<int> nbr, ncount, cell_count, cell_start, cell_atoms, atom_cell, atom_rank;
+  DevBuf<float4> cell_rel;  // positions in cell_atoms order, relative to their cell's corner (FP32)
   // in-cutoff sub-list of the current positions, written by the basic-moment
   // kernel and walked by the force kernel (cut_valid: written since the last
   // change of positions or list)
@@ -634,6 +637,7 @@ struct Engine {
     atom_cell.resize(N);
     atom_rank.resize(N);
     cell_atoms.resize(N);
+    cell_rel.resize(N);
     Bbuf.resize(nb * N * elem());
     Gbuf.resize(nb * N * elem());
     ftmp.resize(static_cast<size_t>(N) * (use_float ? sizeof(float4) : sizeof(double4)));
@@ -860,7 +864,7 @@ struct Engine {
       // first build: count pass, size the list, then fill
       ck(cudaMemsetAsync(&d_status.p->max_count, 0, sizeof(int), s), "memset");
       launch_build(s, N, 1, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p, cell_start.p,
-                   cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nullptr, ncount.p, 0, 1, d_status.p);
+                   cell_atoms.p, cell_rel.p, atom_cell.p, atom_rank.p, ncells, nullptr, ncount.p, 0, 1, d_status.p);
       launches += 8;
       Status st{};
       ck(cudaMemcpyAsync(&st, d_status.p, sizeof(Status), cudaMemcpyDeviceToHost, s), "status");
@@ -871,7 +875,7 @@ struct Engine {
     const bool use_inner = opt.skin > kInnerMargin;
     const double inner = model.rc + kInnerMargin;
     launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
-                 cell_start.p, cell_atoms.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
+                 cell_start.p, cell_atoms.p, cell_rel.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
                  d_status.p);
     launches += 8;
     inner_valid = false;

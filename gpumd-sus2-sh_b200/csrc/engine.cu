@@ -191,10 +191,30 @@ __global__ void k_scatter(int N, const Status* __restrict__ st, const int* __res
   cell_atoms[start[atom_cell[i]] + atom_rank[i]] = i;
 }
 
+// Cartesian corner h (cx/ncx, cy/ncy, cz/ncz) of cell (cx, cy, cz); for
+// indices outside [0, n) it is the corner of that cell's periodic image.
+__device__ __forceinline__ void cell_corner(const BoxGeom* __restrict__ g, int cx, int cy, int cz, double& ox,
+                                            double& oy, double& oz) {
+  const double* v = g->cellvec;
+  ox = v[0] * cx + v[1] * cy + v[2] * cz;
+  oy = v[3] * cx + v[4] * cy + v[5] * cz;
+  oz = v[6] * cx + v[7] * cy + v[8] * cz;
+}
+
+// Largest coordinate (A) of an FP32 position relative to its cell corner, and
+// of a cell-to-cell offset, for which the fill's FP32 distance test is used;
+// beyond them it takes the FP64 test.
+constexpr float kRelLimit = 64.0f;
+constexpr double kOffLimit = 256.0;
+
 // Sort each cell's atoms by index so the neighbour order (and every FP sum)
-// is deterministic.
-__global__ void k_sort_cells(int ncells, const Status* __restrict__ st, const int* __restrict__ start,
-                             int* __restrict__ cell_atoms) {
+// is deterministic, and store their positions in that order relative to the
+// cell's corner in FP32 (w = 1 when a coordinate exceeds kRelLimit: such an
+// atom always gets the FP64 test), so the fill reads each cell's candidates
+// contiguously, 16 bytes each.
+__global__ void k_sort_cells(int ncells, const Status* __restrict__ st, const BoxGeom* __restrict__ g,
+                             const int* __restrict__ start, int* __restrict__ cell_atoms,
+                             const double4* __restrict__ ref4, float4* __restrict__ cell_rel) {
   if (!st->rebuilt) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
@@ -208,14 +228,44 @@ __global__ void k_sort_cells(int ncells, const Status* __restrict__ st, const in
     }
     cell_atoms[k + 1] = v;
   }
+  double ox, oy, oz;
+  cell_corner(g, c % g->ncell[0], (c / g->ncell[0]) % g->ncell[1], c / (g->ncell[0] * g->ncell[1]), ox, oy, oz);
+  for (int a = b; a < e; ++a) {
+    const double4 q = ref4[cell_atoms[a]];
+    const float x = static_cast<float>(q.x - ox), y = static_cast<float>(q.y - oy), z = static_cast<float>(q.z - oz);
+    const bool far = !(fabsf(x) <= kRelLimit && fabsf(y) <= kRelLimit && fabsf(z) <= kRelLimit);
+    cell_rel[a] = make_float4(x, y, z, far ? 1.0f : 0.0f);
+  }
 }
 
+// Candidates are classified by an FP32 distance between cell-relative
+// positions (cell_rel) plus the FP64 cell-to-cell offset h (ox/ncx, oy/ncy,
+// oz/ncz) rounded to FP32: below cutoff2 - margin they are in, above
+// cutoff2 + margin out, and in between (or for atoms or offsets beyond the FP32
+// limits) the FP64 test on the full positions decides, exactly as the
+// distance test of the list has always been taken.  The margin is many times
+// the FP32 rounding bound of these short coordinates, so the list (and its
+// order) is the one the FP64 test alone gives.  An accepted candidate's
+// index is loaded only then.
 __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict__ g,
                        double cutoff2, const double4* __restrict__ ref4,
                        const int* __restrict__ start, const int* __restrict__ cell_atoms,
-                       const int* __restrict__ atom_cell, int* __restrict__ nbr,
-                       int* __restrict__ ncount, double4* __restrict__ pos4, int cap, int count_only) {
+                       const float4* __restrict__ cell_rel, const int* __restrict__ atom_cell,
+                       int* __restrict__ nbr, int* __restrict__ ncount, double4* __restrict__ pos4, int cap,
+                       int count_only) {
   if (!st->rebuilt) return;
+  // offsets of the (image) corners of the scanned cells from the home corner,
+  // cellvec (ox, oy, oz) in FP32 (w = 1 beyond kOffLimit), once per CTA
+  __shared__ float4 s_off[125];
+  const int rx = g->reach[0], ry = g->reach[1], rz = g->reach[2];
+  const int wx = 2 * rx + 1, wy = 2 * ry + 1;
+  for (int t = threadIdx.x; t < wx * wy * (2 * rz + 1); t += blockDim.x) {
+    double x, y, z;
+    cell_corner(g, t % wx - rx, (t / wx) % wy - ry, t / (wx * wy) - rz, x, y, z);
+    const bool far = !(fabs(x) <= kOffLimit && fabs(y) <= kOffLimit && fabs(z) <= kOffLimit);
+    s_off[t] = make_float4(static_cast<float>(x), static_cast<float>(y), static_cast<float>(z), far ? 1.0f : 0.0f);
+  }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const double4 p = ref4[i];
@@ -223,6 +273,12 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
   const int cx = cell % g->ncell[0];
   const int cy = (cell / g->ncell[0]) % g->ncell[1];
   const int cz = cell / (g->ncell[0] * g->ncell[1]);
+  double hx, hy, hz;
+  cell_corner(g, cx, cy, cz, hx, hy, hz);
+  const float px = static_cast<float>(p.x - hx), py = static_cast<float>(p.y - hy), pz = static_cast<float>(p.z - hz);
+  const bool far_i = !(fabsf(px) <= kRelLimit && fabsf(py) <= kRelLimit && fabsf(pz) <= kRelLimit);
+  const double margin = 0.01 + 1e-3 * cutoff2;
+  const float lo = static_cast<float>(cutoff2 - margin), hi = static_cast<float>(cutoff2 + margin);
   int k = 0;
   for (int oz = -g->reach[2]; oz <= g->reach[2]; ++oz) {
     int nz = cz + oz, tz = 0;
@@ -252,15 +308,24 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
         const double sx = g->shift[code][0], sy = g->shift[code][1], sz = g->shift[code][2];
         const int nc = (nz * g->ncell[1] + ny) * g->ncell[0] + nx;
         const int a1 = start[nc + 1];
+        const float4 off = s_off[((oz + rz) * wy + (oy + ry)) * wx + (ox + rx)];
+        const bool exact_cell = far_i || off.w != 0.0f;
+        const float fx = off.x - px, fy = off.y - py, fz = off.z - pz;
         for (int a = start[nc]; a < a1; ++a) {
+          const float4 q = cell_rel[a];
+          const float dx = q.x + fx, dy = q.y + fy, dz = q.z + fz;
+          const float d2 = dx * dx + dy * dy + dz * dz;
+          const bool exact = exact_cell || q.w != 0.0f;
+          if (!exact && !(d2 < hi)) continue;  // (a NaN distance goes on to the FP64 test, which rejects it)
           const int j = cell_atoms[a];
           if (j == i && code == kCenterCode) continue;
-          const double4 q = ref4[j];
-          const double dx = q.x - p.x + sx, dy = q.y - p.y + sy, dz = q.z - p.z + sz;
-          if (dx * dx + dy * dy + dz * dz < cutoff2) {
-            if (!count_only && k < cap) nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
-            ++k;
+          if (exact || !(d2 <= lo)) {
+            const double4 qq = ref4[j];
+            const double ex = qq.x - p.x + sx, ey = qq.y - p.y + sy, ez = qq.z - p.z + sz;
+            if (!(ex * ex + ey * ey + ez * ez < cutoff2)) continue;
           }
+          if (!count_only && k < cap) nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
+          ++k;
         }
       }
     }
@@ -593,8 +658,8 @@ void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const 
 
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
                   const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
-                  int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
-                  int cap, int count_only, Status* st) {
+                  int* cell_atoms, float4* cell_rel, int* atom_cell, int* atom_rank, int ncells, int* nbr,
+                  int* ncount, int cap, int count_only, Status* st) {
   (void)g;
   k_decide<<<1, 1, 0, s>>>(st, force, half_skin2);
   cudaMemsetAsync(cell_count, 0, sizeof(int) * (ncells + 1), s);
@@ -606,8 +671,8 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
   k_scan_top<<<1, kScanTile, 0, s>>>(st, nblocks, block_sums);
   k_scan_apply<<<nblocks, kScanTile, 0, s>>>(st, cell_count, ncells, block_sums, cell_start);
   k_scatter<<<blocks_for(N, 256), 256, 0, s>>>(N, st, cell_start, atom_cell, atom_rank, cell_atoms);
-  k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, cell_start, cell_atoms);
-  k_fill<<<blocks_for(N, 128), 128, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms,
+  k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, geom_dev, cell_start, cell_atoms, ref4, cell_rel);
+  k_fill<<<blocks_for(N, 128), 128, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms, cell_rel,
                                              atom_cell, nbr, ncount, pos4, cap, count_only);
 }
 

@@ -26,7 +26,8 @@ struct BoxGeom {
   double hinv[9];
   int pbc[3];
   int ncell[3];     // cells per fractional direction
-  int reach[3];     // cell offsets scanned per direction
+  int reach[3];     // cell offsets scanned per direction (1 or 2)
+  double cellvec[9];  // h with column d divided by ncell[d]: cell (cx,cy,cz)'s corner is cellvec (cx,cy,cz)
   double shift[125][3];  // Cartesian image vectors of codes (base 5, -2..2)
 };
 
@@ -107,8 +108,8 @@ void launch_inner(cudaStream_t s, int N, const Status* st, float half_margin2, d
                   int* inner_count);
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
                   const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
-                  int* cell_atoms, int* atom_cell, int* atom_rank, int ncells, int* nbr, int* ncount,
-                  int cap, int count_only, Status* st);
+                  int* cell_atoms, float4* cell_rel, int* atom_cell, int* atom_rank, int ncells, int* nbr,
+                  int* ncount, int cap, int count_only, Status* st);
 
 // Edge kernels with CTA size `block` (64, 128 or 256 for FP32; 128 for FP64);
 // gate = true selects the gate-model main-pass variants (128 only).
