@@ -147,9 +147,10 @@ __global__ void __launch_bounds__(128)
 
 // Orthorhombic cells, one CTA per cell: the cell's positions are staged in
 // shared memory (FP32, relative to its first atom) and every thread tests its
-// atom against them; per axis only the images that can come within the
-// cutoff are visited (computed from the displacement, at most `reach` each
-// way).  An FP32 pre-test with a 1e-3 A margin admits a superset of the pairs;
+// atom against them.  Cells wider than twice the cutoff take the nearest image
+// of each pair only (below); in narrower cells, per axis, only the images that
+// can come within the cutoff are visited (computed from the displacement, at
+// most `reach` each way).  An FP32 pre-test with a 1e-3 A margin admits a superset of the pairs;
 // each admitted pair gets the exact FP64 test of k_batch_fill, so the lists
 // (and their order: j ascending, then tz, ty, tx ascending) are the same.
 constexpr int kFillTile = 256;
@@ -170,6 +171,75 @@ __global__ void __launch_bounds__(128)
   const int r[3] = {cell_reach[3 * c], cell_reach[3 * c + 1], cell_reach[3 * c + 2]};
   const float cutm = static_cast<float>(sqrt(cutoff2)) + 1.0e-3f;
   const float cutm2 = cutm * cutm;
+  // Cells wider than twice the cutoff along every periodic axis: a pair has at
+  // most one image within the cutoff, the nearest (positions are wrapped into
+  // the cell, so it is -1, 0 or +1 cell away per axis).  Every candidate takes
+  // that image by rounding and is classified in FP32: below cutoff2 - m in,
+  // above cutoff2 + m out, in between the FP64 test below decides (m = 0.01 +
+  // 1e-3 cutoff2 A^2, far above the FP32 rounding of these cell-local
+  // coordinates).  The lists, j ascending, are the general path's.
+  bool wide = true;
+  for (int a = 0; a < 3; ++a)
+    if (r[a] > 0 && !(L[a] > 2.0f * cutm)) wide = false;
+  if (wide) {
+    const float jx = r[0] > 0 ? iL[0] : 0.0f, jy = r[1] > 0 ? iL[1] : 0.0f, jz = r[2] > 0 ? iL[2] : 0.0f;
+    const double margin = 0.01 + 1e-3 * cutoff2;
+    const float lo2 = static_cast<float>(cutoff2 - margin), hi2 = static_cast<float>(cutoff2 + margin);
+    for (int base = a0; base < a1; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      const bool act = i < a1;
+      double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
+      float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+      if (act) {
+        pi = pos4[i];
+        fx = static_cast<float>(pi.x - o.x);
+        fy = static_cast<float>(pi.y - o.y);
+        fz = static_cast<float>(pi.z - o.z);
+      }
+      int k = 0;
+      for (int t0 = a0; t0 < a1; t0 += kFillTile) {
+        const int tn = min(kFillTile, a1 - t0);
+        __syncthreads();  // the previous tile is consumed
+        for (int q = threadIdx.x; q < tn; q += blockDim.x) {
+          const double4 p = pos4[t0 + q];
+          sp[q] = make_float4(static_cast<float>(p.x - o.x), static_cast<float>(p.y - o.y),
+                              static_cast<float>(p.z - o.z), 0.0f);
+        }
+        __syncthreads();
+        if (!act) continue;
+#pragma unroll 4
+        for (int q = 0; q < tn; ++q) {
+          const float4 pj = sp[q];
+          const float dx = pj.x - fx, dy = pj.y - fy, dz = pj.z - fz;
+          const float tx = rintf(dx * jx), ty = rintf(dy * jy), tz = rintf(dz * jz);
+          const float ex = fmaf(-tx, L[0], dx), ey = fmaf(-ty, L[1], dy), ez = fmaf(-tz, L[2], dz);
+          const float m2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+          if (!(m2 < hi2)) continue;  // (a NaN goes on to the FP64 test, which rejects it)
+          const int j = t0 + q;
+          const int ix = -static_cast<int>(tx), iy = -static_cast<int>(ty), iz = -static_cast<int>(tz);
+          if (j == i && ix == 0 && iy == 0 && iz == 0) continue;
+          if (!(m2 <= lo2)) {
+            const double4 pjd = pos4[j];
+            const double gx = (pjd.x - pi.x) + ix * h[0] + iy * h[1] + iz * h[2];
+            const double gy = (pjd.y - pi.y) + ix * h[3] + iy * h[4] + iz * h[5];
+            const double gz = (pjd.z - pi.z) + ix * h[6] + iy * h[7] + iz * h[8];
+            if (!(gx * gx + gy * gy + gz * gz < cutoff2)) continue;
+          }
+          if (!count_only && k < cap) {
+            const int code = (ix + 2) * 25 + (iy + 2) * 5 + (iz + 2);
+            nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
+          }
+          ++k;
+        }
+      }
+      if (act) {
+        ncount[i] = k;
+        atomicMax(&st->max_count, k);
+        if (k > cap && !count_only) st->overflow = 1;
+      }
+    }
+    return;
+  }
   for (int base = a0; base < a1; base += blockDim.x) {
     const int i = base + threadIdx.x;
     const bool act = i < a1;
