@@ -105,6 +105,22 @@ def test_open_boundaries(l3k3_path):
     compare(l3k3_path, mixed, types, pos + np.array([[0.0], [20.0], [0.0]]))
 
 
+def test_atoms_far_outside_an_open_axis(l3k3_path):
+    # periodic x, y and open z with the box only 20 A high: clusters of the
+    # crystal sit up to 150 A below and above it, where the neighbour fill's
+    # cell-relative FP32 coordinates are large (tens of A) or beyond its FP32
+    # limit (FP64 test for every candidate); the list must be the FP64 one
+    box, types, pos = structures.fcc(3, 3, 2, 3.8, (0.5, 0.5), 0.05, seed=22)
+    n = types.size
+    shifts = np.array([-150.0, -60.0, 0.0, 45.0, 140.0])
+    pos_all = np.concatenate([pos + np.array([[0.0], [0.0], [dz]]) for dz in shifts], axis=1)
+    types_all = np.concatenate([types] * len(shifts))
+    obox = Box.orthorhombic(11.4, 11.4, 20.0, pbc=(1, 1, 0))
+    assert pos_all.shape[1] == n * len(shifts)
+    compare(l3k3_path, obox, types_all, pos_all)
+    compare(l3k3_path, obox, types_all, pos_all, fp64=True)
+
+
 def per_mu_radial_model(src, dst):
     """Copy of model ``src`` whose radial functions each get their own (scal,
     shift) per species pair, so no radial argument is shared between them
