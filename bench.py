@@ -135,9 +135,9 @@ def edges_within(box, pos, rc):
 # DRAM bytes of one k_force launch (dram__bytes_read.sum + dram__bytes_write.sum)
 # from one ncu capture of the 524,288-atom l3k3 case (64x64x32 FCC cells, FP32,
 # the build specialised to the model, 128-thread CTAs, walking the in-cutoff
-# sub-list): 267.20 MB read + 39.99 MB written.  The traffic grows with the atom
+# sub-list): 267.15 MB read + 39.17 MB written.  The traffic grows with the atom
 # count, so the bench scales it per atom.
-K_FORCE_DRAM_BYTES_PER_ATOM = (267.20e6 + 39.99e6) / 524288
+K_FORCE_DRAM_BYTES_PER_ATOM = (267.15e6 + 39.17e6) / 524288
 
 
 def k_force_algorithmic_bytes(nbasic, cut_per_atom):
