@@ -154,12 +154,15 @@ __global__ void __launch_bounds__(128)
 // each admitted pair gets the exact FP64 test of k_batch_fill, so the lists
 // (and their order: j ascending, then tz, ty, tx ascending) are the same.
 constexpr int kFillTile = 256;
+// per-thread queue of a tile's near candidates in the wide-cell path
+constexpr int kFillQueue = 96;
 
 __global__ void __launch_bounds__(128)
     k_batch_fill_ortho(int N, const int* __restrict__ off, const double4* __restrict__ pos4,
                        const double* __restrict__ cell_h, const int* __restrict__ cell_reach, double cutoff2,
                        int* __restrict__ nbr, int* __restrict__ ncount, int cap, int count_only, Status* st) {
   __shared__ float4 sp[kFillTile];
+  __shared__ unsigned short s_queue[kFillQueue][128];  // [slot][thread]: one CTA of 128 threads
   const int c = blockIdx.x;
   const double* h = cell_h + 9 * c;
   const bool ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
@@ -207,29 +210,61 @@ __global__ void __launch_bounds__(128)
         }
         __syncthreads();
         if (!act) continue;
-#pragma unroll 4
-        for (int q = 0; q < tn; ++q) {
+        // candidate q of the tile: nearest-image FP32 distance, and the full
+        // test and list write for one within hi2
+        auto dist2 = [&](int q, float& tx, float& ty, float& tz) {
           const float4 pj = sp[q];
           const float dx = pj.x - fx, dy = pj.y - fy, dz = pj.z - fz;
-          const float tx = rintf(dx * jx), ty = rintf(dy * jy), tz = rintf(dz * jz);
+          tx = rintf(dx * jx);
+          ty = rintf(dy * jy);
+          tz = rintf(dz * jz);
           const float ex = fmaf(-tx, L[0], dx), ey = fmaf(-ty, L[1], dy), ez = fmaf(-tz, L[2], dz);
-          const float m2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-          if (!(m2 < hi2)) continue;  // (a NaN goes on to the FP64 test, which rejects it)
+          return fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+        };
+        auto accept = [&](int q, float m2, float tx, float ty, float tz) {
           const int j = t0 + q;
           const int ix = -static_cast<int>(tx), iy = -static_cast<int>(ty), iz = -static_cast<int>(tz);
-          if (j == i && ix == 0 && iy == 0 && iz == 0) continue;
+          if (j == i && ix == 0 && iy == 0 && iz == 0) return;
           if (!(m2 <= lo2)) {
             const double4 pjd = pos4[j];
             const double gx = (pjd.x - pi.x) + ix * h[0] + iy * h[1] + iz * h[2];
             const double gy = (pjd.y - pi.y) + ix * h[3] + iy * h[4] + iz * h[5];
             const double gz = (pjd.z - pi.z) + ix * h[6] + iy * h[7] + iz * h[8];
-            if (!(gx * gx + gy * gy + gz * gz < cutoff2)) continue;
+            if (!(gx * gx + gy * gy + gz * gz < cutoff2)) return;
           }
           if (!count_only && k < cap) {
             const int code = (ix + 2) * 25 + (iy + 2) * 5 + (iz + 2);
             nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
           }
           ++k;
+        };
+        // two phases keep the lanes busy: a uniform scan queues the tile's
+        // candidates within hi2 (a fifth or so), then each thread tests and
+        // writes its queue; a queue that would overflow (never at physical
+        // densities) is replaced by a direct pass over the tile, same order
+        int nq = 0;
+#pragma unroll 4
+        for (int q = 0; q < tn; ++q) {
+          float tx, ty, tz;
+          const float m2 = dist2(q, tx, ty, tz);
+          if (m2 < hi2) {  // (a NaN distance is rejected, as the FP64 test would)
+            if (nq < kFillQueue) s_queue[nq][threadIdx.x] = static_cast<unsigned short>(q);
+            ++nq;
+          }
+        }
+        if (nq <= kFillQueue) {
+          for (int u = 0; u < nq; ++u) {
+            const int q = s_queue[u][threadIdx.x];
+            float tx, ty, tz;
+            const float m2 = dist2(q, tx, ty, tz);
+            accept(q, m2, tx, ty, tz);
+          }
+        } else {
+          for (int q = 0; q < tn; ++q) {
+            float tx, ty, tz;
+            const float m2 = dist2(q, tx, ty, tz);
+            if (m2 < hi2) accept(q, m2, tx, ty, tz);
+          }
         }
       }
       if (act) {
