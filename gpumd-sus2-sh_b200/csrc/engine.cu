@@ -206,6 +206,9 @@ __device__ __forceinline__ void cell_corner(const BoxGeom* __restrict__ g, int c
 // beyond them it takes the FP64 test.
 constexpr float kRelLimit = 64.0f;
 constexpr double kOffLimit = 256.0;
+// CTA size of the fill and its per-thread queue of one cell's near candidates
+constexpr int kFillBlock = 128;
+constexpr int kFillQueue = 32;
 
 // Sort each cell's atoms by index so the neighbour order (and every FP sum)
 // is deterministic, and store their positions in that order relative to the
@@ -257,6 +260,7 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
   // offsets of the (image) corners of the scanned cells from the home corner,
   // cellvec (ox, oy, oz) in FP32 (w = 1 beyond kOffLimit), once per CTA
   __shared__ float4 s_off[125];
+  __shared__ unsigned short s_queue[kFillQueue][kFillBlock];  // [slot][thread]
   const int rx = g->reach[0], ry = g->reach[1], rz = g->reach[2];
   const int wx = 2 * rx + 1, wy = 2 * ry + 1;
   for (int t = threadIdx.x; t < wx * wy * (2 * rz + 1); t += blockDim.x) {
@@ -311,21 +315,51 @@ __global__ void k_fill(int N, Status* __restrict__ st, const BoxGeom* __restrict
         const float4 off = s_off[((oz + rz) * wy + (oy + ry)) * wx + (ox + rx)];
         const bool exact_cell = far_i || off.w != 0.0f;
         const float fx = off.x - px, fy = off.y - py, fz = off.z - pz;
-        for (int a = start[nc]; a < a1; ++a) {
+        const int a0 = start[nc];
+        // candidate a: FP32 distance, and whether it needs the FP64 test
+        auto dist2 = [&](int a, bool& exact) {
           const float4 q = cell_rel[a];
           const float dx = q.x + fx, dy = q.y + fy, dz = q.z + fz;
-          const float d2 = dx * dx + dy * dy + dz * dz;
-          const bool exact = exact_cell || q.w != 0.0f;
-          if (!exact && !(d2 < hi)) continue;  // (a NaN distance goes on to the FP64 test, which rejects it)
+          exact = exact_cell || q.w != 0.0f;
+          return dx * dx + dy * dy + dz * dz;
+        };
+        auto accept = [&](int a, float d2, bool exact) {
           const int j = cell_atoms[a];
-          if (j == i && code == kCenterCode) continue;
+          if (j == i && code == kCenterCode) return;
           if (exact || !(d2 <= lo)) {
             const double4 qq = ref4[j];
             const double ex = qq.x - p.x + sx, ey = qq.y - p.y + sy, ez = qq.z - p.z + sz;
-            if (!(ex * ex + ey * ey + ez * ez < cutoff2)) continue;
+            if (!(ex * ex + ey * ey + ez * ez < cutoff2)) return;
           }
           if (!count_only && k < cap) nbr[static_cast<size_t>(k) * N + i] = j | (code << 24);
           ++k;
+        };
+        // a uniform scan queues the cell's candidates that may be in (about
+        // one in seven), then the accept work runs over the queue, so lanes do
+        // not idle on it; a queue that would overflow is replaced by a direct
+        // pass over the cell (same order)
+        int nq = 0;
+        for (int a = a0; a < a1; ++a) {
+          bool exact;
+          const float d2 = dist2(a, exact);
+          if (exact || d2 < hi) {  // (a NaN distance is rejected, as the FP64 test would)
+            if (nq < kFillQueue) s_queue[nq][threadIdx.x] = static_cast<unsigned short>(a - a0);
+            ++nq;
+          }
+        }
+        if (nq <= kFillQueue && a1 - a0 <= 65535) {
+          for (int u = 0; u < nq; ++u) {
+            const int a = a0 + s_queue[u][threadIdx.x];
+            bool exact;
+            const float d2 = dist2(a, exact);
+            accept(a, d2, exact);
+          }
+        } else {
+          for (int a = a0; a < a1; ++a) {
+            bool exact;
+            const float d2 = dist2(a, exact);
+            if (exact || d2 < hi) accept(a, d2, exact);
+          }
         }
       }
     }
@@ -672,8 +706,8 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
   k_scan_apply<<<nblocks, kScanTile, 0, s>>>(st, cell_count, ncells, block_sums, cell_start);
   k_scatter<<<blocks_for(N, 256), 256, 0, s>>>(N, st, cell_start, atom_cell, atom_rank, cell_atoms);
   k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, geom_dev, cell_start, cell_atoms, ref4, cell_rel);
-  k_fill<<<blocks_for(N, 128), 128, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms, cell_rel,
-                                             atom_cell, nbr, ncount, pos4, cap, count_only);
+  k_fill<<<blocks_for(N, kFillBlock), kFillBlock, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms,
+                                                           cell_rel, atom_cell, nbr, ncount, pos4, cap, count_only);
 }
 
 void launch_inner(cudaStream_t s, int N, const Status* st, float half_margin2, double inner2, const double4* pos4,
