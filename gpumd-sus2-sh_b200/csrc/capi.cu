@@ -346,6 +346,14 @@ struct Engine {
   DevBuf<double4> pos4, ref4;
   DevBuf<int> nbr, ncount, cell_count, cell_start, cell_atoms, atom_cell, atom_rank;
   DevBuf<float4> cell_rel;  // positions in cell_atoms order, relative to their cell's corner (FP32)
+  // the per-call neighbour work after the rebuild decision as one CUDA graph
+  // with IF nodes (rebuilt when a size or buffer it holds changes); off for
+  // good after any graph error, the plain launches then do the same work
+  bool nbr_graph_ok = true;
+  cudaStream_t nbr_capture = nullptr;
+  cudaGraph_t nbr_graph = nullptr;
+  cudaGraphExec_t nbr_exec = nullptr;
+  NeighborGraphArgs nbr_args;
   // in-cutoff sub-list of the current positions, written by the basic-moment
   // kernel and walked by the force kernel (cut_valid: written since the last
   // change of positions or list)
@@ -424,6 +432,9 @@ struct Engine {
   double cg_compile_ms = 0.0;
 
   ~Engine() {
+    if (nbr_exec) cudaGraphExecDestroy(nbr_exec);
+    if (nbr_graph) cudaGraphDestroy(nbr_graph);
+    if (nbr_capture) cudaStreamDestroy(nbr_capture);
     if (io_side) {
       cudaStreamSynchronize(io_side);
       cudaStreamDestroy(io_side);
@@ -874,17 +885,67 @@ struct Engine {
     }
     const bool use_inner = opt.skin > kInnerMargin;
     const double inner = model.rc + kInnerMargin;
-    launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
-                 cell_start.p, cell_atoms.p, cell_rel.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
-                 d_status.p);
-    launches += 8;
     inner_valid = false;
-    if (use_inner) {
-      launch_inner(s, N, d_status.p, static_cast<float>(0.25 * kInnerMargin * kInnerMargin), inner * inner, pos4.p,
-                   nbr.p, ncount.p, cap, d_geom.p, inner_nbr.p, inner_count.p);
-      launches += 1;
-      inner_valid = true;
+    const float half_margin2 = static_cast<float>(0.25 * kInnerMargin * kInnerMargin);
+    bool graphed = false;
+    // (a caller capturing this stream into its own graph gets the plain launches)
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &capturing) != cudaSuccess) capturing = cudaStreamCaptureStatusActive;
+    if (opt.neighbor_graph && nbr_graph_ok && capturing == cudaStreamCaptureStatusNone) {
+      NeighborGraphArgs g;
+      g.N = N;
+      g.ncells = ncells;
+      g.cap = cap;
+      g.use_inner = use_inner ? 1 : 0;
+      g.cutoff2 = cutoff2;
+      g.inner2 = inner * inner;
+      g.half_margin2 = half_margin2;
+      g.geom = d_geom.p;
+      g.pos4 = pos4.p;
+      g.ref4 = ref4.p;
+      g.cell_count = cell_count.p;
+      g.cell_start = cell_start.p;
+      g.cell_atoms = cell_atoms.p;
+      g.atom_cell = atom_cell.p;
+      g.atom_rank = atom_rank.p;
+      g.nbr = nbr.p;
+      g.ncount = ncount.p;
+      g.inner_nbr = inner_nbr.p;
+      g.inner_count = inner_count.p;
+      g.cell_rel = cell_rel.p;
+      g.st = d_status.p;
+      if (!nbr_exec || !(g == nbr_args)) {
+        if (nbr_exec) cudaGraphExecDestroy(nbr_exec);
+        if (nbr_graph) cudaGraphDestroy(nbr_graph);
+        nbr_exec = nullptr;
+        nbr_graph = nullptr;
+        if (!nbr_capture) ck(cudaStreamCreateWithFlags(&nbr_capture, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (build_neighbor_graph(nbr_capture, g, &nbr_graph, &nbr_exec) == cudaSuccess) {
+          nbr_args = g;
+        } else {
+          cudaGetLastError();  // the plain launches below do the same work
+          nbr_graph_ok = false;
+        }
+      }
+      if (nbr_exec) {
+        launch_decide(s, d_status.p, force ? 1 : 0, half_skin2);
+        ck(cudaGraphLaunch(nbr_exec, s), "neighbour graph launch");
+        launches += 2 + (force ? 8 : 0);  // k_decide, k_cond and, when the host forced a build, its kernels
+        graphed = true;
+      }
     }
+    if (!graphed) {
+      launch_build(s, N, force ? 1 : 0, half_skin2, cutoff2, geom, d_geom.p, pos4.p, ref4.p, cell_count.p,
+                   cell_start.p, cell_atoms.p, cell_rel.p, atom_cell.p, atom_rank.p, ncells, nbr.p, ncount.p, cap, 0,
+                   d_status.p);
+      launches += 8;
+      if (use_inner) {
+        launch_inner(s, N, d_status.p, half_margin2, inner * inner, pos4.p, nbr.p, ncount.p, cap, d_geom.p,
+                     inner_nbr.p, inner_count.p);
+        launches += 1;
+      }
+    }
+    if (use_inner) inner_valid = true;
     ck(cudaGetLastError(), "neighbour build launch");
     have_ref = true;
     force_next = false;

@@ -690,12 +690,23 @@ void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const 
   k_pack<<<blocks_for(N, 256), 256, 0, s>>>(N, x, type, ref4, pos4, geom_dev, have_ref, species, st);
 }
 
+void launch_decide(cudaStream_t s, Status* st, int force, float half_skin2) {
+  k_decide<<<1, 1, 0, s>>>(st, force, half_skin2);
+}
+
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
                   const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
                   int* cell_atoms, float4* cell_rel, int* atom_cell, int* atom_rank, int ncells, int* nbr,
                   int* ncount, int cap, int count_only, Status* st) {
   (void)g;
-  k_decide<<<1, 1, 0, s>>>(st, force, half_skin2);
+  launch_decide(s, st, force, half_skin2);
+  launch_rebuild(s, N, cutoff2, geom_dev, pos4, ref4, cell_count, cell_start, cell_atoms, cell_rel, atom_cell,
+                 atom_rank, ncells, nbr, ncount, cap, count_only, st);
+}
+
+void launch_rebuild(cudaStream_t s, int N, double cutoff2, const BoxGeom* geom_dev, double4* pos4, double4* ref4,
+                    int* cell_count, int* cell_start, int* cell_atoms, float4* cell_rel, int* atom_cell,
+                    int* atom_rank, int ncells, int* nbr, int* ncount, int cap, int count_only, Status* st) {
   cudaMemsetAsync(cell_count, 0, sizeof(int) * (ncells + 1), s);
   k_bin<<<blocks_for(N, 256), 256, 0, s>>>(N, st, geom_dev, pos4, ref4, cell_count, atom_cell, atom_rank);
   // block sums live in the spare tail of cell_count (sized by the caller)
@@ -708,6 +719,81 @@ void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cut
   k_sort_cells<<<blocks_for(ncells, 128), 128, 0, s>>>(ncells, st, geom_dev, cell_start, cell_atoms, ref4, cell_rel);
   k_fill<<<blocks_for(N, kFillBlock), kFillBlock, 0, s>>>(N, st, geom_dev, cutoff2, ref4, cell_start, cell_atoms,
                                                            cell_rel, atom_cell, nbr, ncount, pos4, cap, count_only);
+}
+
+// The IF conditions of the neighbour graph, from k_decide's decision: a build,
+// and a refresh of the inner list (at a build, or once an atom has moved more
+// than half the inner margin since it).
+__global__ void k_cond(const Status* __restrict__ st, float half_margin2, int use_inner,
+                       cudaGraphConditionalHandle build, cudaGraphConditionalHandle inner) {
+  const int b = st->rebuilt;
+  cudaGraphSetConditional(build, b ? 1u : 0u);
+  const bool refresh = use_inner && (b || __uint_as_float(st->maxdisp2_bits) > half_margin2);
+  cudaGraphSetConditional(inner, refresh ? 1u : 0u);
+}
+
+cudaError_t build_neighbor_graph(cudaStream_t capture, const NeighborGraphArgs& g, cudaGraph_t* graph_out,
+                                 cudaGraphExec_t* exec_out) {
+  *graph_out = nullptr;
+  *exec_out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaGraphCreate(&graph, 0);
+  if (e != cudaSuccess) return e;
+  auto fail = [&](cudaError_t err) {
+    cudaGraphDestroy(graph);
+    return err;
+  };
+  cudaGraphConditionalHandle hb, hi;
+  if ((e = cudaGraphConditionalHandleCreate(&hb, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) return fail(e);
+  if ((e = cudaGraphConditionalHandleCreate(&hi, graph, 0, cudaGraphCondAssignDefault)) != cudaSuccess) return fail(e);
+  // k_cond
+  const Status* st = g.st;
+  float half_margin2 = g.half_margin2;
+  int use_inner = g.use_inner;
+  void* cond_args[] = {&st, &half_margin2, &use_inner, &hb, &hi};
+  cudaKernelNodeParams kp = {};
+  kp.func = reinterpret_cast<void*>(k_cond);
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(1);
+  kp.kernelParams = cond_args;
+  cudaGraphNode_t ncond;
+  if ((e = cudaGraphAddKernelNode(&ncond, graph, nullptr, 0, &kp)) != cudaSuccess) return fail(e);
+  // IF build: the rebuild kernels, captured into the body graph
+  cudaGraphNodeParams cb = {};
+  cb.type = cudaGraphNodeTypeConditional;
+  cb.conditional.handle = hb;
+  cb.conditional.type = cudaGraphCondTypeIf;
+  cb.conditional.size = 1;
+  cudaGraphNode_t nbuild;
+  if ((e = cudaGraphAddNode(&nbuild, graph, &ncond, 1, &cb)) != cudaSuccess) return fail(e);
+  cudaGraph_t body = cb.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+      cudaSuccess)
+    return fail(e);
+  launch_rebuild(capture, g.N, g.cutoff2, g.geom, g.pos4, g.ref4, g.cell_count, g.cell_start, g.cell_atoms,
+                 g.cell_rel, g.atom_cell, g.atom_rank, g.ncells, g.nbr, g.ncount, g.cap, 0, g.st);
+  if ((e = cudaStreamEndCapture(capture, &body)) != cudaSuccess) return fail(e);
+  // IF inner refresh: k_inner
+  cudaGraphNodeParams ci = {};
+  ci.type = cudaGraphNodeTypeConditional;
+  ci.conditional.handle = hi;
+  ci.conditional.type = cudaGraphCondTypeIf;
+  ci.conditional.size = 1;
+  cudaGraphNode_t ninner;
+  if ((e = cudaGraphAddNode(&ninner, graph, &nbuild, 1, &ci)) != cudaSuccess) return fail(e);
+  cudaGraph_t ibody = ci.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(capture, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)) !=
+      cudaSuccess)
+    return fail(e);
+  if (g.use_inner)
+    launch_inner(capture, g.N, g.st, g.half_margin2, g.inner2, g.pos4, g.nbr, g.ncount, g.cap, g.geom, g.inner_nbr,
+                 g.inner_count);
+  if ((e = cudaStreamEndCapture(capture, &ibody)) != cudaSuccess) return fail(e);
+  cudaGraphExec_t exec = nullptr;
+  if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return fail(e);
+  *graph_out = graph;
+  *exec_out = exec;
+  return cudaSuccess;
 }
 
 void launch_inner(cudaStream_t s, int N, const Status* st, float half_margin2, double inner2, const double4* pos4,

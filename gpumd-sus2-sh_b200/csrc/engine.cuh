@@ -106,6 +106,42 @@ void launch_pack(cudaStream_t s, int N, const double* x, const int* type, const 
 void launch_inner(cudaStream_t s, int N, const Status* st, float half_margin2, double inner2, const double4* pos4,
                   const int* nbr, const int* ncount, int cap, const BoxGeom* geom_dev, int* inner_nbr,
                   int* inner_count);
+// The neighbour build in two parts: the rebuild decision (k_decide) and the
+// rebuild kernels (each returns at once when no rebuild was decided).
+void launch_decide(cudaStream_t s, Status* st, int force, float half_skin2);
+void launch_rebuild(cudaStream_t s, int N, double cutoff2, const BoxGeom* geom_dev, double4* pos4, double4* ref4,
+                    int* cell_count, int* cell_start, int* cell_atoms, float4* cell_rel, int* atom_cell,
+                    int* atom_rank, int ncells, int* nbr, int* ncount, int cap, int count_only, Status* st);
+
+// Everything the per-call neighbour work after the decision needs.
+struct NeighborGraphArgs {
+  int N = 0, ncells = 0, cap = 0, use_inner = 0;
+  double cutoff2 = 0.0, inner2 = 0.0;
+  float half_margin2 = 0.0f;
+  const BoxGeom* geom = nullptr;
+  double4 *pos4 = nullptr, *ref4 = nullptr;
+  int *cell_count = nullptr, *cell_start = nullptr, *cell_atoms = nullptr, *atom_cell = nullptr,
+      *atom_rank = nullptr, *nbr = nullptr, *ncount = nullptr, *inner_nbr = nullptr, *inner_count = nullptr;
+  float4* cell_rel = nullptr;
+  Status* st = nullptr;
+  bool operator==(const NeighborGraphArgs& o) const {
+    return N == o.N && ncells == o.ncells && cap == o.cap && use_inner == o.use_inner && cutoff2 == o.cutoff2 &&
+           inner2 == o.inner2 && half_margin2 == o.half_margin2 && geom == o.geom && pos4 == o.pos4 &&
+           ref4 == o.ref4 && cell_count == o.cell_count && cell_start == o.cell_start &&
+           cell_atoms == o.cell_atoms && atom_cell == o.atom_cell && atom_rank == o.atom_rank && nbr == o.nbr &&
+           ncount == o.ncount && inner_nbr == o.inner_nbr && inner_count == o.inner_count &&
+           cell_rel == o.cell_rel && st == o.st;
+  }
+};
+
+// The per-call neighbour work after launch_decide as one CUDA graph: a
+// one-thread kernel sets two IF conditions from the decision, so the rebuild
+// kernels run only when a build is due and k_inner only when the inner list
+// needs a refresh (a step without a rebuild launches neither).  The body
+// graphs are captured on `capture`.
+cudaError_t build_neighbor_graph(cudaStream_t capture, const NeighborGraphArgs& args, cudaGraph_t* graph,
+                                 cudaGraphExec_t* exec);
+
 void launch_build(cudaStream_t s, int N, int force, float half_skin2, double cutoff2, const BoxGeom& g,
                   const BoxGeom* geom_dev, double4* pos4, double4* ref4, int* cell_count, int* cell_start,
                   int* cell_atoms, float4* cell_rel, int* atom_cell, int* atom_rank, int ncells, int* nbr,

@@ -918,6 +918,8 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       o.edge_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_model_edges") {
       o.model_edges = parse_bool(val, key);
+    } else if (key == "sus2_sh_neighbor_graph") {
+      o.neighbor_graph = parse_bool(val, key);
     } else if (key == "sus2_sh_cg_jit") {
       o.cg_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_cg_split") {

@@ -141,6 +141,8 @@ struct Options {
                                     // for a shape built ahead of time
   bool model_edges = true;          // sus2_sh_model_edges=0 keeps the FP32 edge kernels that read
                                     // the radial coefficients from their parameters
+  bool neighbor_graph = true;       // sus2_sh_neighbor_graph=0 launches the neighbour-build kernels
+                                    // on every call instead of a graph that skips them
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

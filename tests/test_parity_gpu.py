@@ -256,6 +256,37 @@ def test_md_steps_with_skin_rebuilds(l3k3_path):
     assert np.sqrt(((md.force.view(3, -1).cpu().numpy() - f0) ** 2).mean()) < F_RMS32
 
 
+def test_neighbor_graph_matches_plain_launches(l3k3_path):
+    # the neighbour work after the rebuild decision as a CUDA graph with IF
+    # nodes (skipping the rebuild kernels on steps without a build) against
+    # the plain launches: the same energies for the same positions (bit for
+    # bit: no atomics in the energy), the same builds over a hot MD run, and the
+    # same end of the run within FP32 rounding (the F_j scatter's FP32 atomics
+    # add in a varying order, so two runs drift apart at the 1e-8 eV level)
+    from sus2sh.md import NVE
+    box, types, pos = structures.fcc(6, 6, 6, 3.8, (0.64, 0.36), 0.05, seed=10)
+    masses = [structures.AMU["Cu"], structures.AMU["Zr"]]
+    vel = structures.maxwell_boltzmann(types, masses, 2000.0, seed=11)
+    out = []
+    for graph in (1, 0):
+        pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr", "sus2_sh_rebuild_interval=7",
+                                              f"sus2_sh_neighbor_graph={graph}"])
+        md = NVE(pot, box, types, pos, vel, masses, dt_fs=2.0)
+        md.initial_force()
+        torch.cuda.synchronize()
+        pe0 = md.pe.cpu().numpy().copy()
+        for _ in range(30):
+            md.step()
+        torch.cuda.synchronize()
+        assert pot.sync() == 0
+        out.append((pe0, md.pe.cpu().numpy().copy(), md.force.cpu().numpy().copy(), pot.info()["neighbor_builds"]))
+        pot.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][3] == out[1][3] >= 4
+    assert np.abs(out[0][1] - out[1][1]).max() < 1e-6
+    assert np.sqrt(((out[0][2] - out[1][2]) ** 2).mean()) < 1e-5
+
+
 def test_neighbor_overflow_is_reported_and_recovered(l3k3_path):
     # dilute first frame sizes the list; a compressed cluster then overflows it
     rng = np.random.default_rng(12)
