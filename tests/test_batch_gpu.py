@@ -55,6 +55,34 @@ def test_batch_matches_oracle_cell_by_cell(l3k3_path, batch, fp64):
     pot.close()
 
 
+def test_batch_dense_wide_cells(l3k3_path):
+    # cells wider than twice the cutoff: 256 atoms at 0.14 atoms/A^3 (one
+    # tile, about 127 near candidates per atom) overflow the wide-cell path's
+    # queue so its direct pass takes over; 700 atoms at 0.15 (three tiles) and
+    # a cell of ordinary density stay within it
+    cells = [structures.random_insertion(256, 0.14, 1.6, (1.0, 1.0, 1.0), seed=51),
+             structures.random_insertion(300, 0.06, 2.1, (1.0, 1.0, 1.2), seed=52),
+             structures.random_insertion(700, 0.15, 1.6, (1.1, 0.9, 1.0), seed=53)]
+    boxes = [c[0] for c in cells]
+    types = np.concatenate([c[1] for c in cells]).astype(np.int32)
+    pos = np.concatenate([c[2] for c in cells], axis=1)
+    off = np.concatenate([[0], np.cumsum([c[1].size for c in cells])]).astype(np.int32)
+    H = np.stack([b.cpu_h.reshape(9) for b in boxes])
+    assert all((np.diag(b.cpu_h.reshape(3, 3)) > 12.1).all() for b in boxes)
+    dev = torch.device("cuda")
+    pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr"])
+    pe, f, w, ce, cw = _run(pot, off, H, types, pos, dev)
+    pot.close()
+    orc = O.Oracle(l3k3_path)
+    for c, box in enumerate(boxes):
+        a, b = off[c], off[c + 1]
+        pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types[a:b], pos[:, a:b])
+        # relative bars: dense random packings give large synthetic-model energies
+        assert np.abs(pe[a:b] - pe0).max() < 5e-6 * max(1.0, np.abs(pe0).max())
+        assert np.sqrt(((f[:, a:b] - f0) ** 2).mean()) < 1e-5 * max(1.0, np.sqrt((f0 ** 2).mean()))
+        assert np.sqrt(((w[:, a:b] - w0) ** 2).mean()) < 1e-5 * max(1.0, np.sqrt((w0 ** 2).mean()))
+
+
 def test_batch_mixed_triclinic_cells(l3k3_path):
     # every other cell sheared (xy and xz tilts): triclinic cells take the
     # general per-atom image scan, orthorhombic ones the shared-memory scan

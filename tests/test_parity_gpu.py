@@ -121,6 +121,15 @@ def test_atoms_far_outside_an_open_axis(l3k3_path):
     compare(l3k3_path, obox, types_all, pos_all, fp64=True)
 
 
+def test_dense_packing_overflows_the_fill_queue(l3k3_path):
+    # 0.15 atoms/A^3 (about 136 neighbours within rc + skin): a neighbour cell
+    # holds more candidates within the cutoff than the fill's per-thread queue,
+    # so the fill takes its direct pass there; the list must stay the FP64 one
+    box, types, pos = structures.random_insertion(900, 0.15, 1.6, (1.0, 1.1, 0.9), seed=23)
+    compare(l3k3_path, box, types, pos, relative=True)
+    compare(l3k3_path, box, types, pos, fp64=True, relative=True)
+
+
 def per_mu_radial_model(src, dst):
     """Copy of model ``src`` whose radial functions each get their own (scal,
     shift) per species pair, so no radial argument is shared between them
