@@ -632,7 +632,19 @@ struct Engine {
         cg_bin = compile_cg_source(cg_src);
       cg_compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
-    if (model_edges.valid()) ejit_bin = model_edges.get();
+    if (model_edges.valid()) {
+      // a failed model-specialised build falls back to the kernels that read
+      // the coefficients from their parameters (ahead of time, or built for
+      // the shape)
+      try {
+        ejit_bin = model_edges.get();
+      } catch (const std::exception&) {
+        ejit_bin.reset();
+        edge_jit = shape_supported(model.l_max, model.k_max, model.rb_size) ? 0 : 1;
+        if (edge_jit == 1)
+          ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
+      }
+    }
     if (num_atoms > 0) ensure_size(num_atoms);
   }
 
