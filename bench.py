@@ -156,6 +156,22 @@ def flops_model(kmu, rb, C, Bb, P):
     return per_edge_basic, per_edge_force, per_atom_product
 
 
+def max_over_ranks(torch, values, world, device):
+    """Each value's maximum over all ranks, by one MAX all-reduce: the slowest
+    rank's time sets the whole job's throughput.  Every rank calls it at the
+    same point of the run, so the ranks issue the same collectives in the same
+    order."""
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_rate(units_per_rank, world, steps, ms):
+    """Units all ranks processed per second when the slowest rank took ms."""
+    return units_per_rank * world * steps / (ms * 1e-3)
+
+
 def fma_peak(lib):
     v32, v64 = ctypes.c_double(0), ctypes.c_double(0)
     lib.sus2sh_measure_fma_peak(0, ctypes.byref(v32))
@@ -445,13 +461,10 @@ def main():
                                                      min(args.warmup, 3), True, world)
         frms, de, de_total = force_error_vs_fp64(torch, path, box, types, md.pos)
         e2e_val, h2d, d2h = e2e_run(torch, pot, box, types, md.pos, args.e2e_steps)
-        times = torch.tensor([ms, ms64 or 0.0, 1.0 / max(e2e_val, 1e-30)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
-        ms_max, ms64_max, inv_e2e = times.tolist()
+        ms_max, ms64_max, inv_e2e = max_over_ranks(torch, [ms, ms64 or 0.0, 1.0 / max(e2e_val, 1e-30)], world,
+                                                   "cuda")
         if rank == 0:
-            total_atoms = N * world
-            value = total_atoms * args.steps / (ms_max * 1e-3)
+            value = whole_job_rate(N, world, args.steps, ms_max)
             info = pot.info()
             kmu = info["k_max"] * (info["l_max"] + 1)
             C = (info["l_max"] + 1) ** 2
@@ -472,10 +485,10 @@ def main():
                            "model": "SUS2-SH L3 K3 body4 rb8 (248 moments, 806 products)",
                            "l2": "inputs larger than L2 (positions+neighbour list+moments > 126 MB)",
                            "parallelism": f"replicas x{world}"},
-                "fp64": {"value": N * world * args.fp64_steps / (ms64_max * 1e-3) if ms64_max else None,
+                "fp64": {"value": whole_job_rate(N, world, args.fp64_steps, ms64_max) if ms64_max else None,
                          "ms_per_step": ms64_max / args.fp64_steps if ms64_max else None,
                          "steps": args.fp64_steps},
-                "fp32_over_fp64": (value / (N * world * args.fp64_steps / (ms64_max * 1e-3))) if ms64_max else None,
+                "fp32_over_fp64": (value / whole_job_rate(N, world, args.fp64_steps, ms64_max)) if ms64_max else None,
                 "accuracy": {"force_rms_fp32_vs_fp64_eV_per_A": frms, "max_abs_dE_per_atom_eV": de,
                              "abs_dE_total_per_atom_eV": de_total},
                 "stage_ms_per_step": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"},
