@@ -100,31 +100,21 @@ __global__ void k_batch_pack(int N, int ncells, const int* __restrict__ off, con
   atom_cell[i] = c;
 }
 
-__global__ void __launch_bounds__(128)
-    k_batch_fill(int N, const int* __restrict__ off, const int* __restrict__ atom_cell,
-                 const double4* __restrict__ pos4, const double* __restrict__ cell_h,
-                 const int* __restrict__ cell_reach, double cutoff2, int* __restrict__ nbr,
-                 int* __restrict__ ncount, int cap, int count_only, Status* st) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const int c = atom_cell[i];
-  const double* h = cell_h + 9 * c;
-  const int rx = cell_reach[3 * c], ry = cell_reach[3 * c + 1], rz = cell_reach[3 * c + 2];
-  const bool ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
-  if (ortho) return;  // orthorhombic cells: k_batch_fill_ortho
-  const double cut = sqrt(cutoff2);
+// Neighbours of atom i among atoms [j0, j1) of its cell (h, reach r): every
+// image within reach gets the FP64 distance test, j ascending, then tz, ty, tx
+// ascending.  Writes the list and its count and flags an overflow.
+__device__ void fp64_image_scan(int i, int j0, int j1, const double4* __restrict__ pos4,
+                                const double* __restrict__ h, int rx, int ry, int rz, double cutoff2,
+                                int* __restrict__ nbr, int* __restrict__ ncount, int N, int cap, int count_only,
+                                Status* st) {
   const double4 pi = pos4[i];
   int k = 0;
-  const int j1 = off[c + 1];
-  for (int j = off[c]; j < j1; ++j) {
+  for (int j = j0; j < j1; ++j) {
     const double4 pj = pos4[j];
     const double d0x = pj.x - pi.x, d0y = pj.y - pi.y, d0z = pj.z - pi.z;
     for (int tz = -rz; tz <= rz; ++tz) {
-      if (ortho && fabs(d0z + tz * h[8]) >= cut) continue;
       for (int ty = -ry; ty <= ry; ++ty) {
-        if (ortho && fabs(d0y + ty * h[4]) >= cut) continue;
         for (int tx = -rx; tx <= rx; ++tx) {
-          if (ortho && fabs(d0x + tx * h[0]) >= cut) continue;
           if (j == i && tx == 0 && ty == 0 && tz == 0) continue;
           const double dx = d0x + tx * h[0] + ty * h[1] + tz * h[2];
           const double dy = d0y + tx * h[3] + ty * h[4] + tz * h[5];
@@ -145,6 +135,21 @@ __global__ void __launch_bounds__(128)
   if (k > cap && !count_only) st->overflow = 1;
 }
 
+__global__ void __launch_bounds__(128)
+    k_batch_fill(int N, const int* __restrict__ off, const int* __restrict__ atom_cell,
+                 const double4* __restrict__ pos4, const double* __restrict__ cell_h,
+                 const int* __restrict__ cell_reach, double cutoff2, int* __restrict__ nbr,
+                 int* __restrict__ ncount, int cap, int count_only, Status* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int c = atom_cell[i];
+  const double* h = cell_h + 9 * c;
+  const bool ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 && h[7] == 0.0;
+  if (ortho) return;  // orthorhombic cells: k_batch_fill_ortho
+  fp64_image_scan(i, off[c], off[c + 1], pos4, h, cell_reach[3 * c], cell_reach[3 * c + 1], cell_reach[3 * c + 2],
+                  cutoff2, nbr, ncount, N, cap, count_only, st);
+}
+
 // Orthorhombic cells, one CTA per cell: the cell's positions are staged in
 // shared memory (FP32, relative to its first atom) and every thread tests its
 // atom against them.  Cells wider than twice the cutoff take the nearest image
@@ -153,7 +158,11 @@ __global__ void __launch_bounds__(128)
 // most `reach` each way).  An FP32 pre-test with a 1e-3 A margin admits a superset of the pairs;
 // each admitted pair gets the exact FP64 test of k_batch_fill, so the lists
 // (and their order: j ascending, then tz, ty, tx ascending) are the same.
+// Both FP32 tests hold their margins for coordinates (relative to the cell's
+// first atom) up to kCompact; a cell with an atom farther out (a long periodic
+// edge, or atoms far along an open axis) takes the FP64 scan of k_batch_fill.
 constexpr int kFillTile = 256;
+constexpr double kCompact = 512.0;
 // per-thread queue of a tile's near candidates in the wide-cell path
 constexpr int kFillQueue = 96;
 
@@ -169,6 +178,17 @@ __global__ void __launch_bounds__(128)
   const int a0 = off[c], a1 = off[c + 1];
   if (!ortho || a1 <= a0) return;  // uniform across the block
   const double4 o = pos4[a0];
+  bool spread = false;
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const double4 p = pos4[a];
+    spread |= !(fabs(p.x - o.x) <= kCompact && fabs(p.y - o.y) <= kCompact && fabs(p.z - o.z) <= kCompact);
+  }
+  if (__syncthreads_or(spread)) {  // uniform across the block
+    for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x)
+      fp64_image_scan(i, a0, a1, pos4, h, cell_reach[3 * c], cell_reach[3 * c + 1], cell_reach[3 * c + 2], cutoff2,
+                      nbr, ncount, N, cap, count_only, st);
+    return;
+  }
   const float L[3] = {static_cast<float>(h[0]), static_cast<float>(h[4]), static_cast<float>(h[8])};
   const float iL[3] = {1.0f / L[0], 1.0f / L[1], 1.0f / L[2]};
   const int r[3] = {cell_reach[3 * c], cell_reach[3 * c + 1], cell_reach[3 * c + 2]};

@@ -17,19 +17,20 @@ def batch():
     return structures.cell_batch(24, 16, 512, seed=41)
 
 
-def _run(pot, off, H, types, pos, dev, cell=True):
+def _run(pot, off, H, types, pos, dev, cell=True, pbc=None):
     N = types.size
     ncells = off.size - 1
     t = torch.as_tensor(types, device=dev)
     x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
     o = torch.as_tensor(off, device=dev)
     h = torch.as_tensor(H.reshape(-1).copy(), device=dev)
+    cp = torch.as_tensor(np.ascontiguousarray(pbc, dtype=np.int32).reshape(-1), device=dev) if pbc is not None else None
     pe = torch.zeros(N, dtype=torch.float64, device=dev)
     f = torch.zeros(3 * N, dtype=torch.float64, device=dev)
     w = torch.zeros(9 * N, dtype=torch.float64, device=dev)
     ce = torch.zeros(ncells, dtype=torch.float64, device=dev)
     cw = torch.zeros(9 * ncells, dtype=torch.float64, device=dev)
-    pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce, cell_virial=cw)
+    pot.compute_batch(o, h, t, x, pe, f, w, cell_pbc=cp, cell_energy=ce, cell_virial=cw)
     torch.cuda.synchronize()
     assert pot.sync() == 0
     return pe.cpu().numpy(), f.view(3, N).cpu().numpy(), w.view(9, N).cpu().numpy(), ce.cpu().numpy(), \
@@ -81,6 +82,47 @@ def test_batch_dense_wide_cells(l3k3_path):
         assert np.abs(pe[a:b] - pe0).max() < 5e-6 * max(1.0, np.abs(pe0).max())
         assert np.sqrt(((f[:, a:b] - f0) ** 2).mean()) < 1e-5 * max(1.0, np.sqrt((f0 ** 2).mean()))
         assert np.sqrt(((w[:, a:b] - w0) ** 2).mean()) < 1e-5 * max(1.0, np.sqrt((w0 ** 2).mean()))
+
+
+def _segments(nx, ny, nz, shifts, seed):
+    """Copies of one FCC block shifted along z."""
+    _, types, pos = structures.fcc(nx, ny, nz, 3.8, (0.5, 0.5), 0.05, seed=seed)
+    return (np.concatenate([types] * len(shifts)).astype(np.int32),
+            np.concatenate([pos + np.array([[0.0], [0.0], [s]]) for s in shifts], axis=1))
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_batch_cells_spread_over_thousands_of_angstrom(l3k3_path, fp64):
+    # orthorhombic cells whose atoms lie thousands of A apart: a 7.6 x 7.6 x
+    # 6000 A periodic wire of FCC segments (one across the z boundary) and a
+    # cell periodic in x, y (15.2 A) with FCC slabs up to 7000 A out along
+    # its open z axis.  Such cells take the FP64 image scan instead of the
+    # FP32 pre-tests (whose margins hold for cell-local coordinates); a compact
+    # cell after them keeps the shared-memory scan.  Lists and results must
+    # be the oracle's.
+    t1, p1 = _segments(2, 2, 3, [0.0, 1500.0, 3000.0, 5988.6], 61)
+    p1[2] %= 6000.0
+    t2, p2 = _segments(4, 4, 2, [0.0, -7000.0, -6992.4, 6000.0], 62)
+    b3, t3, p3 = structures.fcc(4, 4, 4, 3.8, (0.64, 0.36), 0.05, seed=63)
+    boxes = [Box.orthorhombic(7.6, 7.6, 6000.0), Box.orthorhombic(15.2, 15.2, 20.0, pbc=(1, 1, 0)), b3]
+    types = np.concatenate([t1, t2, t3]).astype(np.int32)
+    pos = np.concatenate([p1, p2, p3], axis=1)
+    off = np.concatenate([[0], np.cumsum([t1.size, t2.size, t3.size])]).astype(np.int32)
+    H = np.stack([b.cpu_h.reshape(9) for b in boxes])
+    pbc = np.stack([b.pbc for b in boxes])
+    dev = torch.device("cuda")
+    pot = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr"] + (["sus2_float=0"] if fp64 else []))
+    pe, f, w, ce, cw = _run(pot, off, H, types, pos, dev, pbc=pbc)
+    pot.close()
+    orc = O.Oracle(l3k3_path)
+    etol, tol = (1e-9, 1e-9) if fp64 else (1e-6, 1e-5)
+    for c, box in enumerate(boxes):
+        a, b = off[c], off[c + 1]
+        pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types[a:b], pos[:, a:b])
+        assert np.abs(pe[a:b] - pe0).max() < etol, c
+        assert np.sqrt(((f[:, a:b] - f0) ** 2).mean()) < tol, c
+        assert np.sqrt(((w[:, a:b] - w0) ** 2).mean()) < tol, c
+        assert abs(ce[c] - pe0.sum()) < etol * (b - a), c
 
 
 def test_batch_mixed_triclinic_cells(l3k3_path):
