@@ -366,6 +366,7 @@ struct Engine {
   DevBuf<unsigned char> Bbuf, Gbuf, scratch, ftmp;
   DevBuf<Status> d_status;
   Status* h_status = nullptr;  // pinned
+  int device = -1;             // the device current at creation; all tables live there
   cudaStream_t last_stream = nullptr;
   size_t prod_smem = 0;
   int prod_tile = 32;
@@ -602,6 +603,7 @@ struct Engine {
       d_smap.upload(model.moment_mapping);
       d_sw.upload(model.moment_coeffs);
     }
+    ck(cudaGetDevice(&device), "cudaGetDevice");
     ck(cudaMallocHost(&h_geom, sizeof(BoxGeom)), "cudaMallocHost");
     ck(cudaMallocHost(&h_status, sizeof(Status)), "cudaMallocHost");
     std::memset(h_status, 0, sizeof(Status));
@@ -1278,6 +1280,7 @@ bool cg_view(const sus2sh_handle* h, CgView* out) {
   out->species = h->e.d_species.p;
   out->species_count = h->e.model.species_count;
   out->use_float = h->e.use_float ? 1 : 0;
+  out->device = h->e.device;
   return true;
 }
 void set_last_error(const std::string& msg) { g_last_error = msg; }

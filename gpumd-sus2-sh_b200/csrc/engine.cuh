@@ -95,6 +95,7 @@ struct CgView {
   const double* species;
   int species_count;
   int use_float;
+  int device;  // device the handle's tables were created on
 };
 
 // ---- launchers (engine.cu) ----------------------------------------------

@@ -2,12 +2,13 @@
 // adjoint) on caller-provided basic moments, allocating no device memory.
 //
 // Why it exists: some callers cannot call cudaMalloc at the moment they need
-// the contraction -- code running inside a CUDA stream capture (allocation is
-// not capturable), MD codes that reserve all device memory up front in their
-// own pools and forbid allocations during a run, and real-time loops where an
-// allocation's implicit synchronisation is not acceptable.  The handle's model
-// tables are created once by sus2sh_create; this entry point then needs only
-// the caller's input/output arrays plus the fixed work area below.
+// the contraction.  MD codes that reserve all device memory up front in their
+// own pools forbid allocations during a run (a cudaMalloc there can fail
+// once the pool holds the GPU's memory, and it bypasses their accounting);
+// real-time loops cannot take the device-wide synchronisation an allocation
+// or free may imply.  The handle's model tables are created once by
+// sus2sh_create; this entry point then needs only the caller's input/output
+// arrays plus the fixed work area below.
 //
 // The work area (the per-atom value/adjoint slots of the CG program, laid out
 // [slot][N]) is one file-scope __device__ array of kNoAllocScratchBytes
@@ -98,8 +99,15 @@ __global__ void __launch_bounds__(128)
     code += nt;
     cf += nt;
   }
-  int ti = type[atom];
-  if (ti < 0 || ti >= species) ti = 0;  // table lookups stay in bounds
+  const int ti = type[atom];
+  if (ti < 0 || ti >= species) {
+    // A species outside the model: the atom's energy and adjoints are NaN, so
+    // the caller sees the bad input instead of another species' numbers.
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    pe[atom] = nan;
+    for (int b = 0; b < p.nbasic; ++b) G[static_cast<size_t>(b) * N + atom] = static_cast<T>(nan);
+    return;
+  }
   const double ct = species_coeffs[ti];
   pe[atom] = shift_coeffs[ti] + ct + ct * E;
   const T sc = static_cast<T>(ct);
@@ -131,6 +139,13 @@ extern "C" int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int
     set_last_error("sus2sh_cg_energy_noalloc: no usable current device");
     return SUS2SH_E_CUDA;
   }
+  if (dev != v.device) {
+    // the model tables live on the handle's device; the work area and the
+    // launch would be on the current one
+    set_last_error("sus2sh_cg_energy_noalloc: the current device (" + std::to_string(dev) +
+                   ") is not the device the handle was created on (" + std::to_string(v.device) + ")");
+    return SUS2SH_E_ARG;
+  }
   void* scratch = nullptr;
   {
     // First call on each device: resolve the device address of the array
@@ -148,18 +163,22 @@ extern "C" int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int
     }
     scratch = g_scratch_addr[dev];
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int grid = (N + 127) / 128;
+  // cudaLaunchKernelEx returns this launch's own status; an error the caller
+  // left pending from earlier work stays pending for the caller to read.
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((N + 127) / 128);
+  cfg.blockDim = dim3(128);
+  cfg.stream = static_cast<cudaStream_t>(stream);
+  cudaError_t rc;
   if (v.use_float) {
-    k_cg_noalloc<float><<<grid, 128, 0, s>>>(N, v.prog, type, static_cast<const float*>(basics),
-                                              static_cast<float*>(basic_adjoint), static_cast<float*>(scratch),
-                                              v.shift, v.species, v.species_count, potential);
+    rc = cudaLaunchKernelEx(&cfg, k_cg_noalloc<float>, N, v.prog, type, static_cast<const float*>(basics),
+                            static_cast<float*>(basic_adjoint), static_cast<float*>(scratch), v.shift, v.species,
+                            v.species_count, potential);
   } else {
-    k_cg_noalloc<double><<<grid, 128, 0, s>>>(N, v.prog, type, static_cast<const double*>(basics),
-                                               static_cast<double*>(basic_adjoint), static_cast<double*>(scratch),
-                                               v.shift, v.species, v.species_count, potential);
+    rc = cudaLaunchKernelEx(&cfg, k_cg_noalloc<double>, N, v.prog, type, static_cast<const double*>(basics),
+                            static_cast<double*>(basic_adjoint), static_cast<double*>(scratch), v.shift,
+                            v.species, v.species_count, potential);
   }
-  const cudaError_t rc = cudaGetLastError();
   if (rc != cudaSuccess) {
     set_last_error(std::string("sus2sh_cg_energy_noalloc: launch failed: ") + cudaGetErrorString(rc));
     return SUS2SH_E_CUDA;

@@ -151,21 +151,25 @@ int sus2sh_profile_read(sus2sh_handle* h, double* out, int n);
 /* No counterpart in the reference.  The CG product stage alone (forward
  * contraction, site energy E_i and adjoints dE_i/dB_b(i)) on basic moments the
  * caller provides, for callers that cannot allocate device memory at call
- * time: code inside a CUDA stream capture, MD codes that reserve all device
- * memory up front and forbid allocations during a run, and real-time loops
- * that cannot take an allocation's implicit synchronisation.  It calls no
+ * time: MD codes that reserve all device memory up front in their own pools
+ * and forbid allocations during a run, and real-time loops that cannot take
+ * the synchronisation an allocation or free may imply.  It calls no
  * cudaMalloc, cudaFree or allocating library routine.
  *   basics        [alpha_index_basic_count][N], the model's basic order,
  *                 float for an FP32 handle (sus2_float=1), double otherwise
  *   potential     [N] double, assigned
  *   basic_adjoint [alpha_index_basic_count][N], same type as basics, assigned
+ * An atom whose species lies outside [0, species_count) gets NaN energy and
+ * NaN adjoints.  The device current at the call must be the one the handle
+ * was created on (SUS2SH_E_ARG otherwise).
  * Its work area is one fixed 16 MiB device array inside the library (held by
  * every GPU that loads the library until the process exits), so
  * N * 2 * (program value slots) * sizeof(element) must be at most 16 MiB;
  * larger N is rejected with SUS2SH_E_ARG and a message giving the limit.  The
  * first call on each device resolves that array's device address with the
  * device current; make that first call before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race, so serialise them. */
+ * share the array: calls that overlap on the GPU race, so serialise them.  A
+ * CUDA error left pending by the caller's earlier work is not consumed. */
 int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, const void* basics,
                              double* potential, void* basic_adjoint, void* stream);
 

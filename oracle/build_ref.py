@@ -20,7 +20,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_ROOT = os.environ.get("SUS2SH_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: $SUS2SH_REFERENCE_ROOT, else a directory named
+# "reference" beside this repository's root; absent (the usual case away from
+# the development machine) means the prebuilt files in _ref/ are used as they are.
+REF_ROOT = os.environ.get("SUS2SH_REFERENCE_ROOT") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 
 ZBL_HEADER = os.path.join("src", "force", "sus2_zbl_common.cuh")
 ZBL_TEST = os.path.join("codex_tests", "gpumd_sh_zbl_common_check.cpp")
@@ -29,7 +33,7 @@ BIN_ZBL_CHECK = os.path.join(OUT, "zbl_common_check")
 
 
 def reference_present(root: str = REF_ROOT) -> bool:
-    return os.path.exists(os.path.join(root, ZBL_HEADER)) and os.path.exists(os.path.join(root, ZBL_TEST))
+    return bool(root) and os.path.exists(os.path.join(root, ZBL_HEADER)) and os.path.exists(os.path.join(root, ZBL_TEST))
 
 
 def build(root: str = REF_ROOT, force: bool = False) -> dict:

@@ -75,3 +75,35 @@ def test_noalloc_rejects_sizes_beyond_the_work_area(l3k3_path):
     msg = lib.sus2sh_last_error().decode()
     assert "fixed maximum" in msg and "N <=" in msg
     pot.close()
+
+
+def test_noalloc_marks_unknown_species_with_nan(l3k3_path):
+    """An atom whose species lies outside the model gets NaN energy and NaN
+    adjoints; the other atoms keep the values of a call without it."""
+    box, types, pos = structures.fcc(2, 2, 2, 3.8, (0.5, 0.5), 0.05, seed=22)
+    N = types.size
+    dev = torch.device("cuda")
+    pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr"])
+    orc = O.Oracle(l3k3_path)
+    B = orc.basics(box.cpu_h, box.pbc, types, pos)
+    Bd = torch.as_tensor(B, dtype=torch.float32, device=dev).contiguous()
+    lib = _lib.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = []
+    for bad in (None, 5):
+        tt = types.copy()
+        if bad is not None:
+            tt[bad] = 7                      # species_count is 2
+        t = torch.as_tensor(tt, device=dev)
+        pe = torch.zeros(N, dtype=torch.float64, device=dev)
+        G = torch.zeros(tuple(B.shape), dtype=torch.float32, device=dev)
+        rc = lib.sus2sh_cg_energy_noalloc(pot.handle, N, _ptr(t), _ptr(Bd), _ptr(pe), _ptr(G), stream)
+        assert rc == 0, lib.sus2sh_last_error().decode()
+        torch.cuda.synchronize()
+        out.append((pe.cpu().numpy(), G.cpu().numpy()))
+    (pe0, g0), (pe1, g1) = out
+    assert np.isnan(pe1[5]) and np.isnan(g1[:, 5]).all()
+    keep = np.arange(N) != 5
+    assert np.isfinite(pe1[keep]).all()
+    assert np.array_equal(pe1[keep], pe0[keep]) and np.array_equal(g1[:, keep], g0[:, keep])
+    pot.close()
