@@ -16,10 +16,13 @@ runs the same workload for the FP32/FP64 ratio.  Multi-GPU runs are
 independent replicas (weak scaling, no collective on the data path); timing is
 the max over ranks.
 
---impl reference times the reference-semantics CPU evaluation (the FP64 oracle
-port; the reference itself cannot be built without an upstream GPUMD tree) on
-this host's cores, one force evaluation of a 6,912-atom sample of the same
-crystal and model per step.
+--impl reference times the reference's own SUS2-SH engine: src/force/sus2_sh.cu,
+unmodified, compiled for sm_100a against minimal GPUMD stand-ins
+(oracle/_ref/ref_sus2sh, built by oracle/build_ref.py), on the same 1,024,000-atom
+frame and model on this GPU, one SUS2_SH::compute per step (its default FP32
+path; its FP64 path and its own stage profile are reported beside it).  Where
+that build or a GPU is absent it falls back to the FP64 oracle port on this
+host's cores.
 """
 import argparse
 import ctypes
@@ -172,7 +175,10 @@ def whole_job_rate(units_per_rank, world, steps, ms):
     return units_per_rank * world * steps / (ms * 1e-3)
 
 
-def fma_peak(lib):
+def fma_peak():
+    """FP32 and FP64 FMA throughput of this GPU (libsus2sh_tools.so probe)."""
+    from sus2sh import _lib
+    lib = _lib.load_tools()
     v32, v64 = ctypes.c_double(0), ctypes.c_double(0)
     lib.sus2sh_measure_fma_peak(0, ctypes.byref(v32))
     lib.sus2sh_measure_fma_peak(1, ctypes.byref(v64))
@@ -180,8 +186,8 @@ def fma_peak(lib):
 
 
 def make_workload(model_dir, rank):
-    from sus2sh import models, structures
-    path = models.preset_model("l3k3", model_dir)
+    from sus2sh import structures
+    path = MODEL_FIXTURE  # the seeded l3k3 model (preset "l3k3"), shared with the reference arm
     box, types, pos = structures.fcc(*CELLS_RUN, A, (0.64, 0.36), 0.0, seed=1000 + rank)
     masses = [structures.AMU["Cu"], structures.AMU["Zr"]]
     vel = structures.maxwell_boltzmann(types, masses, TEMP, seed=2000 + rank)
@@ -390,29 +396,69 @@ def cpu_baseline_sample(path, cells=20, reps=3):
                       f"the same FCC Cu-Zr crystal and model (same per-atom work), OpenMP {threads} threads"}
 
 
-def reference_arm(args):
-    world, rank, local = dist_env()
-    if rank != 0:
-        return
-    sys.path.insert(0, ORACLE)
+MODEL_FIXTURE = os.path.join(REPO, "tests", "golden", "models", "l3k3.mtp")
+
+
+def _reference_gpu_arm(args, path, box, types, pos):
+    """The reference's own SUS2-SH engine (src/force/sus2_sh.cu, unmodified,
+    nvcc sm_100a against minimal GPUMD stand-ins: oracle/_ref/ref_sus2sh) on
+    the full workload frame, called as GPUMD's Force::compute calls it.  The
+    reference rebuilds its neighbour list inside every call, so a call on a
+    static frame costs what an MD step's force call costs; the integrator is
+    not timed (it is GPUMD's)."""
+    import numpy as np
+    import ref_engine
+    N = int(types.size)
+    sym = ("Cu", "Zr")
+    pe32, f32, w32, ms32, _ = ref_engine.run(path, box.cpu_h, box.pbc, types, pos, sym, steps=args.steps,
+                                             warmup=args.warmup, timeout=1800)
+    k = max(1, min(args.steps, 10))
+    _, _, _, _, out = ref_engine.run(path, box.cpu_h, box.pbc, types, pos,
+                                     (*sym, "sus2_sh_profile=1", f"sus2_sh_profile_interval={k}"), steps=k,
+                                     warmup=k, timeout=1800)
+    stages = ref_engine.profile_stages(out)
+    k64 = max(1, min(args.steps, 5))
+    pe64, f64, _, ms64, _ = ref_engine.run(path, box.cpu_h, box.pbc, types, pos, (*sym, "sus2_float=0"), steps=k64,
+                                           warmup=2, timeout=1800)
+    value = N / (ms32 * 1e-3)
+    sample = ("the reference's own CUDA engine (src/force/sus2_sh.cu, unmodified, nvcc sm_100a against minimal "
+              "GPUMD stand-ins) on the full 1,024,000-atom frame on this GPU; the reference has no CPU path; "
+              "one host thread drives it")
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-step/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded FCC Cu-Zr, seeded random l3k3 model: tests/golden/models/l3k3.mtp)",
+        "config": {"workload": "1.024M-atom l3k3 Cu-Zr (80x80x40 FCC, a=3.8 A, 64/36), SUS2_SH::compute per step",
+                   "atoms": N, "inputs": "larger than L2 (positions 24.6 MB, moments 2 x 1 GB)"},
+        "reference_build": "oracle/_ref/ref_sus2sh (src/force/sus2_sh.cu unmodified, sus2_float=1 default path)",
+        "stage_ms_per_step": stages,
+        "fp64": {"value": N / (ms64 * 1e-3), "ms_per_step": ms64, "steps": k64},
+        "accuracy": {"force_rms_fp32_vs_fp64": float(np.sqrt(((f32 - f64) ** 2).mean())),
+                     "max_site_energy_fp32_vs_fp64": float(np.abs(pe32 - pe64).max())},
+        "cpu_baseline": {"value": value, "unit": "atom-step/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "atom-step/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def _reference_cpu_arm(args, path):
+    """Without the reference build: the FP64 oracle port on this host's
+    cores, one force evaluation of a 6,912-atom slice per step."""
     import sus2sh_oracle
-    from sus2sh import models, structures
-    with tempfile.TemporaryDirectory() as d:
-        path = models.preset_model("l3k3", d)
-        box, types, pos = structures.fcc(12, 12, 12, A, (0.64, 0.36), 0.0, seed=7)
-        orc = sus2sh_oracle.Oracle(path)
-        threads = os.cpu_count() or 1
-        for _ in range(args.warmup):
-            orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
-        dt = time.perf_counter() - t0
+    from sus2sh import structures
+    box, types, pos = structures.fcc(12, 12, 12, A, (0.64, 0.36), 0.0, seed=7)
+    orc = sus2sh_oracle.Oracle(path)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+    dt = time.perf_counter() - t0
     value = types.size * args.steps / dt
     sample = (f"one FP64 force evaluation per step of a {types.size}-atom 12^3-cell slice of the 1.024M-atom "
-              f"FCC Cu-Zr crystal, same l3k3 model; reference-semantics C port (the reference needs an "
-              f"upstream GPUMD tree that is not available), OpenMP {threads} threads")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "atom-step/s", "n_gpus": args.gpus,
+              f"FCC Cu-Zr crystal, same l3k3 model; reference-semantics C port, OpenMP {threads} threads")
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "atom-step/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded FCC Cu-Zr, seeded random l3k3 model)",
@@ -421,6 +467,23 @@ def reference_arm(args):
             "cpu_baseline": {"value": value, "unit": "atom-step/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "atom-step/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def reference_arm(args):
+    """Rank 0 alone; loads no library of this repository (the model is the
+    committed fixture, the structure plain numpy)."""
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, ORACLE)
+    import ref_engine
+    from sus2sh import structures
+    import torch
+    if ref_engine.available() and torch.cuda.is_available():
+        box, types, pos = structures.fcc(*args.cells, A, (0.64, 0.36), 0.0, seed=1000)
+        line = _reference_gpu_arm(args, MODEL_FIXTURE, box, types, pos)
+    else:
+        line = _reference_cpu_arm(args, MODEL_FIXTURE)
     print(json.dumps(line), flush=True)
 
 
@@ -472,7 +535,7 @@ def main():
             edges = edges_within(box, pos, pot.rc)
             force_ms_launch = prof["force_ms"] / max(prof["calls"], 1)
             force_flops = edges * ff
-            fp32_peak, fp64_peak = fma_peak(lib)
+            fp32_peak, fp64_peak = fma_peak()
             achieved = force_flops / (force_ms_launch * 1e-3) / 1e12
             step_flops = edges * (fb + ff) + N * fp
             line = {

@@ -1,7 +1,7 @@
 // Handle, CG-program compiler and the extern "C" entry points of sus2sh.h /
-// sus2sh_tools.h.
+// sus2sh_diag.h.
 #include "../../include/sus2sh.h"
-#include "../../include/sus2sh_tools.h"
+#include "../../include/sus2sh_diag.h"
 #include "cg_codegen.h"
 #include "edge_jit.h"
 #include "engine.cuh"
@@ -1564,71 +1564,6 @@ int sus2sh_profile_read(sus2sh_handle* h, double* out, int n) {
   return SUS2SH_OK;
 }
 
-// ---- tools -----------------------------------------------------------------
-int sus2sh_write_synthetic_model(const char* path, int species, int l_max, int k_max, int body_order,
-                                 const int* body_l_max, int n_body_l_max, int rb_size, double r_min, double rc,
-                                 int rational, const double* shift_coeffs, double radial_sigma,
-                                 double moment_sigma, double scal, double rshift, unsigned long long seed) {
-  if (!path || !shift_coeffs) return SUS2SH_E_ARG;
-  return guarded([&] {
-    sus2sh::SynthSpec sp;
-    sp.species = species;
-    sp.l_max = l_max;
-    sp.k_max = k_max;
-    sp.body_order = body_order;
-    sp.rb_size = rb_size;
-    sp.r_min = r_min;
-    sp.rc = rc;
-    sp.rational = rational;
-    if (body_l_max)
-      for (int i = 0; i < n_body_l_max; ++i) sp.body_l_max_list.push_back(body_l_max[i]);
-    sp.shift.assign(shift_coeffs, shift_coeffs + species);
-    sp.radial_sigma = radial_sigma;
-    sp.moment_sigma = moment_sigma;
-    sp.scal = scal;
-    sp.rshift = rshift;
-    sp.seed = seed;
-    sus2sh::write_synthetic_model(path, sp);
-  });
-}
-
-int sus2sh_standard_graph_counts(int l_max, int k_max, int body_order, const int* body_l_max, int n_body_l_max,
-                                 int* out) {
-  if (!out) return SUS2SH_E_ARG;
-  return guarded([&] {
-    std::vector<int> bl = sus2sh::default_body_l_max(l_max);
-    if (body_l_max)
-      for (int i = 0; i < n_body_l_max && 2 + i < 7; ++i) bl[2 + i] = body_l_max[i];
-    const sus2sh::StandardGraph g = sus2sh::build_standard_graph(l_max, k_max, body_order, bl);
-    out[0] = g.node_count;
-    out[1] = static_cast<int>(g.basic_k.size());
-    out[2] = static_cast<int>(g.products.size());
-    out[3] = static_cast<int>(g.scalars.size());
-    out[4] = g.tensor_blocks;
-    out[5] = g.cg_blocks;
-    out[6] = g.cg_terms;
-    out[7] = g.max_layer;
-  });
-}
-
-int sus2sh_md_kick_drift(int N, double dt, const double* inv_mass_type, const int* type, double* force,
-                         double* velocity, double* position, double* potential, double* virial, void* stream) {
-  sus2sh::launch_nve_kick_drift(static_cast<cudaStream_t>(stream), N, dt, inv_mass_type, type, force, velocity,
-                                position, potential, virial);
-  return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
-}
-
-int sus2sh_md_kick(int N, double dt, const double* inv_mass_type, const int* type, const double* force,
-                   double* velocity, void* stream) {
-  sus2sh::launch_nve_kick(static_cast<cudaStream_t>(stream), N, dt, inv_mass_type, type, force, velocity);
-  return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
-}
-
-int sus2sh_reduce(int N, const double* potential, const double* virial, double* out, void* stream) {
-  sus2sh::launch_reduce(static_cast<cudaStream_t>(stream), N, potential, virial, out);
-  return cudaGetLastError() == cudaSuccess ? SUS2SH_OK : SUS2SH_E_CUDA;
-}
-
 int sus2sh_cg_kernel_info(const char* path, int use_float, int split, int* info, char* text, size_t text_size) {
   if (!path || !info) return SUS2SH_E_ARG;
   return guarded([&] {
@@ -1741,57 +1676,6 @@ int sus2sh_zbl_pair(int zi, int zj, double r, double inner, double outer, double
   const sus2sh::zbl::PairValue v = sus2sh::zbl::pair(zi, zj, r, inner, outer);
   *energy = v.energy;
   *dEdr = v.dEdr;
-  return SUS2SH_OK;
-}
-
-int sus2sh_measure_fma_peak(int fp64, double* tflops) {
-  if (!tflops) return SUS2SH_E_ARG;
-  *tflops = sus2sh::measure_fma_tflops(fp64 != 0);
-  return *tflops > 0 ? SUS2SH_OK : SUS2SH_E_CUDA;
-}
-
-int sus2sh_random_insertion(int N, double lx, double ly, double lz, double dmin, unsigned long long seed,
-                            double* position) {
-  if (N <= 0 || !position || !(dmin > 0.0)) return SUS2SH_E_ARG;
-  // grid of cells >= dmin; each cell holds few points
-  const int nx = std::max(1, static_cast<int>(lx / dmin)), ny = std::max(1, static_cast<int>(ly / dmin)),
-            nz = std::max(1, static_cast<int>(lz / dmin));
-  const double cx = lx / nx, cy = ly / ny, cz = lz / nz;
-  std::vector<std::vector<int>> cells(static_cast<size_t>(nx) * ny * nz);
-  std::mt19937_64 rng(seed);
-  std::uniform_real_distribution<double> U(0.0, 1.0);
-  const double d2 = dmin * dmin;
-  long long attempts = 0;
-  const long long budget = 2000LL * N + 1000000LL;
-  int placed = 0;
-  while (placed < N) {
-    if (++attempts > budget) return -5;
-    const double x = U(rng) * lx, y = U(rng) * ly, z = U(rng) * lz;
-    const int ix = std::min(nx - 1, static_cast<int>(x / cx)), iy = std::min(ny - 1, static_cast<int>(y / cy)),
-              iz = std::min(nz - 1, static_cast<int>(z / cz));
-    bool ok = true;
-    for (int oz = -1; oz <= 1 && ok; ++oz)
-      for (int oy = -1; oy <= 1 && ok; ++oy)
-        for (int ox = -1; ox <= 1 && ok; ++ox) {
-          const int jx = (ix + ox + nx) % nx, jy = (iy + oy + ny) % ny, jz = (iz + oz + nz) % nz;
-          for (int p : cells[(static_cast<size_t>(jz) * ny + jy) * nx + jx]) {
-            double dx = position[p] - x, dy = position[p + N] - y, dz = position[p + 2 * N] - z;
-            dx -= lx * std::round(dx / lx);
-            dy -= ly * std::round(dy / ly);
-            dz -= lz * std::round(dz / lz);
-            if (dx * dx + dy * dy + dz * dz < d2) {
-              ok = false;
-              break;
-            }
-          }
-        }
-    if (!ok) continue;
-    position[placed] = x;
-    position[placed + N] = y;
-    position[placed + 2 * N] = z;
-    cells[(static_cast<size_t>(iz) * ny + iy) * nx + ix].push_back(placed);
-    ++placed;
-  }
   return SUS2SH_OK;
 }
 

@@ -565,40 +565,6 @@ __global__ void __launch_bounds__(128)
     for (int q = 0; q < 9; ++q) virial[static_cast<size_t>(q) * N + i] += w[q];
 }
 
-// ---------------------------------------------------------------------------
-// MD integrator (velocity Verlet); units A, fs, amu, eV.
-// ---------------------------------------------------------------------------
-constexpr double kAccel = 9.648533212331002e-3;  // (eV/A/amu) -> A/fs^2
-
-// Half kick + drift; the force (and optionally energy/virial) arrays are
-// zeroed after use so the next accumulating force call starts from zero.
-__global__ void k_kick_drift(int N, double dt, const double* __restrict__ inv_mass_type,
-                             const int* __restrict__ type, double* __restrict__ f,
-                             double* __restrict__ v, double* __restrict__ x,
-                             double* __restrict__ pe, double* __restrict__ vir) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const double a = 0.5 * dt * kAccel * inv_mass_type[type[i]];
-  for (int d = 0; d < 3; ++d) {
-    const double vv = v[i + d * N] + a * f[i + d * N];
-    v[i + d * N] = vv;
-    x[i + d * N] += dt * vv;
-    f[i + d * N] = 0.0;
-  }
-  if (pe) pe[i] = 0.0;
-  if (vir)
-    for (int q = 0; q < 9; ++q) vir[static_cast<size_t>(q) * N + i] = 0.0;
-}
-
-__global__ void k_kick(int N, double dt, const double* __restrict__ inv_mass_type,
-                       const int* __restrict__ type, const double* __restrict__ f,
-                       double* __restrict__ v) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const double a = 0.5 * dt * kAccel * inv_mass_type[type[i]];
-  for (int d = 0; d < 3; ++d) v[i + d * N] += a * f[i + d * N];
-}
-
 // Sum of per-atom energy (out[0]) and virial (out[1..9]); one FP64 atomic
 // per block and component.
 __global__ void k_reduce(int N, const double* __restrict__ pe, const double* __restrict__ vir,
@@ -624,55 +590,9 @@ __global__ void k_reduce(int N, const double* __restrict__ pe, const double* __r
   }
 }
 
-// FMA throughput probe: 8 independent dependency chains per thread, each
-// thread writes only its own output slot.
-template <typename T>
-__global__ void __launch_bounds__(256) k_fma_peak(int iters, T seed, T* __restrict__ out) {
-  T a0 = seed + threadIdx.x, a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3);
-  T a4 = a0 + T(4), a5 = a0 + T(5), a6 = a0 + T(6), a7 = a0 + T(7);
-  const T m = T(0.9999), c = T(1e-4);
-  for (int k = 0; k < iters; ++k) {
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
-      a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
-    }
-  }
-  out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
-}
-
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
-
-double measure_fma_tflops(bool fp64) {
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int blocks = sms * 8, threads = 256, iters = fp64 ? 512 : 2048;
-  void* out = nullptr;
-  if (cudaMalloc(&out, sizeof(double) * blocks * threads) != cudaSuccess) return -1.0;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  float best = 1e30f;
-  for (int rep = 0; rep < 6; ++rep) {
-    cudaEventRecord(e0);
-    if (fp64) k_fma_peak<double><<<blocks, threads>>>(iters, 1.0, static_cast<double*>(out));
-    else k_fma_peak<float><<<blocks, threads>>>(iters, 1.0f, static_cast<float*>(out));
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (rep > 0 && ms < best) best = ms;
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaFree(out);
-  if (cudaGetLastError() != cudaSuccess) return -1.0;
-  const double flops = 2.0 * 8.0 * 16.0 * iters * static_cast<double>(blocks) * threads;
-  return flops / (best * 1e-3) / 1e12;
-}
 
 void launch_reduce(cudaStream_t s, int N, const double* pe, const double* virial, double* out) {
   cudaMemsetAsync(out, 0, 10 * sizeof(double), s);
@@ -923,21 +843,12 @@ void launch_finalize(cudaStream_t s, int N, const void* ftmp, double* force, dou
   k_finalize<T><<<blocks_for(N, 256), 256, 0, s>>>(N, ftmp, force, sign);
 }
 
-void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_mass_type, const int* type,
-                           double* force, double* vel, double* pos, double* pe, double* vir) {
-  k_kick_drift<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel, pos, pe, vir);
-}
 
 void launch_zbl(cudaStream_t s, int mode, int N, int cap, const double4* pos4, const int* nbr, const int* ncount,
                 const double (*shift)[3], const int* atom_cell, const ZblTables& z, const double* weight,
                 double* pe, double* force, double* virial, double sign) {
   k_zbl<<<blocks_for(N, 128), 128, 0, s>>>(mode, N, cap, pos4, nbr, ncount, shift, atom_cell, z, weight, pe, force,
                                            virial, sign);
-}
-
-void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_type, const int* type,
-                     const double* force, double* vel) {
-  k_kick<<<blocks_for(N, 256), 256, 0, s>>>(N, dt, inv_mass_type, type, force, vel);
 }
 
 template int launch_basic<float>(cudaStream_t, const EdgeArgs<float>&, float*, int, bool);

@@ -220,17 +220,6 @@ void launch_zbl(cudaStream_t s, int mode, int N, int cap, const double4* pos4, c
                 const double (*shift)[3], const int* atom_cell, const ZblTables& z, const double* weight,
                 double* pe, double* force, double* virial, double sign);
 
-// Integrator kernels for the benchmark MD driver.
-void launch_nve_kick_drift(cudaStream_t s, int N, double dt, const double* inv_mass_type,
-                           const int* type, double* force, double* vel, double* pos, double* pe,
-                           double* vir);
-void launch_nve_kick(cudaStream_t s, int N, double dt, const double* inv_mass_type,
-                     const int* type, const double* force, double* vel);
-
 bool shape_supported(int l_max, int k_max, int rb);
-
-// Measured FMA throughput of the current device (TFLOP/s, 2 flops per FMA),
-// best of five launches; -1 on error.
-double measure_fma_tflops(bool fp64);
 
 }  // namespace sus2sh

@@ -11,7 +11,6 @@
 #include <fstream>
 #include <functional>
 #include <map>
-#include <random>
 #include <sstream>
 #include <tuple>
 #include <unordered_map>
@@ -938,82 +937,6 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
     // ignored: this engine has a single execution plan.
   }
   return o;
-}
-
-// ---------------------------------------------------------------------------
-// Seeded synthetic model writer: a standard graph plus random coefficients,
-// in the text layout the reference reader accepts.
-// ---------------------------------------------------------------------------
-void write_synthetic_model(const std::string& path, const SynthSpec& sp) {
-  if (sp.species <= 0 || sp.l_max < 0 || sp.l_max > 6 || sp.k_max <= 0 || sp.body_order < 2 ||
-      sp.body_order > 6 || sp.rb_size <= 0 || sp.rb_size > 16 ||
-      static_cast<int>(sp.shift.size()) != sp.species)
-    throw InputError("Invalid synthetic model specification.");
-  std::vector<int> blmax = default_body_l_max(sp.l_max);
-  if (!sp.body_l_max_list.empty())
-    for (size_t i = 0; i < sp.body_l_max_list.size(); ++i) blmax[2 + i] = sp.body_l_max_list[i];
-  const StandardGraph g = build_standard_graph(sp.l_max, sp.k_max, sp.body_order, blmax);
-  const int S = sp.species, kmu = sp.k_max * (sp.l_max + 1);
-  std::mt19937_64 rng(sp.seed);
-  std::normal_distribution<double> nrm(0.0, 1.0);
-  FILE* f = std::fopen(path.c_str(), "w");
-  if (!f) throw InputError("Cannot write synthetic model: " + path);
-  auto list = [&](const char* key, const std::vector<double>& v) {
-    std::fprintf(f, "%s = {", key);
-    for (size_t i = 0; i < v.size(); ++i) std::fprintf(f, "%s%.17g", i ? ", " : "", v[i]);
-    std::fprintf(f, "}\n");
-  };
-  std::fprintf(f, "MTP\nversion = 1.1.0\npotential_name = SUS2-SH synthetic\n");
-  std::fprintf(f, "potential_tag = SUS2-SH\nscaling = 1.0\nscaling_map = LK\n");
-  std::fprintf(f, "species_count = %d\n", S);
-  std::fprintf(f, "sh_l_max = %d\nsh_k_max = %d\nsh_body_order = %d\nsh_parity = even\n",
-               sp.l_max, sp.k_max, sp.body_order);
-  if (!sp.body_l_max_list.empty()) {
-    std::fprintf(f, "sh_body_l_max = {");
-    for (size_t i = 0; i < sp.body_l_max_list.size(); ++i)
-      std::fprintf(f, "%s%d", i ? ", " : "", sp.body_l_max_list[i]);
-    std::fprintf(f, "}\n");
-  }
-  std::fprintf(f, "radial_basis_type = %s\n", sp.rational ? "RBChebyshev_sss_rational" : "RBChebyshev_sss");
-  std::fprintf(f, "\tmin_dist = %.17g\n\tmax_dist = %.17g\n", sp.r_min, sp.rc);
-  std::fprintf(f, "\tradial_basis_size = %d\n\tradial_funcs_count = %d\n", sp.rb_size, kmu);
-  list("shift_coeffs", sp.shift);
-  std::vector<double> scal(2 * S * S * kmu);
-  const double rshift = sp.rshift < 0.0 ? 0.5 * (sp.r_min + sp.rc) : sp.rshift;
-  for (int mu = 0; mu < kmu; ++mu)
-    for (int p = 0; p < S * S; ++p) {
-      scal[2 * mu * S * S + p] = sp.scal;
-      scal[2 * mu * S * S + S * S + p] = rshift;
-    }
-  list("scal_coeffs", scal);
-  std::fprintf(f, "\tradial_coeffs\n");
-  for (int mu = 0; mu < kmu; ++mu) {
-    std::fprintf(f, "\t\t{");
-    for (int n = 0; n < sp.rb_size; ++n) std::fprintf(f, "%s%.17g", n ? ", " : "", sp.radial_sigma * nrm(rng));
-    for (int t = 0; t < S; ++t) std::fprintf(f, ", %.17g", sp.radial_type_coeff);
-    std::fprintf(f, "}\n");
-  }
-  std::fprintf(f, "alpha_moments_count = %d\n", g.node_count);
-  std::fprintf(f, "alpha_index_basic_count = %d\nalpha_index_basic = {", static_cast<int>(g.basic_k.size()));
-  for (size_t i = 0; i < g.basic_k.size(); ++i)
-    std::fprintf(f, "%s{%d, %d, %d}", i ? ", " : "", g.basic_k[i], g.basic_l[i], g.basic_m[i]);
-  std::fprintf(f, "}\n");
-  std::fprintf(f, "sh_product_count = %d\nsh_products = {", static_cast<int>(g.products.size()));
-  for (size_t p = 0; p < g.products.size(); ++p)
-    std::fprintf(f, "%s{%d, %d, %d, %.17g}", p ? ", " : "", g.products[p].left, g.products[p].right,
-                 g.products[p].target, g.products[p].coeff);
-  std::fprintf(f, "}\n");
-  std::fprintf(f, "alpha_scalar_moments = %d\nalpha_moment_mapping = {", static_cast<int>(g.scalars.size()));
-  for (size_t s = 0; s < g.scalars.size(); ++s) std::fprintf(f, "%s%d", s ? ", " : "", g.scalars[s]);
-  std::fprintf(f, "}\n");
-  std::fprintf(f, "sh_scalar_info_count = %d\nsh_scalar_info = {", static_cast<int>(g.scalars.size()));
-  for (size_t s = 0; s < g.scalar_body.size(); ++s) std::fprintf(f, "%s{%d}", s ? ", " : "", g.scalar_body[s]);
-  std::fprintf(f, "}\n");
-  list("species_coeffs", std::vector<double>(S, 1.0));
-  std::vector<double> w(g.scalars.size());
-  for (double& x : w) x = sp.moment_sigma * nrm(rng);
-  list("moment_coeffs", w);
-  std::fclose(f);
 }
 
 }  // namespace sus2sh

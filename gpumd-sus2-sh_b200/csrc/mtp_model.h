@@ -148,25 +148,5 @@ struct Options {
 // the reference's tuning switches are accepted and ignored.
 Options parse_options(const HostModel& m, int nopts, const char** opts);
 
-// ---- synthetic model writer (seeded) -----------------------------------------
-struct SynthSpec {
-  int species = 2;
-  int l_max = 3;
-  int k_max = 3;
-  int body_order = 4;
-  int rb_size = 8;
-  double r_min = 2.0;
-  double rc = 5.0;
-  int rational = 0;
-  std::vector<int> body_l_max_list;      // empty: none written
-  std::vector<double> shift;             // [S] site energy shifts
-  double radial_sigma = 0.1;
-  double moment_sigma = 0.01;
-  double scal = 1.0;                     // radial tanh scale
-  double rshift = -1.0;                  // radial shift; <0 -> (r_min+rc)/2
-  double radial_type_coeff = 1.0;
-  unsigned long long seed = 0;
-};
-void write_synthetic_model(const std::string& path, const SynthSpec& spec);
 
 }  // namespace sus2sh

@@ -1,5 +1,6 @@
 """Minimal NVE velocity-Verlet driver around the engine, standing in for
-GPUMD's integrator (not vendored by the reference) in the benchmark.
+GPUMD's integrator (not vendored by the reference) in the benchmark; its
+kernels are in libsus2sh_tools.so.
 
 All state is device-resident (torch CUDA tensors, GPUMD SoA layouts); each
 step is kick+drift (which also zeroes the force/energy/virial accumulators),
@@ -32,7 +33,7 @@ class NVE:
         self.pe = torch.zeros(self.N, dtype=torch.float64, device=dev)
         self.force = torch.zeros(3 * self.N, dtype=torch.float64, device=dev)
         self.virial = torch.zeros(9 * self.N, dtype=torch.float64, device=dev)
-        self.lib = _lib.load()
+        self.lib = _lib.load_tools()
         self.kernel_launches_per_step = None
 
     def _stream(self):
@@ -47,11 +48,11 @@ class NVE:
     def step(self):
         p = lambda t: ctypes.c_void_p(t.data_ptr())
         s = self._stream()
-        _lib.check(self.lib.sus2sh_md_kick_drift(self.N, self.dt, p(self.inv_mass), p(self.type), p(self.force),
+        _lib.check_tools(self.lib.sus2sh_md_kick_drift(self.N, self.dt, p(self.inv_mass), p(self.type), p(self.force),
                                                  p(self.vel), p(self.pos), p(self.pe), p(self.virial), s),
                    "md kick_drift")
         self.pot.compute(self.box, self.type, self.pos, self.pe, self.force, self.virial)
-        _lib.check(self.lib.sus2sh_md_kick(self.N, self.dt, p(self.inv_mass), p(self.type), p(self.force),
+        _lib.check_tools(self.lib.sus2sh_md_kick(self.N, self.dt, p(self.inv_mass), p(self.type), p(self.force),
                                            p(self.vel), s), "md kick")
 
     def kinetic_energy(self) -> float:

@@ -1,8 +1,8 @@
 """Seeded synthetic SUS2-SH models of the benchmark workloads.
 
 The reference's trained Cu-Zr models are not shipped, so every workload uses a
-model written by ``sus2sh_write_synthetic_model`` (standard real-CG graph,
-random coefficients).  Choices not fixed by the workload description are
+model written by ``sus2sh_write_synthetic_model`` (libsus2sh_tools.so:
+standard real-CG graph, random coefficients).  Choices not fixed by the workload description are
 recorded here: species_coeffs = 1, radial type coefficients = 1, every radial
 (scal, shift) = (1.0, (r_min + rc)/2), and the Al site shift -3.0 eV.
 """
@@ -30,10 +30,10 @@ PRESETS = {
 def write_model(path: str, species=2, l_max=3, k_max=3, body_order=4, rb_size=8, r_min=2.0, rc=5.0,
                 rational=0, shift=(-3.5, -5.0), radial_sigma=0.1, moment_sigma=0.01, scal=1.0,
                 rshift=-1.0, seed=0, body_l_max=None) -> str:
-    lib = _lib.load()
+    lib = _lib.load_tools()
     sh = (ctypes.c_double * species)(*shift)
     bl = (ctypes.c_int * len(body_l_max))(*body_l_max) if body_l_max else None
-    _lib.check(lib.sus2sh_write_synthetic_model(
+    _lib.check_tools(lib.sus2sh_write_synthetic_model(
         path.encode(), species, l_max, k_max, body_order, ctypes.cast(bl, ctypes.c_void_p) if bl else None,
         len(body_l_max) if body_l_max else 0, rb_size, r_min, rc, rational,
         ctypes.cast(sh, ctypes.c_void_p), radial_sigma, moment_sigma, scal, rshift,

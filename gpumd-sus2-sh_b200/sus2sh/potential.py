@@ -172,10 +172,11 @@ class SUS2_SH:
 
 
 def standard_graph_counts(l_max, k_max, body_order, body_l_max=None) -> dict:
-    lib = _lib.load()
+    """Counts of the standard graph (libsus2sh_tools.so)."""
+    lib = _lib.load_tools()
     out = (ctypes.c_int * 8)()
     bl = (ctypes.c_int * len(body_l_max))(*body_l_max) if body_l_max else None
-    _lib.check(lib.sus2sh_standard_graph_counts(l_max, k_max, body_order,
+    _lib.check_tools(lib.sus2sh_standard_graph_counts(l_max, k_max, body_order,
                                                 ctypes.cast(bl, ctypes.c_void_p) if bl else None,
                                                 len(body_l_max) if body_l_max else 0, out),
                "sus2sh_standard_graph_counts")

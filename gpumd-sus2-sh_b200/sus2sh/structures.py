@@ -53,7 +53,7 @@ def random_insertion(N: int, density: float, dmin: float, edge_ratios=(1.0, 1.0,
     scale = (N / density / np.prod(r)) ** (1.0 / 3.0)
     lx, ly, lz = (r * scale).tolist()
     pos = np.zeros(3 * N)
-    lib = _lib.load()
+    lib = _lib.load_tools()
     rc = lib.sus2sh_random_insertion(N, lx, ly, lz, dmin, ctypes.c_ulonglong(int(seed) & (2**64 - 1)),
                                      pos.ctypes.data_as(ctypes.c_void_p))
     if rc != 0:

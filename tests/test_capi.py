@@ -10,13 +10,13 @@ import pytest
 import sus2sh
 from sus2sh import _lib
 
-HEADERS = [os.path.join(os.path.dirname(__file__), "..", "include", h) for h in ("sus2sh.h", "sus2sh_tools.h")]
+INCLUDE = os.path.join(os.path.dirname(__file__), "..", "include")
 
 
-def declared_functions():
+def declared_functions(*headers):
     names = set()
-    for h in HEADERS:
-        text = open(h).read()
+    for h in headers:
+        text = open(os.path.join(INCLUDE, h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names |= set(re.findall(r"\b(sus2sh_[a-z0-9_]+)\s*\(", text))
     return names
@@ -24,10 +24,24 @@ def declared_functions():
 
 def test_library_exports_every_declared_symbol():
     lib = _lib.load()
-    decl = declared_functions()
+    decl = declared_functions("sus2sh.h", "sus2sh_diag.h")
     assert decl == set(_lib.EXPORTS)
     for name in decl:
         assert hasattr(lib, name), name
+
+
+def test_tools_library_is_separate_from_the_engine():
+    """The writer, integrator, insertion and FMA probe are in
+    libsus2sh_tools.so, and libsus2sh.so exports none of them."""
+    import subprocess
+    tools = _lib.load_tools()
+    decl = declared_functions("sus2sh_tools.h")
+    assert decl == set(_lib.TOOLS_EXPORTS)
+    for name in decl:
+        assert hasattr(tools, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], stdout=subprocess.PIPE, text=True).stdout
+    engine_syms = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert not (decl & engine_syms), decl & engine_syms
 
 
 def test_is_sus2_sh_file(l3k3_path, tmp_path):
@@ -110,3 +124,13 @@ def test_null_arguments_rejected():
     assert lib.sus2sh_create(None, 0, 0, None, None) == -3
     assert lib.sus2sh_compute(None, 10, None, None, None, None, None, None, None, None) == -3
     assert lib.sus2sh_sync(None, None) == -3
+
+
+def test_model_fixture_matches_the_writer(tmp_path):
+    """tests/golden/models/l3k3.mtp (read by the benchmark's reference arm)
+    is exactly what the seeded writer produces for preset l3k3."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_model_fixtures as fx
+    fresh = fx.write_fresh("l3k3", str(tmp_path))
+    assert open(fresh, "rb").read() == open(fx.FIXTURES["l3k3"], "rb").read()

@@ -30,7 +30,8 @@ Boxes: the config-0 crystal (30.4 A, the reference's neighbour-list path),
 a 108-atom cell (11.4 A), 16-atom cells thinner than twice the cutoff (the
 reference's own explicit-image kernels, ``sus2_sh.cu:7668-7769``), a
 triclinic box and open boundaries; models: the l3k3 Cu-Zr model, ZBL,
-both gate modes, and l = 1, 2, 5, 6 shapes.
+both gate modes (energies against the reference's, forces against central
+differences of the reference's energies), and l = 1, 2, 5, 6 shapes.
 """
 import os
 
@@ -136,15 +137,33 @@ def test_zbl_model(l3k3_path, tmp_path):
 
 @pytest.mark.parametrize("mode", ["mu-scalar-full", "mu-body-linear-combo"])
 def test_gate_models(l3k3_path, tmp_path, mode):
-    # the reference runs gate models in FP32 only (sus2_sh.cu:7862)
+    """Gate models (the reference runs them in FP32 only, sus2_sh.cu:7862).
+    Site energies match the reference's.  Forces are the gradient of that
+    energy: central differences of the reference's own energies (step
+    0.01 A) agree with the engine's forces to their FP32 noise.  The
+    reference's own force output does not (it differs from the same
+    differences by up to 2e-2 eV/A on this cell), so forces are compared with
+    the reference's energy, not with its force array."""
     path = models.add_gate(l3k3_path, str(tmp_path / f"gate_{mode}.mtp"), mode=mode)
-    box, types, pos = structures.fcc(4, 4, 4, 3.8, (0.5, 0.5), 0.05, seed=7)
-    r32 = ref_engine.run(path, box.cpu_h, box.pbc, types, pos, ("Cu", "Zr", "sus2_float=1"))[:3]
-    orc = O.Oracle(path)
-    e_ref = _errors(orc.efs(box.cpu_h, box.pbc, types, pos), r32)
-    e_eng = _errors(engine_efs(path, box, types, pos), r32)
-    assert e_ref[0] < E_REF32 and e_ref[1] < F_REF32, e_ref
-    assert e_eng[0] < E_REF32 and e_eng[1] < F_REF32, e_eng
+    box, types, pos = structures.fcc(3, 3, 3, 3.8, (0.5, 0.5), 0.05, seed=7)
+    opts = ("Cu", "Zr", "sus2_float=1")
+    pe_r, f_r, _ = ref_engine.run(path, box.cpu_h, box.pbc, types, pos, opts)[:3]
+    pe_e, f_e, _ = engine_efs(path, box, types, pos)
+    assert np.abs(pe_e - pe_r).max() < E_REF32
+    h = 0.01
+    worst_engine, worst_ref = 0.0, 0.0
+    for a in (0, 5, 17):
+        for d in range(3):
+            e = []
+            for sgn in (1, -1):
+                p = pos.copy()
+                p[d, a] += sgn * h
+                e.append(ref_engine.run(path, box.cpu_h, box.pbc, types, p, opts)[0].sum())
+            fd = -(e[0] - e[1]) / (2 * h)
+            worst_engine = max(worst_engine, abs(f_e[d, a] - fd))
+            worst_ref = max(worst_ref, abs(f_r[d, a] - fd))
+    print({"engine_vs_reference_fd": worst_engine, "reference_forces_vs_reference_fd": worst_ref})
+    assert worst_engine < 2e-3, worst_engine
 
 
 @pytest.mark.parametrize("shape", [(1, 1, 3, 4), (2, 2, 4, 8), (5, 2, 3, 8), (6, 1, 3, 6)])
