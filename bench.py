@@ -343,7 +343,7 @@ def batch_cells_run(torch, path, ncells=4096, reps=10):
             "tiles": {"basic_block": info["basic_block"], "force_block": info["force_block"]}}
 
 
-def large_model_run(torch, model_dir, reps=5, atoms=262144):
+def large_model_run(torch, model_dir, reps=5, atoms=262144, opts=()):
     """Large-model workload: Cu-Zr-Al body-5 L=4 K=4 rb10 rational-map model
     (5985 moments, 33,389 products) on 262,144 random-insertion atoms
     (0.06 A^-3, d_min 2.1 A, 50/35/15), FP32; static positions, one
@@ -353,7 +353,7 @@ def large_model_run(torch, model_dir, reps=5, atoms=262144):
     box, types, pos = structures.random_insertion(atoms, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=77)
     N = types.size
     dev = torch.device("cuda")
-    pot = SUS2_SH(path, N, ["Cu", "Zr", "Al"])
+    pot = SUS2_SH(path, N, ["Cu", "Zr", "Al", *opts])
     t = torch.as_tensor(types, device=dev)
     x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
     z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)
@@ -410,8 +410,9 @@ def _reference_gpu_arm(args, path, box, types, pos):
     import ref_engine
     N = int(types.size)
     sym = ("Cu", "Zr")
-    pe32, f32, w32, ms32, _ = ref_engine.run(path, box.cpu_h, box.pbc, types, pos, sym, steps=args.steps,
-                                             warmup=args.warmup, timeout=1800)
+    pe32, f32, w32, ms32, out32 = ref_engine.run(path, box.cpu_h, box.pbc, types, pos, sym, steps=args.steps,
+                                                 warmup=args.warmup, timeout=1800)
+    spread = {k: v for k, v in ref_engine.timing(out32).items() if k.startswith("ref_ms_")}
     k = max(1, min(args.steps, 10))
     _, _, _, _, out = ref_engine.run(path, box.cpu_h, box.pbc, types, pos,
                                      (*sym, "sus2_sh_profile=1", f"sus2_sh_profile_interval={k}"), steps=k,
@@ -433,6 +434,7 @@ def _reference_gpu_arm(args, path, box, types, pos):
                    "atoms": N, "inputs": "larger than L2 (positions 24.6 MB, moments 2 x 1 GB)"},
         "reference_build": "oracle/_ref/ref_sus2sh (src/force/sus2_sh.cu unmodified, sus2_float=1 default path)",
         "stage_ms_per_step": stages,
+        "step_ms_spread": spread,
         "fp64": {"value": N / (ms64 * 1e-3), "ms_per_step": ms64, "steps": k64},
         "accuracy": {"force_rms_fp32_vs_fp64": float(np.sqrt(((f32 - f64) ** 2).mean())),
                      "max_site_energy_fp32_vs_fp64": float(np.abs(pe32 - pe64).max())},

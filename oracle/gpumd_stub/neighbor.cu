@@ -2,16 +2,13 @@
 // Neighbor class (neighbor.cuh).  Cell list in fractional coordinates: cells
 // at least rc thick along each periodic axis with three or more cells, one
 // cell spanning the axis otherwise (open axes, thin axes); atoms sorted by
-// cell with a stable sort, so lists are deterministic; each atom scans its
-// cell's neighbourhood once per distinct cell and tests the minimum-image
-// r^2 < rc^2 in FP64.
+// cell with a stable radix sort, so lists are deterministic; each atom scans
+// its cell's neighbourhood once per distinct cell and tests the
+// minimum-image r^2 < rc^2 in FP64.
 #include "neighbor.cuh"
 
-#include <thrust/device_ptr.h>
-#include <thrust/execution_policy.h>
-#include <thrust/scan.h>
-#include <thrust/sequence.h>
-#include <thrust/sort.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cstdio>
@@ -80,6 +77,11 @@ __global__ void k_stub_search(int N, Box box, int nx, int ny, int nz, double rc2
   NN[i] = n < max_nbr ? n : max_nbr;
 }
 
+__global__ void k_stub_iota(int N, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) out[i] = i;
+}
+
 }  // namespace
 
 void Neighbor::initialize(double, int, int max_nbr) { max_nbr_ = max_nbr; }
@@ -95,23 +97,35 @@ void Neighbor::find_neighbor_global(double rc, Box& box, const GPU_Vector<int>& 
     nb_[d] = n >= 3 ? n : 1;
   }
   const int ncell = nb_[0] * nb_[1] * nb_[2];
-  cell_.resize(N);
-  order_.resize(N);
-  start_.resize(ncell);
-  count_.resize(ncell);
+  if (cell_.size() != static_cast<size_t>(N)) {
+    cell_.resize(N);
+    keys_.resize(N);
+    index_.resize(N);
+    order_.resize(N);
+  }
+  if (start_.size() < static_cast<size_t>(ncell)) {
+    start_.resize(ncell);
+    count_.resize(ncell);
+  }
+  // scratch of the radix sort and the scan, sized once for this N and ncell
+  size_t sort_bytes = 0, scan_bytes = 0;
+  CHECK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, cell_.data(), keys_.data(), index_.data(),
+                                        order_.data(), N));
+  CHECK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, count_.data(), start_.data(), ncell));
+  const size_t need = std::max(sort_bytes, scan_bytes);
+  if (temp_.size() < need) temp_.resize(need);
   CHECK(cudaMemset(count_.data(), 0, sizeof(int) * ncell));
   const double* x = position.data();
   const int grid = (N + 127) / 128;
   k_stub_bin<<<grid, 128>>>(N, box, nb_[0], nb_[1], nb_[2], x, x + N, x + 2 * N, cell_.data(), count_.data());
   CHECK(cudaGetLastError());
-  thrust::device_ptr<int> cell(cell_.data()), order(order_.data()), cnt(count_.data()), st(start_.data());
-  thrust::exclusive_scan(thrust::device, cnt, cnt + ncell, st);
-  // sort a copy of the cell keys so cell_ keeps each atom's own cell
-  GPU_Vector<int> keys(N);
-  CHECK(cudaMemcpy(keys.data(), cell_.data(), sizeof(int) * N, cudaMemcpyDeviceToDevice));
-  thrust::device_ptr<int> k(keys.data());
-  thrust::sequence(thrust::device, order, order + N);
-  thrust::stable_sort_by_key(thrust::device, k, k + N, order);
+  k_stub_iota<<<grid, 128>>>(N, index_.data());
+  CHECK(cudaGetLastError());
+  size_t bytes = temp_.size();
+  CHECK(cub::DeviceScan::ExclusiveSum(temp_.data(), bytes, count_.data(), start_.data(), ncell));
+  bytes = temp_.size();
+  CHECK(cub::DeviceRadixSort::SortPairs(temp_.data(), bytes, cell_.data(), keys_.data(), index_.data(),
+                                        order_.data(), N));
 }
 
 void Neighbor::find_local_neighbor_from_global(double rc, Box& box, const GPU_Vector<double>& position,
@@ -119,6 +133,7 @@ void Neighbor::find_local_neighbor_from_global(double rc, Box& box, const GPU_Ve
   const int N = static_cast<int>(NN.size());
   if (overflow_.size() != 1) overflow_.resize(1);
   CHECK(cudaMemset(overflow_.data(), 0, sizeof(int)));
+  // the cell grid of find_neighbor_global is reused (same box and positions)
   const double* x = position.data();
   const int grid = (N + 127) / 128;
   k_stub_search<<<grid, 128>>>(N, box, nb_[0], nb_[1], nb_[2], rc * rc, x, x + N, x + 2 * N, cell_.data(),

@@ -5,7 +5,8 @@
 // from both ends, r^2 < rc^2 by the minimum image.  The engine uses it only
 // for boxes at least twice the cutoff thick along every periodic axis (it
 // switches to its own image kernels otherwise), so the minimum image is the
-// only image within rc.
+// only image within rc.  Buffers are kept between calls and grow only with
+// N, so a call allocates nothing in the steady state.
 #pragma once
 #include "box.cuh"
 #include "utilities/gpu_vector.cuh"
@@ -20,10 +21,13 @@ public:
 
 private:
   int max_nbr_ = 512;
-  int nb_[3] = {1, 1, 1};  // cells per axis
-  GPU_Vector<int> cell_;     // cell of each atom, then sorted
-  GPU_Vector<int> order_;    // atoms sorted by cell (stable: by index within a cell)
-  GPU_Vector<int> start_;    // first sorted position of each cell
-  GPU_Vector<int> count_;    // atoms per cell
-  GPU_Vector<int> overflow_;
+  int nb_[3] = {1, 1, 1};     // cells per axis
+  GPU_Vector<int> cell_;        // cell of each atom
+  GPU_Vector<int> keys_;        // cell keys sorted along with order_
+  GPU_Vector<int> index_;       // 0..N-1
+  GPU_Vector<int> order_;       // atoms sorted by cell (stable: by index within a cell)
+  GPU_Vector<int> start_;       // first sorted position of each cell
+  GPU_Vector<int> count_;       // atoms per cell
+  GPU_Vector<int> overflow_;    // [0] overflow flag
+  GPU_Vector<unsigned char> temp_;  // sort/scan scratch, kept between calls
 };

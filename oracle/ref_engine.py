@@ -87,9 +87,14 @@ def run(path: str, box_h, pbc, types, pos, opts=(), steps: int = 1, warmup: int 
     pe = data[:N]
     f = data[N:4 * N].reshape(3, N)
     w = data[4 * N:].reshape(9, N)
-    line = [ln for ln in out.splitlines() if ln.startswith('{"ref_ms_per_step"')]
-    ms = json.loads(line[-1])["ref_ms_per_step"] if line else float("nan")
+    ms = timing(out).get("ref_ms_per_step", float("nan"))
     return pe, f, w, ms, out
+
+
+def timing(stdout: str) -> dict:
+    """The driver's timing line: mean, median, min and max ms per call."""
+    line = [ln for ln in stdout.splitlines() if ln.startswith('{"ref_ms_per_step"')]
+    return json.loads(line[-1]) if line else {}
 
 
 def profile_stages(stdout: str) -> dict | None:

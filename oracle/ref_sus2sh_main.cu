@@ -13,12 +13,14 @@
 //       in.bin : int32 N, int32 pbc[3], double h[9] (row-major, box vectors as
 //                columns), int32 type[N], double position[3N] (SoA x, y, z)
 //       out.bin: double potential[N], force[3N], virial[9N] of the last call
-//       prints {"ref_ms_per_step": t, "steps": K, "N": N}: the mean CUDA-event
-//       time of SUS2_SH::compute over the K calls after `warmup` untimed ones.
+//       prints {"ref_ms_per_step": mean, "ref_ms_median", "ref_ms_min",
+//       "ref_ms_max", "steps": K, "N": N}: CUDA-event times of SUS2_SH::compute
+//       over the K calls after `warmup` untimed ones.
 // Options are the run.in tokens after the file name: species symbols first,
 // then the reference's own switches (sus2_float=0|1, sus2_sh_profile=1, ...).
 #include "sus2_sh.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -87,6 +89,7 @@ int main(int argc, char** argv) {
   CHECK(cudaEventCreate(&e0));
   CHECK(cudaEventCreate(&e1));
   double total_ms = 0.0;
+  std::vector<float> step_ms;
   for (int s = 0; s < warmup + steps; ++s) {
     CHECK(cudaMemset(d_pe.data(), 0, sizeof(double) * d_pe.size()));
     CHECK(cudaMemset(d_f.data(), 0, sizeof(double) * d_f.size()));
@@ -97,7 +100,10 @@ int main(int argc, char** argv) {
     CHECK(cudaEventSynchronize(e1));
     float ms = 0.0f;
     CHECK(cudaEventElapsedTime(&ms, e0, e1));
-    if (s >= warmup) total_ms += ms;
+    if (s >= warmup) {
+      total_ms += ms;
+      step_ms.push_back(ms);
+    }
   }
   CHECK(cudaGetLastError());
   std::vector<double> pe(N), f(3 * static_cast<size_t>(N)), vir(9 * static_cast<size_t>(N));
@@ -113,7 +119,12 @@ int main(int argc, char** argv) {
   std::fwrite(f.data(), sizeof(double), f.size(), out);
   std::fwrite(vir.data(), sizeof(double), vir.size(), out);
   std::fclose(out);
-  std::printf("{\"ref_ms_per_step\": %.6f, \"steps\": %d, \"N\": %d}\n", steps > 0 ? total_ms / steps : 0.0, steps,
-              N);
+  std::vector<float> sorted = step_ms;
+  std::sort(sorted.begin(), sorted.end());
+  const double med = sorted.empty() ? 0.0 : sorted[sorted.size() / 2];
+  const double lo = sorted.empty() ? 0.0 : sorted.front(), hi = sorted.empty() ? 0.0 : sorted.back();
+  std::printf("{\"ref_ms_per_step\": %.6f, \"ref_ms_median\": %.6f, \"ref_ms_min\": %.6f, \"ref_ms_max\": %.6f, "
+              "\"steps\": %d, \"N\": %d}\n",
+              steps > 0 ? total_ms / steps : 0.0, med, lo, hi, steps, N);
   return 0;
 }
