@@ -111,6 +111,28 @@ std::vector<double> chebyshev_derivative(const std::vector<double>& c, int kmu, 
   return d;
 }
 
+// Derivative series of Laguerre expansions: L_n' = -(L_0 + ... + L_{n-1}), so
+// sum_n c[mu][n] L_n'(u) = sum_k d[mu][k] L_k(u) with d[mu][k] = -sum_{n>k}
+// c[mu][n] (d[mu][rb-1] = 0).
+std::vector<double> laguerre_derivative(const std::vector<double>& c, int kmu, int rb) {
+  std::vector<double> d(c.size(), 0.0);
+  for (int mu = 0; mu < kmu; ++mu) {
+    const double* cm = &c[static_cast<size_t>(mu) * rb];
+    double* dm = &d[static_cast<size_t>(mu) * rb];
+    double acc = 0.0;
+    for (int k = rb - 2; k >= 0; --k) {
+      acc -= cm[k + 1];
+      dm[k] = acc;
+    }
+  }
+  return d;
+}
+
+// The derivative series of the model's radial basis.
+std::vector<double> radial_derivative(RadialMap kind, const std::vector<double>& c, int kmu, int rb) {
+  return kind == RadialMap::LaguerreLog1p ? laguerre_derivative(c, kmu, rb) : chebyshev_derivative(c, kmu, rb);
+}
+
 // ---------------------------------------------------------------------------
 // CG program: the layered rows of the saved sh_products compiled to the
 // slot machine executed by k_product (see engine.cu for the row kinds).
@@ -321,7 +343,7 @@ struct Engine {
   bool use_float = true;
   RadialSetup rs{};
   std::vector<double> coef;        // [kmu][rb] unscaled
-  std::vector<double> dcoef;       // [kmu][rb] derivative series of coef (chebyshev_derivative)
+  std::vector<double> dcoef;       // [kmu][rb] derivative series of coef (radial_derivative)
   std::vector<double> pair_table;  // [S*S][stride]
 
   // model on device
@@ -523,7 +545,7 @@ struct Engine {
     rs.species = S;
     rs.kmu = kmu;
     rs.rb = rb;
-    rs.rational = model.radial_map == RadialMap::Rational;
+    rs.kind = static_cast<int>(model.radial_map);
     rs.pair_stride = 2 * kmu + 1;
     rs.rc = model.rc;
     bool shared = true;
@@ -550,8 +572,8 @@ struct Engine {
     }
     if (pair_table.size() > static_cast<size_t>(kMaxPairTable))
       throw InputError("SUS2_SH radial pair table too large (species_count^2 * (2*radial_funcs+1) > 8192).");
-    dcoef = chebyshev_derivative(coef, kmu, rb);
-    if (gate) gate_dcoef = chebyshev_derivative(gate_coef, kmu, rb);
+    dcoef = radial_derivative(model.radial_map, coef, kmu, rb);
+    if (gate) gate_dcoef = radial_derivative(model.radial_map, gate_coef, kmu, rb);
     // edge kernels from NVRTC now: specialised to the model (FP32, non-gate),
     // or for the shape when it has no ahead-of-time build (or on request)
     if (opt.edge_jit) {
@@ -567,8 +589,8 @@ struct Engine {
       std::vector<float> table(kMaxCoef);
       table.resize(fill_coef(coef, dcoef, table.data()));
       model_edges = std::async(std::launch::async, [l = model.l_max, k = model.k_max, rb = model.rb_size, table,
-                                                    shared_xi = rs.shared_xi != 0, rational = rs.rational != 0] {
-        return compile_model_edge_kernels(l, k, rb, table, shared_xi, rational);
+                                                    shared_xi = rs.shared_xi != 0, kind = rs.kind] {
+        return compile_model_edge_kernels(l, k, rb, table, shared_xi, kind);
       });
     } else if (edge_jit == 1) {
       ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
@@ -1643,7 +1665,7 @@ int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t
   if (!path || !info) return SUS2SH_E_ARG;
   return guarded([&] {
     const sus2sh::HostModel m = sus2sh::load_model(path);
-    const std::vector<double> dc = sus2sh::chebyshev_derivative(m.radial_coeffs, m.radial_funcs, m.rb_size);
+    const std::vector<double> dc = sus2sh::radial_derivative(m.radial_map, m.radial_coeffs, m.radial_funcs, m.rb_size);
     std::vector<float> table(sus2sh::kMaxCoef);
     table.resize(sus2sh::Engine::fill_coef(m.radial_coeffs, dc, table.data()));
     // one radial argument per pair when every function of every pair has the
@@ -1655,7 +1677,7 @@ int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t
         shared = shared && m.scal_coeffs[2 * mu * S * S + p] == m.scal_coeffs[p] &&
                  m.scal_coeffs[2 * mu * S * S + S * S + p] == m.scal_coeffs[S * S + p];
     const auto bin = sus2sh::compile_model_edge_kernels(m.l_max, m.k_max, m.rb_size, table, shared,
-                                                        m.radial_map == sus2sh::RadialMap::Rational);
+                                                        static_cast<int>(m.radial_map));
     info[0] = bin->basic_registers;
     info[1] = bin->force_registers;
     info[2] = static_cast<int>(bin->compile_ms);

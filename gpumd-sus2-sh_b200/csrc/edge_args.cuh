@@ -10,11 +10,13 @@ constexpr int kMaxCoef = 48 * 16;
 
 // Radial table: per pair p = t_i*S + t_j: [KMU] (scal, shift) pairs then the
 // pair scale; shared_xi means every mu of a pair uses the same (scal, shift).
+// kind: 0 Chebyshev basis of the tanh map, 1 of the rational map, 2 Laguerre
+// basis of log(1 + r / rho) (kRadial* in sh_math.cuh; shift holds rho).
 struct RadialSetup {
   int species;
   int kmu;
   int rb;
-  int rational;
+  int kind;
   int shared_xi;
   int pair_stride;  // floats per pair in the table
   double rc;
@@ -48,7 +50,8 @@ struct EdgeArgs {
   T* gate_adj;               // [Kmu][N] dE/dh accumulated by k_force (atomics)
   // c[mu][n] (uniform across lanes), then, when 2 kmu rb <= kMaxCoef, the
   // derivative series d[mu][n] at offset kmu rb:
-  // sum_n c[mu][n] T_n'(xi) = sum_n d[mu][n] T_n(xi), d[mu][rb-1] = 0.
+  // sum_n c[mu][n] P_n'(x) = sum_n d[mu][n] P_n(x), d[mu][rb-1] = 0, for the
+  // basis polynomials P_n of the kind (Chebyshev T_n or Laguerre L_n).
   // One array keeps the FP32 kernel parameters under 4 KB, where every
   // coefficient is an immediate constant-bank operand.
   T coef[kMaxCoef];

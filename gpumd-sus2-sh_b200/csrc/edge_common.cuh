@@ -12,20 +12,20 @@ namespace edge {
 constexpr int kCenterCode = 62;  // image (0,0,0) in base-5 codes
 
 // Radial coefficient X (c[mu][n], then the derivative series), whether all
-// radial functions of a pair share one radial argument, and whether the
-// radial map is the rational one: from the kernel parameters, or, in a build
-// specialised to one model, compiled in (model_coef() table and the
-// SUS2_MODEL_SHARED_XI / SUS2_MODEL_RATIONAL constants), so every coefficient
-// of an unrolled loop is an immediate operand and the per-edge tests of the
-// radial setup disappear.
+// radial functions of a pair share one radial argument, and the radial basis
+// kind: from the kernel parameters, or, in a build specialised to one model,
+// compiled in (model_coef() table and the SUS2_MODEL_SHARED_XI /
+// SUS2_MODEL_RADIAL_KIND constants), so every coefficient of an unrolled loop
+// is an immediate operand and the per-edge tests of the radial setup
+// disappear.
 #ifdef SUS2_MODEL_COEF
 #define SUS2_COEF(a, X) (::sus2sh::edge::model_coef(X))
 #define SUS2_SHARED_XI(a) (SUS2_MODEL_SHARED_XI != 0)
-#define SUS2_RATIONAL(a) (SUS2_MODEL_RATIONAL != 0)
+#define SUS2_RADIAL_KIND(a) (SUS2_MODEL_RADIAL_KIND)
 #else
 #define SUS2_COEF(a, X) ((a).coef[X])
 #define SUS2_SHARED_XI(a) ((a).rs.shared_xi != 0)
-#define SUS2_RATIONAL(a) ((a).rs.rational != 0)
+#define SUS2_RADIAL_KIND(a) ((a).rs.kind)
 #endif
 
 __device__ __forceinline__ int type_of(const double4& p) {
@@ -87,54 +87,58 @@ __device__ __forceinline__ Edge<double> make_edge<double>(double dx, double dy, 
 }
 
 // R_mu for every mu; the pair table row holds KMU (scal, shift) pairs then
-// the LK pair scale.
+// the LK pair scale.  R_mu = s_pair (r - rc)^2 env(x) sum_n c[mu][n] P_n(x)
+// with x the kind's argument (radial_arg).
 template <typename T, int KMU, int RB>
 __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __restrict__ row,
                                               const Edge<T>& e, T* R) {
   const T f = row[2 * KMU] * e.dr * e.dr;
-  const bool rational = SUS2_RATIONAL(a);
+  const int kind = SUS2_RADIAL_KIND(a);
   if (SUS2_SHARED_XI(a)) {
-    T xi, dxi;
-    radial_map<T>(T(0.5) * row[0] * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
+    T x, dx, env, denv;
+    radial_arg<T>(kind, row[0], row[1], e.rd, x, dx, env, denv);
     T t[RB];
-    chebyshev<RB>(xi, t);
+    radial_poly<RB>(kind, x, t);
+    const T fe = f * env;
 #pragma unroll
     for (int mu = 0; mu < KMU; ++mu) {
       T s = T(0);
 #pragma unroll
       for (int n = 0; n < RB; ++n) s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
-      R[mu] = f * s;
+      R[mu] = fe * s;
     }
   } else {
 #pragma unroll
     for (int mu = 0; mu < KMU; ++mu) {
-      T xi, dxi;
-      radial_map<T>(T(0.5) * row[2 * mu] * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational,
-                    xi, dxi);
+      T x, dx, env, denv;
+      radial_arg<T>(kind, row[2 * mu], row[2 * mu + 1], e.rd, x, dx, env, denv);
       T t[RB];
-      chebyshev<RB>(xi, t);
+      radial_poly<RB>(kind, x, t);
       T s = T(0);
 #pragma unroll
       for (int n = 0; n < RB; ++n) s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
-      R[mu] = f * s;
+      R[mu] = f * env * s;
     }
   }
 }
 
+// R_mu and dR_mu/dr: with f = s_pair (r - rc)^2, s = sum c P_n(x),
+// sd = sum c P_n'(x): dR = (df + f denv/env) env s + f env (dx/dr) sd.
 template <typename T, int KMU, int RB>
 __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T* __restrict__ row,
                                                    const Edge<T>& e, T* R, T* dR) {
   const T ps = row[2 * KMU];
   const T f = ps * e.dr * e.dr;
   const T df = T(2) * ps * e.dr;
-  const bool rational = SUS2_RATIONAL(a);
+  const int kind = SUS2_RADIAL_KIND(a);
   if (SUS2_SHARED_XI(a)) {
-    const T half_scal = T(0.5) * row[0];
-    T xi, dxi;
-    radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
-    const T g = f * half_scal * dxi;  // f * d xi / dr
+    T x, dx, env, denv;
+    radial_arg<T>(kind, row[0], row[1], e.rd, x, dx, env, denv);
+    const T fe = f * env;
+    const T dfe = env * fma(f, denv, df);
+    const T g = fe * dx;  // f env dx/dr
     T t[RB], dt[RB];
-    chebyshev_d<RB>(xi, t, dt);
+    radial_poly_d<RB>(kind, x, t, dt);
 #pragma unroll
     for (int mu = 0; mu < KMU; ++mu) {
       T s = T(0), sd = T(0);
@@ -143,25 +147,24 @@ __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T
         s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
         sd = fma(SUS2_COEF(a, mu * RB + n), dt[n], sd);
       }
-      R[mu] = f * s;
-      dR[mu] = df * s + g * sd;
+      R[mu] = fe * s;
+      dR[mu] = dfe * s + g * sd;
     }
   } else {
 #pragma unroll
     for (int mu = 0; mu < KMU; ++mu) {
-      const T half_scal = T(0.5) * row[2 * mu];
-      T xi, dxi;
-      radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi, dxi);
+      T x, dx, env, denv;
+      radial_arg<T>(kind, row[2 * mu], row[2 * mu + 1], e.rd, x, dx, env, denv);
       T t[RB], dt[RB];
-      chebyshev_d<RB>(xi, t, dt);
+      radial_poly_d<RB>(kind, x, t, dt);
       T s = T(0), sd = T(0);
 #pragma unroll
       for (int n = 0; n < RB; ++n) {
         s = fma(SUS2_COEF(a, mu * RB + n), t[n], s);
         sd = fma(SUS2_COEF(a, mu * RB + n), dt[n], sd);
       }
-      R[mu] = f * s;
-      dR[mu] = df * s + f * half_scal * dxi * sd;
+      R[mu] = f * env * s;
+      dR[mu] = env * (fma(f, denv, df) * s + f * dx * sd);
     }
   }
 }

@@ -48,9 +48,9 @@ long long global_bytes_of(const std::string& log) {
 
 // The coefficient table as an exact hexadecimal float initializer of
 // model_coef(), declared ahead of the kernel headers that call it.
-std::string coef_prelude(const std::vector<float>& coef, bool shared_xi, bool rational) {
+std::string coef_prelude(const std::vector<float>& coef, bool shared_xi, int radial_kind) {
   std::string s = "#define SUS2_MODEL_COEF 1\n#define SUS2_MODEL_SHARED_XI " + std::to_string(shared_xi ? 1 : 0) +
-                  "\n#define SUS2_MODEL_RATIONAL " + std::to_string(rational ? 1 : 0) +
+                  "\n#define SUS2_MODEL_RADIAL_KIND " + std::to_string(radial_kind) +
                   "\nnamespace sus2sh {\nnamespace edge {\n"
                   "__device__ __forceinline__ float model_coef(int i) {\n  constexpr float c[" +
                   std::to_string(std::max<size_t>(coef.size(), 1)) + "] = {";
@@ -69,7 +69,7 @@ std::string coef_prelude(const std::vector<float>& coef, bool shared_xi, bool ra
 // compiled in when coef is given.
 std::shared_ptr<EdgeJitBinary> build(bool fp32, int l, int k, int rb, const std::vector<int>& blocks, bool gate,
                                      const std::vector<float>* coef, int which = 3, bool shared_xi = true,
-                                     bool rational = false) {
+                                     int radial_kind = 0) {
   const auto t0 = std::chrono::steady_clock::now();
   const std::string T = fp32 ? "float" : "double";
   const std::string shape = T + ", " + std::to_string(l) + ", " + std::to_string(k) + ", " + std::to_string(rb);
@@ -81,7 +81,7 @@ std::shared_ptr<EdgeJitBinary> build(bool fp32, int l, int k, int rb, const std:
   const std::string basic_gate_expr = "&sus2sh::edge::k_basic<" + shape + ", 128, true>";
   const std::string force_gate_expr = "&sus2sh::edge::k_force<" + shape + ", 128, true>";
   const std::string src =
-      (coef ? coef_prelude(*coef, shared_xi, rational) : std::string()) + "#include \"edge_kernels.cuh\"\n";
+      (coef ? coef_prelude(*coef, shared_xi, radial_kind) : std::string()) + "#include \"edge_kernels.cuh\"\n";
   nvrtcProgram prog;
   if (nvrtcCreateProgram(&prog, src.c_str(), "sus2sh_edge.cu", kJitHeaderCount, kJitHeaderSources,
                          kJitHeaderNames) != NVRTC_SUCCESS)
@@ -170,14 +170,14 @@ std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, 
 
 std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k_max, int rb,
                                                                 const std::vector<float>& coef, bool shared_xi,
-                                                                bool rational) {
+                                                                int radial_kind) {
   // FNV-1a of the table's bytes
   unsigned long long h = 1469598103934665603ull;
   const unsigned char* b = reinterpret_cast<const unsigned char*>(coef.data());
   for (size_t i = 0; i < coef.size() * sizeof(float); ++i) h = (h ^ b[i]) * 1099511628211ull;
   const std::string key = shape_key(true, l_max, k_max, rb, 0, false) + "/model/" + std::to_string(coef.size()) +
                           "/" + std::to_string(h) + (shared_xi ? "/shared" : "/per-function") +
-                          (rational ? "/rational" : "/tanh");
+                          "/kind" + std::to_string(radial_kind);
   return cached(key, [&] {
     const auto t0 = std::chrono::steady_clock::now();
     const int blocks[3] = {64, 128, 256};
@@ -187,7 +187,7 @@ std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k
     for (int p = 0; p < 6; ++p)
       pool.emplace_back([&, p] {
         try {
-          part[p] = build(true, l_max, k_max, rb, {blocks[p / 2]}, false, &coef, p % 2 ? 2 : 1, shared_xi, rational);
+          part[p] = build(true, l_max, k_max, rb, {blocks[p / 2]}, false, &coef, p % 2 ? 2 : 1, shared_xi, radial_kind);
         } catch (const std::exception& e) {
           failure[p] = e.what();
         }

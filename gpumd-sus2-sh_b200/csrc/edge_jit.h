@@ -37,12 +37,12 @@ std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, 
 // FP32 k_basic / k_force of one model at 64, 128 and 256 threads per CTA,
 // with `coef` (the kernels' coefficient table: c[mu][n], then the derivative
 // series when it fits, as EdgeArgs::coef holds them), whether the radial
-// functions of a pair share one argument, and the radial map compiled in:
+// functions of a pair share one argument, and the radial basis kind compiled in:
 // six NVRTC programs built on parallel host threads.  Cached per process by
 // shape, table and radial setup.
 std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k_max, int rb,
                                                                 const std::vector<float>& coef, bool shared_xi,
-                                                                bool rational);
+                                                                int radial_kind);
 
 // Module of one compiled shape, loaded into the current context.
 class EdgeJitModule {

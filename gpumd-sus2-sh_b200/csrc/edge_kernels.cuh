@@ -185,20 +185,23 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
     if (r2 >= rc2) continue;
     const Edge<T> e = make_edge<T>(dx, dy, dz, r2, rc, rc2);
     const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
-    // R_mu = f s_mu, dR_mu = df s_mu + f fac sd_mu with f = s_pair (r-rc)^2,
-    // s_mu = sum_n c[mu][n] T_n, sd_mu = sum_n d[mu][n] T_n (derivative series);
-    // the common factors are applied after the contractions below
+    // R_mu = fS s_mu, dR_mu = dfS s_mu + fS fac sd_mu.  Shared argument: fS =
+    // f env, dfS = env (df + f denv/env), fac = dx/dr, s_mu = sum_n c[mu][n]
+    // P_n, sd_mu = sum_n d[mu][n] P_n (derivative series).  Per-mu arguments:
+    // fS = f, dfS = df, fac = 1, with env and dx/dr folded into s_mu, sd_mu.
+    // f = s_pair (r-rc)^2; the common factors are applied after the
+    // contractions below.
     const T ps = row[2 * KMU];
     const T f = ps * e.dr * e.dr;
     const T df = T(2) * ps * e.dr;
-    const bool rational = SUS2_RATIONAL(a);
-    T t[RB], fac = T(1);
+    const int kind = SUS2_RADIAL_KIND(a);
+    T t[RB], fac = T(1), fS = f, dfS = df, xarg = T(0);
     if (SUS2_SHARED_XI(a)) {
-      const T half_scal = T(0.5) * row[0];
-      T xi, dxi;
-      radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
-      fac = half_scal * dxi;
-      chebyshev<RB>(xi, t);
+      T env, denv;
+      radial_arg<T>(kind, row[0], row[1], e.rd, xarg, fac, env, denv);
+      fS = f * env;
+      dfS = env * fma(f, denv, df);
+      radial_poly<RB>(kind, xarg, t);
     }
     T P[C];
     sh_poly<L>(e.ux, e.uy, e.uz, P);
@@ -212,13 +215,10 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const int mu = k * (L + 1) + l;
-        T scale = T(1);
+        T scale = T(1), env = T(1), denv = T(0);
         if (!SUS2_SHARED_XI(a)) {
-          const T half_scal = T(0.5) * row[2 * mu];
-          T xi, dxi;
-          radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi, dxi);
-          scale = half_scal * dxi;
-          chebyshev<RB>(xi, t);
+          radial_arg<T>(kind, row[2 * mu], row[2 * mu + 1], e.rd, xarg, scale, env, denv);
+          radial_poly<RB>(kind, xarg, t);
         }
         T v = T(0), d = T(0);
         if constexpr (2 * KMU * RB <= kMaxCoef) {
@@ -230,21 +230,26 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
           }
         } else {
           T tt[RB], dt[RB];
-          chebyshev_d<RB>(t[RB > 1 ? 1 : 0], tt, dt);
+          radial_poly_d<RB>(kind, xarg, tt, dt);
 #pragma unroll
           for (int n = 0; n < RB; ++n) {
             v = fma(SUS2_COEF(a, mu * RB + n), t[n], v);
             d = fma(SUS2_COEF(a, mu * RB + n), dt[n], d);
           }
         }
-        sk[k] = v;
-        sdk[k] = scale * d;
+        if (SUS2_SHARED_XI(a)) {
+          sk[k] = v;
+          sdk[k] = d;
+        } else {
+          sk[k] = env * v;
+          sdk[k] = env * fma(denv, v, scale * d);
+        }
         if constexpr (GATE) {
           T p = T(0);
 #pragma unroll
           for (int m = 0; m <= 2 * l; ++m) p = fma(g[k * C + l * l + m], P[l * l + m], p);
           const size_t at = static_cast<size_t>(mu) * a.N + j;
-          atomicAdd(a.gate_adj + at, p * (f * v) * a.gate_deriv[at]);
+          atomicAdd(a.gate_adj + at, p * (fS * sk[k]) * a.gate_deriv[at]);
           const T gm = a.gate_mult[at];
           sk[k] *= gm;
           sdk[k] *= gm;
@@ -264,11 +269,11 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
       }
     }
     // radial part s = dE/dr along u; tangential part f (V - (u.V) u) / r
-    const T s = df * sG + (f * fac) * sH;
+    const T s = dfS * sG + (fS * fac) * sH;
     T vx, vy, vz;
     sh_poly_grad_contract<L>(e.ux, e.uy, e.uz, Gt, vx, vy, vz);
     const T uv = e.ux * vx + e.uy * vy + e.uz * vz;
-    const T ft = f * e.rinv;
+    const T ft = fS * e.rinv;
     const T dEx = s * e.ux + (vx - uv * e.ux) * ft;
     const T dEy = s * e.uy + (vy - uv * e.uy) * ft;
     const T dEz = s * e.uz + (vz - uv * e.uz) * ft;

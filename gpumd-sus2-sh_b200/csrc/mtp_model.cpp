@@ -297,12 +297,15 @@ HostModel load_model(const std::string& path) {
   m.radial_basis_type = value_of(text, "radial_basis_type =");
   if (m.radial_basis_type == "RBChebyshev_sss" || m.radial_basis_type == "RBChebyshev_sss_lmp") {
     m.radial_map = RadialMap::Tanh;
+  } else if (m.radial_basis_type == "RBLaguerre_log1p" || m.radial_basis_type == "RBLaguerre_log1p_lmp") {
+    m.radial_map = RadialMap::LaguerreLog1p;
   } else if (m.radial_basis_type == "RBChebyshev_sss_rational" ||
              m.radial_basis_type == "RBChebyshev_sss_rational_lmp") {
     m.radial_map = RadialMap::Rational;
   } else {
     throw InputError("Unsupported SUS2_SH radial_basis_type: " + m.radial_basis_type +
-                     ". Supported: RBChebyshev_sss[_lmp], RBChebyshev_sss_rational[_lmp].");
+                     ". Supported: RBChebyshev_sss[_lmp], RBLaguerre_log1p[_lmp], "
+                     "RBChebyshev_sss_rational[_lmp].");
   }
   m.rc = double_of(text, "max_dist =");
   m.zbl_enabled = contains(text, "zbl_enabled =") && parse_bool(value_of(text, "zbl_enabled ="), "zbl_enabled =");

@@ -26,7 +26,9 @@ struct Product {
   double coeff = 0.0;
 };
 
-enum class RadialMap { Tanh = 0, Rational = 1 };
+// The radial basis of the file (kRadial* kinds of sh_math.cuh): Chebyshev of
+// the tanh map, of the rational map, or Laguerre of log(1 + r / rho).
+enum class RadialMap { Tanh = 0, Rational = 1, LaguerreLog1p = 2 };
 
 enum class GateMode { MuBodyLinearCombo = 1, MuScalarFull = 2 };
 

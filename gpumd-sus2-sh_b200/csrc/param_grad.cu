@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(128)
     const int row_i = type_of(pi) * a.rs.species;
     const int cnt = min(a.ncount[i], a.cap);
     const double rc = a.rs.rc, rc2 = rc * rc;
-    const bool rational = a.rs.rational != 0;
+    const int kind = a.rs.kind;
     for (int n = 0; n < cnt; ++n) {
       const int w = __ldg(a.nbr + static_cast<size_t>(n) * a.N + i);
       const int j = w & 0xFFFFFF;
@@ -231,14 +231,20 @@ __global__ void __launch_bounds__(128)
       const T fc = e.dr * e.dr, dfc = T(2) * e.dr;
       T Y[C], Yd[C];
       harmonics_and_tangent<T, L>(e, tx, ty, tz, ud, Y, Yd);
-      // radial basis of the pair: once per edge when every mu shares (scal, shift)
-      T t0[RB], dt0[RB], xr0 = T(0);
+      // radial basis of the pair, once per edge when every mu shares (scal,
+      // shift): phi_n = env P_n(x) and its r-derivative relative to fc,
+      // dphi_n = (denv/env) phi_n + env (dx/dr) P_n'(x), so that the basis
+      // function fc phi_n has derivative dfc phi_n + fc dphi_n
+      T t0[RB], dt0[RB];
       if (a.rs.shared_xi) {
-        const T half_scal = T(0.5) * row[0];
-        T xi, dxi;
-        radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[1])), rational, xi, dxi);
-        chebyshev_d<RB>(xi, t0, dt0);
-        xr0 = fc * half_scal * dxi;
+        T x, dx, env, denv;
+        radial_arg<T>(kind, row[0], row[1], e.rd, x, dx, env, denv);
+        radial_poly_d<RB>(kind, x, t0, dt0);
+#pragma unroll
+        for (int q = 0; q < RB; ++q) {
+          t0[q] *= env;
+          dt0[q] = fma(denv, t0[q], env * dx * dt0[q]);
+        }
       }
 #pragma unroll
       for (int k = 0; k < K; ++k)
@@ -252,26 +258,27 @@ __global__ void __launch_bounds__(128)
             Bm = fma(be[k * C + l * l + m], Y[l * l + m], Bm);
             Cm = fma(be[k * C + l * l + m], Yd[l * l + m], Cm);
           }
-          T t[RB], dt[RB], xr;  // xr = fc * d xi / dr
+          T t[RB], dt[RB];
           if (a.rs.shared_xi) {
 #pragma unroll
             for (int q = 0; q < RB; ++q) {
               t[q] = t0[q];
               dt[q] = dt0[q];
             }
-            xr = xr0;
           } else {
-            const T half_scal = T(0.5) * row[2 * mu];
-            T xi, dxi;
-            radial_map<T>(half_scal * static_cast<T>(e.rd - static_cast<double>(row[2 * mu + 1])), rational, xi,
-                          dxi);
-            chebyshev_d<RB>(xi, t, dt);
-            xr = fc * half_scal * dxi;
+            T x, dx, env, denv;
+            radial_arg<T>(kind, row[2 * mu], row[2 * mu + 1], e.rd, x, dx, env, denv);
+            radial_poly_d<RB>(kind, x, t, dt);
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+              t[q] *= env;
+              dt[q] = fma(denv, t[q], env * dx * dt[q]);
+            }
           }
           const T p1 = ps * fc * (A - Cm);
           const T p2 = ps * ud * Bm;
 #pragma unroll
-          for (int q = 0; q < RB; ++q) acc[mu * RB + q] += p1 * t[q] - p2 * (dfc * t[q] + xr * dt[q]);
+          for (int q = 0; q < RB; ++q) acc[mu * RB + q] += p1 * t[q] - p2 * (dfc * t[q] + fc * dt[q]);
         }
     }
   }

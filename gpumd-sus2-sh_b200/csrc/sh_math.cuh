@@ -417,6 +417,37 @@ SUS2_HD void radial_map(T z, bool rational, T& xi, T& dxi_dz) {
   }
 }
 
+// Radial basis kinds (RadialSetup::kind): the Chebyshev basis of the tanh map
+// (RBChebyshev_sss), of the rational map (RBChebyshev_sss_rational), and the
+// Laguerre basis of u = scal log(1 + r / rho) under the envelope exp(-u/2)
+// (RBLaguerre_log1p, src/force/sus2_sh.cu:363-374,3299-3352: the reference's
+// phi_n = (r - rc)^2 exp(-u/2) L_n(u), rho = max(shift, 1e-8)).
+constexpr int kRadialTanh = 0;
+constexpr int kRadialRational = 1;
+constexpr int kRadialLaguerre = 2;
+constexpr double kLaguerreMinRho = 1.0e-8;
+
+// The polynomial argument x of one radial function at distance r (FP64), with
+// dx/dr, the envelope env (1 for the Chebyshev kinds) and (d env / dr) / env.
+template <typename T>
+SUS2_HD void radial_arg(int kind, T scal, T shift, double r, T& x, T& dx_dr, T& env, T& denv_rel) {
+  if (kind == kRadialLaguerre) {
+    const double rho = static_cast<double>(shift) > kLaguerreMinRho ? static_cast<double>(shift) : kLaguerreMinRho;
+    const T u = scal * log1p(static_cast<T>(r / rho));
+    x = u;
+    dx_dr = scal / static_cast<T>(rho + r);
+    env = exp(T(-0.5) * u);
+    denv_rel = T(-0.5) * dx_dr;
+  } else {
+    const T half = T(0.5) * scal;
+    T dxi;
+    radial_map<T>(half * static_cast<T>(r - static_cast<double>(shift)), kind == kRadialRational, x, dxi);
+    dx_dr = half * dxi;
+    env = T(1);
+    denv_rel = T(0);
+  }
+}
+
 // Chebyshev T_n(xi), n < RB.
 template <int RB, typename T>
 SUS2_HD void chebyshev(T xi, T* t) {
@@ -440,6 +471,46 @@ SUS2_HD void chebyshev_d(T xi, T* t, T* dt) {
     t[n] = T(2) * xi * t[n - 1] - t[n - 2];
     dt[n] = T(2) * (t[n - 1] + xi * dt[n - 1]) - dt[n - 2];
   }
+}
+
+// Laguerre L_n(u), n < RB: L_0 = 1, L_1 = 1 - u,
+// (n+1) L_{n+1} = (2n+1-u) L_n - n L_{n-1}.
+template <int RB, typename T>
+SUS2_HD void laguerre(T u, T* t) {
+  t[0] = T(1);
+  if (RB > 1) t[1] = T(1) - u;
+#pragma unroll
+  for (int n = 1; n + 1 < RB; ++n)
+    t[n + 1] = ((T(2 * n + 1) - u) * t[n] - T(n) * t[n - 1]) * T(1.0 / (n + 1));
+}
+
+// L_n(u) and dL_n/du, n < RB.
+template <int RB, typename T>
+SUS2_HD void laguerre_d(T u, T* t, T* dt) {
+  t[0] = T(1);
+  dt[0] = T(0);
+  if (RB > 1) {
+    t[1] = T(1) - u;
+    dt[1] = T(-1);
+  }
+#pragma unroll
+  for (int n = 1; n + 1 < RB; ++n) {
+    const T inv = T(1.0 / (n + 1));
+    t[n + 1] = ((T(2 * n + 1) - u) * t[n] - T(n) * t[n - 1]) * inv;
+    dt[n + 1] = ((T(2 * n + 1) - u) * dt[n] - t[n] - T(n) * dt[n - 1]) * inv;
+  }
+}
+
+// The basis polynomials of a kind at argument x (and their x-derivatives).
+template <int RB, typename T>
+SUS2_HD void radial_poly(int kind, T x, T* t) {
+  if (kind == kRadialLaguerre) laguerre<RB>(x, t);
+  else chebyshev<RB>(x, t);
+}
+template <int RB, typename T>
+SUS2_HD void radial_poly_d(int kind, T x, T* t, T* dt) {
+  if (kind == kRadialLaguerre) laguerre_d<RB>(x, t, dt);
+  else chebyshev_d<RB>(x, t, dt);
 }
 
 }  // namespace sus2sh

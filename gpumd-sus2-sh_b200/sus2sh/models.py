@@ -29,13 +29,15 @@ PRESETS = {
 
 def write_model(path: str, species=2, l_max=3, k_max=3, body_order=4, rb_size=8, r_min=2.0, rc=5.0,
                 rational=0, shift=(-3.5, -5.0), radial_sigma=0.1, moment_sigma=0.01, scal=1.0,
-                rshift=-1.0, seed=0, body_l_max=None) -> str:
+                rshift=-1.0, seed=0, body_l_max=None, laguerre=False) -> str:
+    """rational: 0 Chebyshev-sss, 1 its rational map; laguerre=True writes the
+    Laguerre-log1p basis (rshift is then rho)."""
     lib = _lib.load_tools()
     sh = (ctypes.c_double * species)(*shift)
     bl = (ctypes.c_int * len(body_l_max))(*body_l_max) if body_l_max else None
     _lib.check_tools(lib.sus2sh_write_synthetic_model(
         path.encode(), species, l_max, k_max, body_order, ctypes.cast(bl, ctypes.c_void_p) if bl else None,
-        len(body_l_max) if body_l_max else 0, rb_size, r_min, rc, rational,
+        len(body_l_max) if body_l_max else 0, rb_size, r_min, rc, 2 if laguerre else rational,
         ctypes.cast(sh, ctypes.c_void_p), radial_sigma, moment_sigma, scal, rshift,
         ctypes.c_ulonglong(seed)), "sus2sh_write_synthetic_model")
     return path

@@ -46,13 +46,13 @@ struct SynthSpec {
   int rb_size = 8;
   double r_min = 2.0;
   double rc = 5.0;
-  int rational = 0;
+  int rational = 0;                  // radial basis: 0 Chebyshev-sss, 1 its rational map, 2 Laguerre-log1p
   std::vector<int> body_l_max_list;  // empty: none written
   std::vector<double> shift;         // [S] site energy shifts
   double radial_sigma = 0.1;
   double moment_sigma = 0.01;
   double scal = 1.0;     // radial tanh scale
-  double rshift = -1.0;  // radial shift; <0 -> (r_min+rc)/2
+  double rshift = -1.0;  // radial shift (Laguerre: rho); <0 -> (r_min+rc)/2
   double radial_type_coeff = 1.0;
   unsigned long long seed = 0;
 };
@@ -90,7 +90,8 @@ void write_synthetic_model(const std::string& path, const SynthSpec& sp) {
       std::fprintf(f, "%s%d", i ? ", " : "", sp.body_l_max_list[i]);
     std::fprintf(f, "}\n");
   }
-  std::fprintf(f, "radial_basis_type = %s\n", sp.rational ? "RBChebyshev_sss_rational" : "RBChebyshev_sss");
+  std::fprintf(f, "radial_basis_type = %s\n",
+               sp.rational == 2 ? "RBLaguerre_log1p" : (sp.rational ? "RBChebyshev_sss_rational" : "RBChebyshev_sss"));
   std::fprintf(f, "\tmin_dist = %.17g\n\tmax_dist = %.17g\n", sp.r_min, sp.rc);
   std::fprintf(f, "\tradial_basis_size = %d\n\tradial_funcs_count = %d\n", sp.rb_size, kmu);
   list("shift_coeffs", sp.shift);

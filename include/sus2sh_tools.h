@@ -21,6 +21,8 @@ const char* sus2sh_tools_last_error(void);
  * radial ~ N(0, radial_sigma), moment weights ~ N(0, moment_sigma),
  * species_coeffs = 1, every radial (scal, shift) = (scal, rshift) with
  * rshift < 0 meaning (r_min + rc)/2, radial type coefficients = 1.
+ * rational selects the radial basis: 0 RBChebyshev_sss, 1
+ * RBChebyshev_sss_rational, 2 RBLaguerre_log1p (shift is then rho).
  * body_l_max may be NULL (n_body_l_max = 0). */
 int sus2sh_write_synthetic_model(const char* path, int species, int l_max, int k_max,
                                  int body_order, const int* body_l_max, int n_body_l_max,

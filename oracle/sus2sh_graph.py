@@ -564,6 +564,8 @@ class MtpModel:
     scalar_body: list = None
     # two-layer mu-body gate (sus2_sh.cu:2153-2268, metadata :2412-2478)
     gate: dict = None
+    # RBLaguerre_log1p[_lmp] radial basis (sus2_sh.cu:363-374,3299-3352)
+    laguerre: bool = False
 
 
 def load_mtp(path: str) -> MtpModel:
@@ -585,8 +587,11 @@ def load_mtp(path: str) -> MtpModel:
     if "sh_parity =" in text and _after(text, "sh_parity =") != "even":
         raise MtpError("SUS2_SH GPUMD backend currently supports even parity models only.")
     rtype = _after(text, "radial_basis_type =")
+    laguerre = False
     if rtype in ("RBChebyshev_sss", "RBChebyshev_sss_lmp"):
         rational = False
+    elif rtype in ("RBLaguerre_log1p", "RBLaguerre_log1p_lmp"):
+        rational, laguerre = False, True
     elif rtype in ("RBChebyshev_sss_rational", "RBChebyshev_sss_rational_lmp"):
         rational = True
     else:
@@ -676,7 +681,7 @@ def load_mtp(path: str) -> MtpModel:
     except ValueError as exc:
         raise MtpError(str(exc)) from exc
     model = MtpModel(S, L, K, body, rtype, rational, max_dist, rb, kmu, M, Bb, nsc, scaling,
-                     blmax, shift, scal, species, moment, mapping, basic, prods, radial, rtc)
+                     blmax, shift, scal, species, moment, mapping, basic, prods, radial, rtc, laguerre=laguerre)
     gate = _parse_gate(text, K, kmu, rb, S) if ("two_layer_gate_enabled =" in text
                                                 and _bool(_after(text, "two_layer_gate_enabled ="))) else None
     if "sh_scalar_info_count =" in text:

@@ -29,7 +29,8 @@
 #endif
 
 typedef struct {
-  int S, L, K, rb, kmu, M, nbasic, nscalar, nprod, rational;
+  int S, L, K, rb, kmu, M, nbasic, nscalar, nprod;
+  int kind; /* radial basis: 0 Chebyshev of tanh, 1 Chebyshev of the rational map, 2 Laguerre of log1p */
   double rc;
   const double* radial;   /* [kmu][rb] */
   const double* scal;     /* [S*S][kmu] */
@@ -201,7 +202,11 @@ void oracle_real_sh(int L, double x, double y, double z, double* Y, double* dY) 
   }
 }
 
-/* R_mu and dR_mu/dr for one pair (FP64). */
+/* R_mu and dR_mu/dr for one pair (FP64).  Chebyshev kinds
+   (sus2_sh.cu:3171-3297): R = f sum_n c_n T_n(xi), xi = tanh(z) or
+   z / sqrt(1 + z^2), z = scal (r - shift) / 2.  Laguerre kind
+   (sus2_sh.cu:3299-3352): R = f exp(-u/2) sum_n c_n L_n(u),
+   u = scal log(1 + r / rho), rho = max(shift, 1e-8).  f = s_pair (r - rc)^2. */
 void oracle_radial(const OracleModel* m, int pair, double r, double* R, double* dR) {
   const double dr = r - m->rc;
   const double f = m->pscale[pair] * dr * dr;
@@ -209,33 +214,52 @@ void oracle_radial(const OracleModel* m, int pair, double r, double* R, double* 
   double t[32], dt[32];
   for (int mu = 0; mu < m->kmu; ++mu) {
     const double sc = m->scal[pair * m->kmu + mu];
-    const double z = 0.5 * sc * (r - m->rshift[pair * m->kmu + mu]);
-    double xi, dxdr;
-    if (m->rational) {
-      const double q = 1.0 / sqrt(1.0 + z * z);
-      xi = z * q;
-      dxdr = 0.5 * sc * q * q * q;
+    const double sh = m->rshift[pair * m->kmu + mu];
+    double x, dxdr, env = 1.0, denv = 0.0;
+    if (m->kind == 2) {
+      const double rho = sh > 1.0e-8 ? sh : 1.0e-8;
+      x = sc * log1p(r / rho);
+      dxdr = sc / (rho + r);
+      env = exp(-0.5 * x);
+      denv = -0.5 * dxdr * env;
+      t[0] = 1.0;
+      dt[0] = 0.0;
+      if (m->rb > 1) {
+        t[1] = 1.0 - x;
+        dt[1] = -1.0;
+      }
+      for (int n = 1; n + 1 < m->rb; ++n) {
+        t[n + 1] = ((2.0 * n + 1.0 - x) * t[n] - n * t[n - 1]) / (n + 1.0);
+        dt[n + 1] = ((2.0 * n + 1.0 - x) * dt[n] - t[n] - n * dt[n - 1]) / (n + 1.0);
+      }
     } else {
-      xi = tanh(z);
-      dxdr = 0.5 * sc * (1.0 - xi * xi);
-    }
-    t[0] = 1.0;
-    dt[0] = 0.0;
-    if (m->rb > 1) {
-      t[1] = xi;
-      dt[1] = 1.0;
-    }
-    for (int n = 2; n < m->rb; ++n) {
-      t[n] = 2.0 * xi * t[n - 1] - t[n - 2];
-      dt[n] = 2.0 * t[n - 1] + 2.0 * xi * dt[n - 1] - dt[n - 2];
+      const double z = 0.5 * sc * (r - sh);
+      if (m->kind == 1) {
+        const double q = 1.0 / sqrt(1.0 + z * z);
+        x = z * q;
+        dxdr = 0.5 * sc * q * q * q;
+      } else {
+        x = tanh(z);
+        dxdr = 0.5 * sc * (1.0 - x * x);
+      }
+      t[0] = 1.0;
+      dt[0] = 0.0;
+      if (m->rb > 1) {
+        t[1] = x;
+        dt[1] = 1.0;
+      }
+      for (int n = 2; n < m->rb; ++n) {
+        t[n] = 2.0 * x * t[n - 1] - t[n - 2];
+        dt[n] = 2.0 * t[n - 1] + 2.0 * x * dt[n - 1] - dt[n - 2];
+      }
     }
     double s = 0.0, sd = 0.0;
     for (int n = 0; n < m->rb; ++n) {
       s += m->radial[mu * m->rb + n] * t[n];
       sd += m->radial[mu * m->rb + n] * dt[n];
     }
-    R[mu] = f * s;
-    if (dR) dR[mu] = df * s + f * sd * dxdr;
+    R[mu] = f * env * s;
+    if (dR) dR[mu] = (df * env + f * denv) * s + f * env * sd * dxdr;
   }
 }
 

@@ -36,7 +36,7 @@ def build_oracle(force: bool = False) -> str:
 
 class _COracleModel(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in
-                ("S", "L", "K", "rb", "kmu", "M", "nbasic", "nscalar", "nprod", "rational")] + [
+                ("S", "L", "K", "rb", "kmu", "M", "nbasic", "nscalar", "nprod", "kind")] + [
         ("rc", ctypes.c_double),
         ("radial", ctypes.c_void_p), ("scal", ctypes.c_void_p), ("rshift", ctypes.c_void_p),
         ("pscale", ctypes.c_void_p), ("basic_mu", ctypes.c_void_p), ("basic_y", ctypes.c_void_p),
@@ -97,7 +97,7 @@ class OracleArrays:
         ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
         return _COracleModel(m.species_count, m.sh_l_max, m.sh_k_max, m.rb_size, m.radial_funcs_count,
                              m.alpha_moments_count, m.alpha_basic_count, len(self.map), len(self.prod_c),
-                             1 if m.rational else 0, m.max_dist,
+                             2 if m.laguerre else (1 if m.rational else 0), m.max_dist,
                              ptr(self.radial), ptr(self.scal), ptr(self.rshift), ptr(self.pscale),
                              ptr(self.basic_mu), ptr(self.basic_y), ptr(self.prod_l), ptr(self.prod_r),
                              ptr(self.prod_t), ptr(self.prod_c), ptr(self.map), ptr(self.w),
@@ -325,13 +325,21 @@ def python_efs(m: MtpModel, h, pbc, types, pos, reach=2):
         for mu in range(kmu):
             off = 2 * mu * S * S + S * zi + zj
             sc, sh = m.scal_coeffs[off], m.scal_coeffs[off + S * S]
-            z = 0.5 * sc * (r - sh)
-            xi = z / math.sqrt(1 + z * z) if m.rational else math.tanh(z)
-            t = [1.0, xi]
-            for n in range(2, rb):
-                t.append(2 * xi * t[-1] - t[-2])
+            env = 1.0
+            if m.laguerre:
+                u = sc * math.log1p(r / max(sh, 1e-8))
+                env = math.exp(-0.5 * u)
+                t = [1.0, 1.0 - u]
+                for n in range(1, rb - 1):
+                    t.append(((2 * n + 1 - u) * t[n] - n * t[n - 1]) / (n + 1))
+            else:
+                z = 0.5 * sc * (r - sh)
+                xi = z / math.sqrt(1 + z * z) if m.rational else math.tanh(z)
+                t = [1.0, xi]
+                for n in range(2, rb):
+                    t.append(2 * xi * t[-1] - t[-2])
             s = sum(m.radial_coeffs[mu * rb + n] * t[n] for n in range(rb))
-            out.append(m.scaling * m.radial_type_coeffs[zi] * m.radial_type_coeffs[zj] * (r - rc) ** 2 * s)
+            out.append(m.scaling * m.radial_type_coeffs[zi] * m.radial_type_coeffs[zj] * (r - rc) ** 2 * env * s)
         return out
 
     def edge_basics(pair, d):

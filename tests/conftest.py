@@ -27,6 +27,17 @@ def l3k3_path(model_dir):
 
 
 @pytest.fixture(scope="session")
+def laguerre_path(model_dir):
+    """An l3k3 Cu-Zr model on the Laguerre-log1p radial basis (rho 3.5 A)."""
+    import os
+    from sus2sh import models
+    path = os.path.join(model_dir, "l3k3_laguerre.mtp")
+    if not os.path.exists(path):
+        models.write_model(path, laguerre=True, seed=20260404)
+    return path
+
+
+@pytest.fixture(scope="session")
 def l4k4_path(model_dir):
     from sus2sh import models
     return models.preset_model("l4k4", model_dir)

@@ -1,7 +1,8 @@
 """Self-consistency of the FP64 oracle: C vs independent pure-Python
 evaluator, forces vs finite differences of the energy, invariances and the
-virial identity.  These pin the oracle where the reference ships no golden
-energies or forces."""
+virial identity, on the Chebyshev-sss and the Laguerre-log1p radial bases.
+(The oracle's energies and forces are also compared with the reference's own
+engine on the GPU, tests/test_ref_parity_gpu.py.)"""
 import numpy as np
 import pytest
 
@@ -10,9 +11,9 @@ from sus2sh import structures
 from sus2sh_graph import load_mtp
 
 
-@pytest.fixture(scope="module")
-def orc(l3k3_path):
-    return O.Oracle(l3k3_path)
+@pytest.fixture(scope="module", params=["chebyshev_sss", "laguerre_log1p"])
+def orc(request, l3k3_path, laguerre_path):
+    return O.Oracle(l3k3_path if request.param == "chebyshev_sss" else laguerre_path)
 
 
 def test_c_oracle_matches_python_evaluator(orc):
