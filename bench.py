@@ -236,7 +236,8 @@ def run_md(torch, path, box, types, pos, vel, masses, steps, warmup, fp64, world
 
 
 def force_error_vs_fp64(torch, path, box, types, x_dev):
-    """FP32 and FP64 engines on the same frame: force RMS and max |dE|/atom."""
+    """FP32 and FP64 engines on the same frame: force RMS and max |dE|/atom,
+    and the FP32 engine's (pe, f[3,N], w[9,N]) on host."""
     from sus2sh import SUS2_SH
     N = types.size
     dev = x_dev.device
@@ -250,12 +251,13 @@ def force_error_vs_fp64(torch, path, box, types, x_dev):
         pot.compute(box, t, x_dev, pe, f, w)
         torch.cuda.synchronize()
         pot.sync()
-        out.append((pe, f))
+        out.append((pe, f, w))
         pot.close()
     frms = float(torch.sqrt(((out[0][1] - out[1][1]) ** 2).mean()))
     de = float((out[0][0] - out[1][0]).abs().max())
     de_total = float((out[0][0].sum() - out[1][0].sum()).abs()) / N
-    return frms, de, de_total
+    host32 = (out[0][0].cpu().numpy(), out[0][1].view(3, N).cpu().numpy(), out[0][2].view(9, N).cpu().numpy())
+    return frms, de, de_total, host32
 
 
 def e2e_run(torch, pot, box, types, x_dev, steps):
@@ -343,7 +345,7 @@ def batch_cells_run(torch, path, ncells=4096, reps=10):
             "tiles": {"basic_block": info["basic_block"], "force_block": info["force_block"]}}
 
 
-def large_model_run(torch, model_dir, reps=5, atoms=262144, opts=()):
+def large_model_run(torch, model_dir, reps=5, atoms=262144, opts=(), accuracy=True):
     """Large-model workload: Cu-Zr-Al body-5 L=4 K=4 rb10 rational-map model
     (5985 moments, 33,389 products) on 262,144 random-insertion atoms
     (0.06 A^-3, d_min 2.1 A, 50/35/15), FP32; static positions, one
@@ -372,28 +374,55 @@ def large_model_run(torch, model_dir, reps=5, atoms=262144, opts=()):
     prof = pot.profile_read()
     flags = pot.sync()
     info = pot.info()
+    if accuracy:
+        pe.zero_(); f.zero_(); w.zero_()
+        pot.compute(box, t, x, pe, f, w)
+        torch.cuda.synchronize()
     pot.close()
-    return {"workload": f"{N:,}-atom Cu-Zr-Al l4k4 body-5 rational model, FP32", "atoms": N,
-            "cg_kernel": {0: "row interpreter", 1: "straight-line", 2: "component-split"}.get(info["cg_kind"]),
-            "ms_per_eval": ms, "atom_steps_per_s": N / (ms * 1e-3), "status_flags": flags,
-            "stage_ms_per_eval": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"}}
+    out = {"workload": f"{N:,}-atom Cu-Zr-Al l4k4 body-5 rational model, FP32", "atoms": N,
+           "cg_kernel": {0: "row interpreter", 1: "straight-line", 2: "component-split"}.get(info["cg_kind"]),
+           "ms_per_eval": ms, "atom_steps_per_s": N / (ms * 1e-3), "status_flags": flags,
+           "stage_ms_per_eval": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"}}
+    if accuracy:
+        # the FP64 engine on the same frame: absolute errors of the FP32 engine
+        pot64 = SUS2_SH(path, N, ["Cu", "Zr", "Al", "sus2_float=0", *opts])
+        pe64, f64, w64 = z(N), z(3 * N), z(9 * N)
+        pot64.compute(box, t, x, pe64, f64, w64)
+        torch.cuda.synchronize()
+        pot64.close()
+        de = pe - pe64
+        out["accuracy_fp32_vs_fp64"] = {
+            "abs_dE_total_per_atom_eV": float(de.sum().abs()) / N, "site_dE_rms_eV": float((de ** 2).mean().sqrt()),
+            "max_abs_site_dE_eV": float(de.abs().max()), "force_rms_eV_per_A": float(((f - f64) ** 2).mean().sqrt()),
+            "virial_rms_eV": float(((w - w64) ** 2).mean().sqrt()),
+            "site_energy_scale_eV": float(pe64.abs().max()), "force_rms_scale_eV_per_A": float((f64 ** 2).mean().sqrt())}
+    return out
 
 
-def cpu_baseline_sample(path, cells=20, reps=3):
+def cpu_baseline_leg(path, box, types, pos, engine_out):
+    """The FP64 oracle (the reference's algorithm restated in C, OpenMP on all
+    host cores) on the full final frame of the timed run: its throughput is
+    the CPU baseline, and its energies, forces and virials are the checker of
+    the FP32 engine's on the same frame (engine_out: pe[N], f[3,N], w[9,N])."""
+    import numpy as np
     sys.path.insert(0, ORACLE)
     import sus2sh_oracle
-    from sus2sh import structures
-    box, types, pos = structures.fcc(cells, cells, cells, A, (0.64, 0.36), 0.0, seed=7)
     orc = sus2sh_oracle.Oracle(path)
     threads = os.cpu_count() or 1
-    orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
     t0 = time.perf_counter()
-    for _ in range(reps):
-        orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
+    pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types, pos, nthreads=threads)
     dt = time.perf_counter() - t0
-    return {"value": types.size * reps / dt, "unit": "atom-step/s", "cores": threads, "kind": "port",
-            "sample": f"{reps} FP64 oracle force evaluations of a {types.size}-atom {cells}^3-cell slice of "
-                      f"the same FCC Cu-Zr crystal and model (same per-atom work), OpenMP {threads} threads"}
+    pe, f, w = engine_out
+    de = pe - pe0
+    accuracy = {"force_rms_fp32_vs_fp64_oracle_eV_per_A": float(np.sqrt(((f - f0) ** 2).mean())),
+                "virial_rms_fp32_vs_fp64_oracle_eV": float(np.sqrt(((w - w0) ** 2).mean())),
+                "abs_dE_total_per_atom_vs_oracle_eV": abs(float(de.sum())) / de.size,
+                "site_dE_rms_vs_oracle_eV": float(np.sqrt((de ** 2).mean())),
+                "max_abs_site_dE_vs_oracle_eV": float(np.abs(de).max())}
+    baseline = {"value": types.size / dt, "unit": "atom-step/s", "cores": threads, "kind": "port",
+                "sample": f"one FP64 oracle force evaluation of the full {types.size}-atom final frame of the "
+                          f"timed run (same crystal and model), OpenMP {threads} threads"}
+    return baseline, accuracy
 
 
 MODEL_FIXTURE = os.path.join(REPO, "tests", "golden", "models", "l3k3.mtp")
@@ -524,7 +553,8 @@ def main():
         if args.fp64_steps > 0:
             pot64, md64, ms64, prof64, _, _ = run_md(torch, path, box, types, pos, vel, masses, args.fp64_steps,
                                                      min(args.warmup, 3), True, world)
-        frms, de, de_total = force_error_vs_fp64(torch, path, box, types, md.pos)
+        frms, de, de_total, final32 = force_error_vs_fp64(torch, path, box, types, md.pos)
+        final_pos = md.pos.view(3, N).cpu().numpy()
         e2e_val, h2d, d2h = e2e_run(torch, pot, box, types, md.pos, args.e2e_steps)
         ms_max, ms64_max, inv_e2e = max_over_ranks(torch, [ms, ms64 or 0.0, 1.0 / max(e2e_val, 1e-30)], world,
                                                    "cuda")
@@ -583,7 +613,8 @@ def main():
                 line["batch_cells"] = batch_cells_run(torch, path)
                 line["large_model"] = large_model_run(torch, d)
             if world == 1 and not args.no_cpu_baseline:
-                line["cpu_baseline"] = cpu_baseline_sample(path)
+                line["cpu_baseline"], acc_oracle = cpu_baseline_leg(path, box, types, final_pos, final32)
+                line["accuracy"].update(acc_oracle)
             print(json.dumps(line), flush=True)
         pot.close()
         if pot64:

@@ -580,7 +580,8 @@ struct Engine {
       edge_jit = 1;
     } else if (use_float && !gate && opt.model_edges) {
       edge_jit = 2;
-    } else if (!shape_supported(model.l_max, model.k_max, model.rb_size)) {
+    } else if (!shape_supported(model.l_max, model.k_max, model.rb_size) || rs.kind == kRadialLaguerre) {
+      // the ahead-of-time kernels carry the Chebyshev bases only
       edge_jit = 1;
     }
     std::future<std::shared_ptr<const EdgeJitBinary>> model_edges;
@@ -593,7 +594,7 @@ struct Engine {
         return compile_model_edge_kernels(l, k, rb, table, shared_xi, kind);
       });
     } else if (edge_jit == 1) {
-      ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
+      ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate, rs.kind);
     }
     // device uploads
     d_code.upload(prog.code);
@@ -664,9 +665,9 @@ struct Engine {
         ejit_bin = model_edges.get();
       } catch (const std::exception&) {
         ejit_bin.reset();
-        edge_jit = shape_supported(model.l_max, model.k_max, model.rb_size) ? 0 : 1;
+        edge_jit = shape_supported(model.l_max, model.k_max, model.rb_size) && rs.kind != kRadialLaguerre ? 0 : 1;
         if (edge_jit == 1)
-          ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate);
+          ejit_bin = compile_edge_kernels(use_float, model.l_max, model.k_max, model.rb_size, 128, gate, rs.kind);
       }
     }
     if (num_atoms > 0) ensure_size(num_atoms);

@@ -25,7 +25,16 @@ constexpr int kCenterCode = 62;  // image (0,0,0) in base-5 codes
 #else
 #define SUS2_COEF(a, X) ((a).coef[X])
 #define SUS2_SHARED_XI(a) ((a).rs.shared_xi != 0)
-#define SUS2_RADIAL_KIND(a) ((a).rs.kind)
+#ifdef SUS2_SHAPE_RADIAL_KIND
+// NVRTC build of a shape for one radial basis kind
+#define SUS2_RADIAL_KIND(a) (SUS2_SHAPE_RADIAL_KIND)
+#else
+// other builds (ahead of time, or NVRTC for a shape): the Chebyshev kinds,
+// tanh or rational map read at run time; Laguerre models get a build with
+// SUS2_SHAPE_RADIAL_KIND, so these kernels carry no Laguerre code
+#define SUS2_RADIAL_KIND(a) ((a).rs.kind == ::sus2sh::kRadialRational ? ::sus2sh::kRadialRational \
+                                                                      : ::sus2sh::kRadialTanh)
+#endif
 #endif
 
 __device__ __forceinline__ int type_of(const double4& p) {
@@ -89,11 +98,13 @@ __device__ __forceinline__ Edge<double> make_edge<double>(double dx, double dy, 
 // R_mu for every mu; the pair table row holds KMU (scal, shift) pairs then
 // the LK pair scale.  R_mu = s_pair (r - rc)^2 env(x) sum_n c[mu][n] P_n(x)
 // with x the kind's argument (radial_arg).
-template <typename T, int KMU, int RB>
+// KIND >= 0 fixes the basis kind at compile time (kernels instantiated per
+// kind); -1 takes SUS2_RADIAL_KIND.
+template <typename T, int KMU, int RB, int KIND = -1>
 __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __restrict__ row,
                                               const Edge<T>& e, T* R) {
   const T f = row[2 * KMU] * e.dr * e.dr;
-  const int kind = SUS2_RADIAL_KIND(a);
+  const int kind = KIND >= 0 ? KIND : SUS2_RADIAL_KIND(a);
   if (SUS2_SHARED_XI(a)) {
     T x, dx, env, denv;
     radial_arg<T>(kind, row[0], row[1], e.rd, x, dx, env, denv);
@@ -124,13 +135,13 @@ __device__ __forceinline__ void radial_values(const EdgeArgs<T>& a, const T* __r
 
 // R_mu and dR_mu/dr: with f = s_pair (r - rc)^2, s = sum c P_n(x),
 // sd = sum c P_n'(x): dR = (df + f denv/env) env s + f env (dx/dr) sd.
-template <typename T, int KMU, int RB>
+template <typename T, int KMU, int RB, int KIND = -1>
 __device__ __forceinline__ void radial_values_ders(const EdgeArgs<T>& a, const T* __restrict__ row,
                                                    const Edge<T>& e, T* R, T* dR) {
   const T ps = row[2 * KMU];
   const T f = ps * e.dr * e.dr;
   const T df = T(2) * ps * e.dr;
-  const int kind = SUS2_RADIAL_KIND(a);
+  const int kind = KIND >= 0 ? KIND : SUS2_RADIAL_KIND(a);
   if (SUS2_SHARED_XI(a)) {
     T x, dx, env, denv;
     radial_arg<T>(kind, row[0], row[1], e.rd, x, dx, env, denv);

@@ -1,6 +1,7 @@
 // NVRTC build of the per-edge kernels for model shapes without an
 // ahead-of-time instantiation.
 #include "edge_jit.h"
+#include "sh_math.cuh"
 
 #include <nvrtc.h>
 
@@ -80,8 +81,11 @@ std::shared_ptr<EdgeJitBinary> build(bool fp32, int l, int k, int rb, const std:
   }
   const std::string basic_gate_expr = "&sus2sh::edge::k_basic<" + shape + ", 128, true>";
   const std::string force_gate_expr = "&sus2sh::edge::k_force<" + shape + ", 128, true>";
-  const std::string src =
-      (coef ? coef_prelude(*coef, shared_xi, radial_kind) : std::string()) + "#include \"edge_kernels.cuh\"\n";
+  // a shape build for the Laguerre basis compiles it in; otherwise the
+  // Chebyshev kinds are read at run time
+  const std::string src = (coef ? coef_prelude(*coef, shared_xi, radial_kind)
+                                : (radial_kind == kRadialLaguerre ? "#define SUS2_SHAPE_RADIAL_KIND 2\n" : "")) +
+                          std::string("#include \"edge_kernels.cuh\"\n");
   nvrtcProgram prog;
   if (nvrtcCreateProgram(&prog, src.c_str(), "sus2sh_edge.cu", kJitHeaderCount, kJitHeaderSources,
                          kJitHeaderNames) != NVRTC_SUCCESS)
@@ -163,9 +167,10 @@ std::shared_ptr<const EdgeJitBinary> cached(const std::string& key, Build&& make
 }  // namespace
 
 std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block,
-                                                          bool gate) {
-  return cached(shape_key(fp32, l_max, k_max, rb, block, gate),
-                [&] { return build(fp32, l_max, k_max, rb, {block}, gate, nullptr); });
+                                                          bool gate, int radial_kind) {
+  const bool lag = radial_kind == kRadialLaguerre;
+  return cached(shape_key(fp32, l_max, k_max, rb, block, gate) + (lag ? "/laguerre" : ""),
+                [&] { return build(fp32, l_max, k_max, rb, {block}, gate, nullptr, 3, true, lag ? radial_kind : 0); });
 }
 
 std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k_max, int rb,

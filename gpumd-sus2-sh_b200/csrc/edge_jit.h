@@ -29,10 +29,12 @@ struct EdgeJitBinary {
 };
 
 // Compiles k_basic<T, L, K, RB, BLOCK> and k_force<...> (T = float if fp32,
-// else double), and their GATE variants when gate is set.  Results are cached for the life of the process; throws
+// else double), and their GATE variants when gate is set, for the Chebyshev
+// radial kinds (read at run time) or, with radial_kind = kRadialLaguerre, for
+// the Laguerre basis.  Results are cached for the life of the process; throws
 // InputError with the compiler log on failure.
 std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, int k_max, int rb, int block,
-                                                          bool gate);
+                                                          bool gate, int radial_kind = 0);
 
 // FP32 k_basic / k_force of one model at 64, 128 and 256 threads per CTA,
 // with `coef` (the kernels' coefficient table: c[mu][n], then the derivative

@@ -53,7 +53,9 @@ __device__ __forceinline__ void harmonics_and_tangent(const Edge<T>& e, T tx, T 
     }
 }
 
-template <typename T, int L, int K, int RB>
+// KIND: the radial basis kind (kRadialLaguerre), or -1 for the Chebyshev
+// kinds read at run time.
+template <typename T, int L, int K, int RB, int KIND>
 __global__ void __launch_bounds__(128)
     k_pg_basic(const EdgeArgs<T> a, const double* __restrict__ fw, T* __restrict__ B, T* __restrict__ Bd) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(128)
     const T ud = e.ux * tx + e.uy * ty + e.uz * tz;
     const T* row = s_tab + (row_i + type_of(pj)) * a.rs.pair_stride;
     T R[KMU], dR[KMU];
-    radial_values_ders<T, KMU, RB>(a, row, e, R, dR);
+    radial_values_ders<T, KMU, RB, KIND>(a, row, e, R, dR);
     T Y[C], Yd[C];
     harmonics_and_tangent<T, L>(e, tx, ty, tz, ud, Y, Yd);
 #pragma unroll
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-template <typename T, int L, int K, int RB>
+template <typename T, int L, int K, int RB, int KIND>
 __global__ void __launch_bounds__(128)
     k_pg_radial(const EdgeArgs<T> a, const double* __restrict__ fw, const T* __restrict__ Galpha,
                 const T* __restrict__ Gbeta, double* __restrict__ grad_c) {
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(128)
     const int row_i = type_of(pi) * a.rs.species;
     const int cnt = min(a.ncount[i], a.cap);
     const double rc = a.rs.rc, rc2 = rc * rc;
-    const int kind = a.rs.kind;
+    const int kind = KIND >= 0 ? KIND : (a.rs.kind == kRadialRational ? kRadialRational : kRadialTanh);
     for (int n = 0; n < cnt; ++n) {
       const int w = __ldg(a.nbr + static_cast<size_t>(n) * a.N + i);
       const int j = w & 0xFFFFFF;
@@ -353,7 +355,10 @@ int launch_pg_basic(cudaStream_t s, const EdgeArgs<T>& a, const double* fw, T* B
   bool ok = false;
 #define SUS2_PG_BASIC(L, K, RB)                                                     \
   if (!ok && a.l_max == L && a.k_max == K && a.rs.rb == RB) {                       \
-    k_pg_basic<T, L, K, RB><<<grid, 128, sm, s>>>(a, fw, B, Bd);                    \
+    if (a.rs.kind == kRadialLaguerre)                                               \
+      k_pg_basic<T, L, K, RB, kRadialLaguerre><<<grid, 128, sm, s>>>(a, fw, B, Bd); \
+    else                                                                            \
+      k_pg_basic<T, L, K, RB, -1><<<grid, 128, sm, s>>>(a, fw, B, Bd);              \
     ok = true;                                                                      \
   }
   SUS2_PG_SHAPES(SUS2_PG_BASIC)
@@ -385,7 +390,10 @@ int launch_pg_radial(cudaStream_t s, const EdgeArgs<T>& a, const double* fw, con
   bool ok = false;
 #define SUS2_PG_RADIAL(L, K, RB)                                                    \
   if (!ok && a.l_max == L && a.k_max == K && a.rs.rb == RB) {                       \
-    k_pg_radial<T, L, K, RB><<<grid, 128, sm, s>>>(a, fw, Galpha, Gbeta, grad_c);   \
+    if (a.rs.kind == kRadialLaguerre)                                               \
+      k_pg_radial<T, L, K, RB, kRadialLaguerre><<<grid, 128, sm, s>>>(a, fw, Galpha, Gbeta, grad_c); \
+    else                                                                            \
+      k_pg_radial<T, L, K, RB, -1><<<grid, 128, sm, s>>>(a, fw, Galpha, Gbeta, grad_c); \
     ok = true;                                                                      \
   }
   SUS2_PG_SHAPES(SUS2_PG_RADIAL)

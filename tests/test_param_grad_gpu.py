@@ -2,9 +2,9 @@
 term) against central finite differences of the FP64 oracle's loss.
 
 Loss of the fitting workload: L = sum_c (E_c - E_t)^2 + 0.1 sum |F - F_t|^2
-over 108-atom FCC cells, targets from a second seeded model, gradients with
-respect to the linear weights (moment_coeffs) and radial coefficients,
-FD step 1e-4."""
+over 64 FCC cells of 108 atoms, targets from a second seeded model, gradients
+with respect to the linear weights (moment_coeffs) and radial coefficients
+(16 of each sampled), FD step 1e-4."""
 import numpy as np
 import pytest
 
@@ -35,7 +35,7 @@ def _oracle_loss(orc, cells, targets):
 def setup(model_dir):
     path = models.preset_model("l3k3", model_dir)
     tpath = models.preset_model("l3k3_target", model_dir)
-    cells = _cells(2, 300)
+    cells = _cells(64, 300)  # the fitting workload: 64 cells of 108 atoms
     torc = O.Oracle(tpath)
     targets = []
     for box, types, pos in cells:
@@ -53,8 +53,8 @@ def test_param_grad_matches_finite_differences(setup, fp64):
     L0 = _oracle_loss(orc, cells, targets)
     assert abs(L - L0) < (1e-9 if fp64 else 1e-5) * max(1.0, abs(L0))
     rng = np.random.default_rng(5)
-    ws = rng.choice(gw.size, 8, replace=False)
-    cs = rng.choice(gc.size, 8, replace=False)
+    ws = rng.choice(gw.size, 16, replace=False)
+    cs = rng.choice(gc.size, 16, replace=False)
     rel = 1e-5 if fp64 else 2e-3
     for kind, idxs, g, arr in (("w", ws, gw, orc.arrays.w), ("c", cs, gc, orc.arrays.radial)):
         scale = np.abs(g).max()
