@@ -459,8 +459,21 @@ static int build_nlist(const Geo* g, int N, const double* pos, double rc, NList*
 }
 
 /* ---- energy / forces / virial -------------------------------------------- */
+/* center (optional): only atoms with center[i] != 0 are centres: their site
+   energies, the forces of those energies on every atom, and their virials;
+   the other atoms (ghosts of a spatial decomposition) get pe = vir = 0. */
+int oracle_efs_centers(const OracleModel* m, int N, const double* h, const int* pbc, const int* type,
+                       const double* pos, const unsigned char* center, double* pe, double* f, double* vir,
+                       int nthreads);
+
 int oracle_efs(const OracleModel* m, int N, const double* h, const int* pbc, const int* type,
                const double* pos, double* pe, double* f, double* vir, int nthreads) {
+  return oracle_efs_centers(m, N, h, pbc, type, pos, NULL, pe, f, vir, nthreads);
+}
+
+int oracle_efs_centers(const OracleModel* m, int N, const double* h, const int* pbc, const int* type,
+                       const double* pos, const unsigned char* center, double* pe, double* f, double* vir,
+                       int nthreads) {
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
   const int nt = omp_get_max_threads();
@@ -489,6 +502,11 @@ int oracle_efs(const OracleModel* m, int N, const double* h, const int* pbc, con
 #pragma omp for schedule(dynamic, 32)
     for (int i = 0; i < N; ++i) {
       const int ti = type[i];
+      if (center && !center[i]) {
+        pe[i] = 0.0;
+        for (int k = 0; k < 9; ++k) vir[(size_t)k * N + i] = 0.0;
+        continue;
+      }
       memset(Mv, 0, sizeof(double) * m->M);
       for (int q = nl.start[i]; q < nl.start[i + 1]; ++q) {
         const Edge* e = nl.e + q;

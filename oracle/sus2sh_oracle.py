@@ -228,6 +228,25 @@ class Oracle:
                 raise RuntimeError("oracle_zbl_efs failed")
         return pe, f, vir
 
+    def efs_centers(self, h, pbc, types, pos, center, nthreads: int = 0):
+        """As efs, but only atoms with center != 0 are centres (site energies,
+        the forces of those energies on every atom, their virials); the other
+        atoms get zero energy and virial.  Plain models (no gate, no ZBL)."""
+        if self.gate is not None or self.zbl is not None:
+            raise ValueError("efs_centers: plain models only")
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        N = pos.shape[1]
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        h = np.ascontiguousarray(np.asarray(h, dtype=np.float64).ravel())
+        pbc = np.ascontiguousarray(np.asarray(pbc, dtype=np.int32))
+        mask = np.ascontiguousarray(np.asarray(center) != 0, dtype=np.uint8)
+        pe, f, vir = np.zeros(N), np.zeros((3, N)), np.zeros((9, N))
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        if self.lib.oracle_efs_centers(ctypes.byref(self._c), N, ptr(h), ptr(pbc), ptr(types), ptr(pos), ptr(mask),
+                                       ptr(pe), ptr(f), ptr(vir), nthreads) != 0:
+            raise RuntimeError("oracle_efs_centers failed")
+        return pe, f, vir
+
     def basics(self, h, pbc, types, pos, nthreads: int = 0):
         pos = np.ascontiguousarray(pos, dtype=np.float64)
         N = pos.shape[1]
