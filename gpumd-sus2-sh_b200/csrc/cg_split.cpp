@@ -19,6 +19,7 @@
 // component, and every chunk of global work, is its own __noinline__
 // function, which keeps ptxas time linear in the graph size.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -60,6 +61,33 @@ struct Component {
   std::vector<int> locals;  // moments, in row order
   std::vector<Term> terms;  // terminal terms with at least one local operand
 };
+
+// The terms of a row grouped by the magnitude of their coefficient as the
+// working precision rounds it (in order of first appearance), with each
+// term's sign.
+struct MagGroup {
+  double magnitude;
+  std::vector<size_t> terms;
+  std::vector<bool> negative;
+};
+
+std::vector<MagGroup> magnitude_groups(const Row& row, bool use_float) {
+  std::vector<MagGroup> out;
+  std::map<double, size_t> index;
+  for (size_t t = 0; t < row.coeff.size(); ++t) {
+    double c = row.coeff[t];
+    if (use_float) c = static_cast<double>(static_cast<float>(c));
+    const double m = std::fabs(c);
+    auto it = index.find(m);
+    if (it == index.end()) {
+      it = index.emplace(m, out.size()).first;
+      out.push_back({m, {}, {}});
+    }
+    out[it->second].terms.push_back(t);
+    out[it->second].negative.push_back(c < 0.0);
+  }
+  return out;
+}
 
 }  // namespace
 
@@ -298,17 +326,25 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
     auto val = [&](int x) -> std::string {  // value of local or global
       if (cls[x] != kLocal) return g(x);
       if (!have_v.count(x)) {
+        // v = sum_t c_t a_t b_t as sum over the row's coefficient magnitudes m of
+        // m * (sum of +-a_t b_t): one multiply-add per term and one per
+        // magnitude (real-CG rows repeat magnitudes) instead of two per term
         const Row& row = lay.rows[row_of[x]];
-        std::vector<std::string> ls, rs;
-        for (size_t t = 0; t < row.left.size(); ++t) {
-          ls.push_back(g(row.left[t]));
-          rs.push_back(g(row.right[t]));
+        const std::vector<MagGroup> groups = magnitude_groups(row, use_float);
+        const std::string xs = std::to_string(x);
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+          const std::string sn = "s" + xs + "_" + std::to_string(gi);
+          const MagGroup& gr = groups[gi];
+          for (size_t k = 0; k < gr.terms.size(); ++k) {
+            const size_t t = gr.terms[k];
+            const std::string la = (gr.negative[k] ? "-" : "") + g(row.left[t]), rb = g(row.right[t]);
+            if (k == 0) f << "  " << T << " " << sn << " = " << la << " * " << rb << ";\n";
+            else f << "  " << sn << " = " << FMA << "(" << la << ", " << rb << ", " << sn << ");\n";
+          }
+          if (gi == 0) f << "  " << T << " v" << xs << " = " << lit(gr.magnitude, use_float) << " * " << sn << ";\n";
+          else f << "  v" << xs << " = " << FMA << "(" << lit(gr.magnitude, use_float) << ", " << sn << ", v" << xs
+                 << ");\n";
         }
-        f << "  " << T << " v" << x << " = " << lit(row.coeff[0], use_float) << " * " << ls[0] << " * " << rs[0]
-          << ";\n";
-        for (size_t t = 1; t < row.left.size(); ++t)
-          f << "  v" << x << " = " << FMA << "(" << lit(row.coeff[t], use_float) << " * " << ls[t] << ", " << rs[t]
-            << ", v" << x << ");\n";
         terms_emitted += static_cast<long long>(row.left.size());
         have_v.insert(x);
       }
@@ -368,13 +404,21 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
         // back-propagation through the row of x into the global accumulators
         // (a local without any adjoint contributes nothing)
         if (h || !kx.empty()) {
+          // one product m * gx per coefficient magnitude of the row, then two
+          // multiply-adds per term with the term's sign on the operand
           const Row& row = lay.rows[row_of[x]];
-          for (size_t t = 0; t < row.left.size(); ++t) {
-            const int a = row.left[t], b = row.right[t];
-            const std::string pn = "p" + xs + "_" + std::to_string(t);
-            f << "  const " << T << " " << pn << " = " << lit(row.coeff[t], use_float) << " * " << gx << ";\n";
-            acc(have_q, "q", a, pn, g(b));
-            acc(have_q, "q", b, pn, g(a));
+          const std::vector<MagGroup> groups = magnitude_groups(row, use_float);
+          for (size_t gi = 0; gi < groups.size(); ++gi) {
+            const MagGroup& gr = groups[gi];
+            const std::string pn = "p" + xs + "_" + std::to_string(gi);
+            f << "  const " << T << " " << pn << " = " << lit(gr.magnitude, use_float) << " * " << gx << ";\n";
+            for (size_t k = 0; k < gr.terms.size(); ++k) {
+              const size_t t = gr.terms[k];
+              const int a = row.left[t], b = row.right[t];
+              const std::string ps = gr.negative[k] ? "(-" + pn + ")" : pn;
+              acc(have_q, "q", a, ps, g(b));
+              acc(have_q, "q", b, ps, g(a));
+            }
           }
           terms_emitted += 2 * static_cast<long long>(row.left.size());
         }
