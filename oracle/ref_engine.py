@@ -113,3 +113,18 @@ def profile_stages(stdout: str) -> dict | None:
             k, v = part.split("=", 1)
             out[k.strip()] = float(v.strip().split()[0])
     return out
+
+
+if __name__ == "__main__":
+    # python oracle/ref_engine.py frame <out.bin>: the benchmark's static
+    # 1,024,000-atom Cu-Zr frame (80x80x40 FCC, a = 3.8 A, 64/36, seed 1000)
+    # as input for oracle/_ref/ref_sus2sh run, e.g. to profile the reference.
+    import sys
+    if len(sys.argv) != 3 or sys.argv[1] != "frame":
+        raise SystemExit("usage: ref_engine.py frame <out.bin>")
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "gpumd-sus2-sh_b200"))
+    from sus2sh import structures
+    box, types, pos = structures.fcc(80, 80, 40, 3.8, (0.64, 0.36), 0.0, seed=1000)
+    write_input(sys.argv[2], box.cpu_h, box.pbc, types, pos)
+    print(f"wrote {types.size} atoms to {sys.argv[2]}")
