@@ -381,11 +381,15 @@ def large_model_run(torch, model_dir, reps=5, atoms=262144, opts=(), accuracy=Tr
     pot.close()
     out = {"workload": f"{N:,}-atom Cu-Zr-Al l4k4 body-5 rational model, FP32", "atoms": N,
            "cg_kernel": {0: "row interpreter", 1: "straight-line", 2: "component-split"}.get(info["cg_kind"]),
+           "cg_build": {0: None, 1: "one NVRTC program", 2: "parallel relocatable units"}.get(info["cg_build"]),
+           "cg_compile_ms": info["cg_jit_compile_ms"], "cg_from_disk_cache": bool(info["cg_from_disk_cache"]),
            "ms_per_eval": ms, "atom_steps_per_s": N / (ms * 1e-3), "status_flags": flags,
            "stage_ms_per_eval": {k: v / max(prof["calls"], 1) for k, v in prof.items() if k != "calls"}}
     if accuracy:
         # the FP64 engine on the same frame: absolute errors of the FP32 engine
-        pot64 = SUS2_SH(path, N, ["Cu", "Zr", "Al", "sus2_float=0", *opts])
+        # (its CG kernel from the parallel build: the same results as the
+        # one-program build, without the minute of single-threaded compile)
+        pot64 = SUS2_SH(path, N, ["Cu", "Zr", "Al", "sus2_float=0", "sus2_sh_cg_whole=0", *opts])
         pe64, f64, w64 = z(N), z(3 * N), z(9 * N)
         pot64.compute(box, t, x, pe64, f64, w64)
         torch.cuda.synchronize()

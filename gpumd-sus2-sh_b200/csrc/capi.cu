@@ -654,7 +654,7 @@ struct Engine {
       const auto t0 = std::chrono::steady_clock::now();
       std::string why;
       if (choose_cg_source(model, lay, prog.basic_canon, prog.ncanon, use_float, opt.cg_split, &cg_src, &why))
-        cg_bin = compile_cg_source(cg_src);
+        cg_bin = compile_cg_source(cg_src, opt.cg_whole ? CgBuild::kWhole : CgBuild::kParallel);
       cg_compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     if (model_edges.valid()) {
@@ -1548,7 +1548,7 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[34] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[36] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
@@ -1561,8 +1561,9 @@ int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
                      e.ejit_bin ? static_cast<int>(e.ejit_bin->compile_ms) : 0,
                      e.gate ? static_cast<int>(e.model.gate.mode) : 0,
                      e.cg_bin.cubin.empty() ? 0 : (e.cg_src.split ? 2 : 1),
-                     e.cg_mod.registers(), e.cg_mod.local_bytes()};
-  const int k = std::min(n, 34);
+                     e.cg_mod.registers(), e.cg_mod.local_bytes(),
+                     e.cg_bin.cubin.empty() ? 0 : (e.cg_bin.whole ? 1 : 2), e.cg_bin.from_disk ? 1 : 0};
+  const int k = std::min(n, 36);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -1598,11 +1599,12 @@ int sus2sh_cg_kernel_info(const char* path, int use_float, int split, int* info,
     std::string why;
     if (split == 2) {
       src = sus2sh::generate_pg_source(m, lay, use_float != 0, prog.basic_canon, prog.ncanon);
-    } else if (!sus2sh::choose_cg_source(m, lay, prog.basic_canon, prog.ncanon, use_float != 0, split, &src,
-                                         &why)) {
+    } else if (!sus2sh::choose_cg_source(m, lay, prog.basic_canon, prog.ncanon, use_float != 0,
+                                         split == 3 ? 1 : split, &src, &why)) {
       throw InputError("no CG kernel for this graph (" + why + "); the row interpreter runs it");
     }
-    const sus2sh::CgBinary bin = sus2sh::compile_cg_source(src);
+    const sus2sh::CgBinary bin =
+        sus2sh::compile_cg_source(src, split == 3 ? sus2sh::CgBuild::kParallel : sus2sh::CgBuild::kWhole);
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     int spill = 0;
     const size_t p = bin.log.find("bytes spill stores");

@@ -6,10 +6,14 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <nvJitLink.h>
 #include <nvrtc.h>
 
 #include <algorithm>
+#include <cerrno>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -499,18 +503,24 @@ int max_registers(const std::string& log) {
   return best;
 }
 
-CgBinary build_binary(const CgSource& src) {
+CgBinary build_one_program(const std::string& code) {
   CgBinary out;
+  UnitResult u = compile_unit(code, false);
+  if (!u.error.empty()) throw InputError(u.error);
+  out.cubin = std::move(u.cubin);
+  out.log = std::move(u.log);
+  out.registers = max_registers(out.log);
+  out.whole = true;
+  return out;
+}
+
+CgBinary build_binary(const CgSource& src, CgBuild build) {
   const JitLinkApi& jl = jitlink();
-  if (src.units.size() < 2 || !jl.ok) {
+  if (src.units.size() < 2 || build == CgBuild::kWhole || !jl.ok) {
     // one program (also the fallback when nvJitLink 12.9 is not available)
-    UnitResult u = compile_unit(src.code, false);
-    if (!u.error.empty()) throw InputError(u.error);
-    out.cubin = std::move(u.cubin);
-    out.log = std::move(u.log);
-    out.registers = max_registers(out.log);
-    return out;
+    return build_one_program(src.code);
   }
+  CgBinary out;
   // component-split kernel: the units compile in parallel as relocatable
   // code and nvJitLink joins them
   std::vector<UnitResult> res(src.units.size());
@@ -565,23 +575,149 @@ CgBinary build_binary(const CgSource& src) {
   return out;
 }
 
+// ---- on-disk cache of whole-program builds
+//
+// One file per kernel source: a 64-byte header (magic, format, source size,
+// two independent 64-bit hashes of the source, NVRTC version, log and cubin
+// sizes), the ptxas report, the cubin.  Written to a temporary name and
+// renamed, so readers never see a partial file; a file that does not match
+// its header is ignored and rewritten.
+constexpr char kCacheMagic[8] = {'S', 'U', 'S', '2', 'C', 'G', 'B', '1'};
+
+struct CacheHeader {
+  char magic[8];
+  uint64_t code_size, h1, h2;
+  int32_t nvrtc_major, nvrtc_minor;
+  uint64_t log_size, cubin_size;
+  uint64_t reserved;
+};
+static_assert(sizeof(CacheHeader) == 64, "cache header layout");
+
+uint64_t hash2(const std::string& s) {
+  // a second, independent hash (64-bit multiply-xorshift over 8-byte words)
+  uint64_t h = 0x9E3779B97F4A7C15ull ^ s.size();
+  size_t i = 0;
+  for (; i + 8 <= s.size(); i += 8) {
+    uint64_t w;
+    std::memcpy(&w, s.data() + i, 8);
+    h = (h ^ w) * 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 31;
+  }
+  for (; i < s.size(); ++i) h = (h ^ static_cast<unsigned char>(s[i])) * 0x94D049BB133111EBull;
+  return h ^ (h >> 29);
+}
+
+std::string cache_path(const std::string& dir, const std::string& code, CacheHeader* hdr) {
+  std::memcpy(hdr->magic, kCacheMagic, 8);
+  hdr->code_size = code.size();
+  hdr->h1 = fnv1a(code);
+  hdr->h2 = hash2(code);
+  int major = 0, minor = 0;
+  nvrtcVersion(&major, &minor);
+  hdr->nvrtc_major = major;
+  hdr->nvrtc_minor = minor;
+  hdr->log_size = hdr->cubin_size = hdr->reserved = 0;
+  char name[160];
+  std::snprintf(name, sizeof(name), "/cg_%016llx_%016llx_nvrtc%d.%d_sm100a.cubin",
+                static_cast<unsigned long long>(hdr->h1), static_cast<unsigned long long>(hdr->h2), major, minor);
+  return dir + name;
+}
+
+bool cache_read(const std::string& path, const CacheHeader& want, CgBinary* out) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  CacheHeader h;
+  bool ok = std::fread(&h, sizeof(h), 1, f) == 1 && std::memcmp(h.magic, want.magic, 8) == 0 &&
+            h.code_size == want.code_size && h.h1 == want.h1 && h.h2 == want.h2 &&
+            h.nvrtc_major == want.nvrtc_major && h.nvrtc_minor == want.nvrtc_minor && h.cubin_size > 0 &&
+            h.cubin_size < (1ull << 31) && h.log_size < (1ull << 26);
+  if (ok) {
+    out->log.resize(h.log_size);
+    out->cubin.resize(h.cubin_size);
+    ok = (h.log_size == 0 || std::fread(&out->log[0], 1, h.log_size, f) == h.log_size) &&
+         std::fread(out->cubin.data(), 1, h.cubin_size, f) == h.cubin_size && std::fgetc(f) == EOF;
+  }
+  std::fclose(f);
+  if (!ok) return false;
+  out->registers = max_registers(out->log);
+  out->whole = true;
+  out->from_disk = true;
+  return true;
+}
+
+bool make_dirs(const std::string& dir) {
+  for (size_t p = 1; p <= dir.size(); ++p) {
+    if (p < dir.size() && dir[p] != '/') continue;
+    const std::string sub = dir.substr(0, p);
+    if (mkdir(sub.c_str(), 0755) != 0 && errno != EEXIST) return false;
+  }
+  struct stat st;
+  return stat(dir.c_str(), &st) == 0 && S_ISDIR(st.st_mode);
+}
+
+void cache_write(const std::string& dir, const std::string& path, CacheHeader hdr, const CgBinary& bin) {
+  if (!make_dirs(dir)) return;
+  hdr.log_size = bin.log.size();
+  hdr.cubin_size = bin.cubin.size();
+  char suffix[64];
+  std::snprintf(suffix, sizeof(suffix), ".tmp%ld_%zu", static_cast<long>(getpid()),
+                std::hash<std::thread::id>()(std::this_thread::get_id()));
+  const std::string tmp = path + suffix;
+  FILE* f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return;
+  bool ok = std::fwrite(&hdr, sizeof(hdr), 1, f) == 1 &&
+            (bin.log.empty() || std::fwrite(bin.log.data(), 1, bin.log.size(), f) == bin.log.size()) &&
+            std::fwrite(bin.cubin.data(), 1, bin.cubin.size(), f) == bin.cubin.size();
+  ok = std::fclose(f) == 0 && ok;
+  if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
+
 }  // namespace
 
-CgBinary compile_cg_source(const CgSource& src) {
+std::string cg_cache_dir() {
+  if (const char* d = std::getenv("SUS2SH_CACHE_DIR")) {
+    const std::string s = d;
+    if (s.empty() || s == "off" || s == "0") return "";
+    return s;
+  }
+  if (const char* x = std::getenv("XDG_CACHE_HOME"))
+    if (*x) return std::string(x) + "/sus2sh";
+  if (const char* home = std::getenv("HOME"))
+    if (*home) return std::string(home) + "/.cache/sus2sh";
+  return "";
+}
+
+CgBinary compile_cg_source(const CgSource& src, CgBuild build) {
   // binaries are cached per process: models of the same graph (or the same
   // model loaded twice) compile once
-  static std::mutex mu;
-  static std::map<std::string, std::shared_ptr<const CgBinary>> cache;
+  static std::mutex* mu = new std::mutex;  // never destroyed: safe at process exit
+  static auto* cache = new std::map<std::string, std::shared_ptr<const CgBinary>>;
+  const bool whole = build == CgBuild::kWhole || src.units.size() < 2;
   const std::string key = src.kernel_name + ":" + std::to_string(src.code.size()) + ":" +
-                          std::to_string(fnv1a(src.code));
+                          std::to_string(fnv1a(src.code)) + (whole ? ":whole" : ":units");
   {
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(key);
-    if (it != cache.end()) return *it->second;
+    std::lock_guard<std::mutex> lock(*mu);
+    auto it = cache->find(key);
+    if (it != cache->end()) return *it->second;
   }
-  auto bin = std::make_shared<const CgBinary>(build_binary(src));
-  std::lock_guard<std::mutex> lock(mu);
-  return *cache.emplace(key, bin).first->second;
+  std::shared_ptr<const CgBinary> bin;
+  if (whole) {
+    // one-program builds go through the disk cache
+    const std::string dir = cg_cache_dir();
+    CacheHeader hdr;
+    const std::string path = dir.empty() ? std::string() : cache_path(dir, src.code, &hdr);
+    CgBinary b;
+    if (!path.empty() && cache_read(path, hdr, &b)) {
+      bin = std::make_shared<const CgBinary>(std::move(b));
+    } else {
+      bin = std::make_shared<const CgBinary>(build_one_program(src.code));
+      if (!path.empty()) cache_write(dir, path, hdr, *bin);
+    }
+  } else {
+    bin = std::make_shared<const CgBinary>(build_binary(src, build));
+  }
+  std::lock_guard<std::mutex> lock(*mu);
+  return *cache->emplace(key, bin).first->second;
 }
 
 // ---------------------------------------------------------------------------

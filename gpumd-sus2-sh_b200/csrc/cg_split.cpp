@@ -350,10 +350,16 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
       }
       return "v" + std::to_string(x);
     };
+    // accumulators of local values (h, k) start with their first product; those
+    // of globals (q) start from the global's adjoint in shared memory, so the
+    // flush at the global's last use in the component is a single store
     auto acc = [&](std::set<int>& have, const char* pfx, int x, const std::string& a, const std::string& b) {
       const std::string nm = pfx + std::to_string(x);
       if (!have.count(x)) {
-        f << "  " << T << " " << nm << " = " << a << " * " << b << ";\n";
+        if (&have == &have_q)
+          f << "  " << T << " " << nm << " = " << FMA << "(" << a << ", " << b << ", " << sa(gslot[x]) << ");\n";
+        else
+          f << "  " << T << " " << nm << " = " << a << " * " << b << ";\n";
         have.insert(x);
       } else {
         f << "  " << nm << " = " << FMA << "(" << a << ", " << b << ", " << nm << ");\n";
@@ -426,7 +432,7 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
       auto fl = flush_at.find(static_cast<int>(e));
       if (fl != flush_at.end())
         for (int y : fl->second)
-          if (have_q.count(y)) f << "  " << sa(gslot[y]) << " += q" << y << ";\n";
+          if (have_q.count(y)) f << "  " << sa(gslot[y]) << " = q" << y << ";\n";
     }
     f << "  return e;\n}\n";
     add_fn(sig, f.str());

@@ -926,6 +926,8 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       o.cg_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_cg_split") {
       o.cg_split = parse_bool(val, key) ? 1 : 0;
+    } else if (key == "sus2_sh_cg_whole") {
+      o.cg_whole = parse_bool(val, key);
     } else if (key == "sus2_sh_reference_rounding") {
       o.reference_rounding = parse_bool(val, key);
     } else if (key == "sus2_radial_direct" || key == "sus2_sh_radial_direct" || key == "radial_direct") {

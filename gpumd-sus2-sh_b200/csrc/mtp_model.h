@@ -138,6 +138,9 @@ struct Options {
   bool cg_jit = true;               // sus2_sh_cg_jit=0 runs the CG row interpreter instead
   int cg_split = -1;                // sus2_sh_cg_split=0|1: never / always the component-split
                                     // CG kernel (-1: graphs above the single-function limit)
+  bool cg_whole = true;             // sus2_sh_cg_whole=0 compiles a component-split CG kernel as
+                                    // parallel relocatable units (fast load, slower kernel)
+                                    // instead of one program (disk-cached)
   bool autotune = true;             // sus2_sh_autotune=0 keeps 128-thread edge-kernel CTAs
   bool edge_jit = false;            // sus2_sh_edge_jit=1 compiles the edge kernels at load even
                                     // for a shape built ahead of time

@@ -194,7 +194,13 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * 1 mu-body-linear-combo, 2 mu-scalar-full) [31] CG kernel kind (0 row
  * interpreter, 1 one straight-line function, 2 component-split) [32] [33]
  * registers and local-memory bytes per thread of the loaded CG kernel, call
- * tree included (-1 before the first evaluation).  Returns the number written. */
+ * tree included (-1 before the first evaluation) [34] how the CG kernel was
+ * compiled (0 none, 1 one NVRTC program, 2 parallel relocatable units joined
+ * by nvJitLink: option sus2_sh_cg_whole=0 for component-split kernels)
+ * [35] 1 when that program was read from the on-disk cache of one-program
+ * builds ($SUS2SH_CACHE_DIR, else $XDG_CACHE_HOME/sus2sh or
+ * ~/.cache/sus2sh; SUS2SH_CACHE_DIR=off disables it).  Returns the number
+ * written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

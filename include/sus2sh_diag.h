@@ -16,7 +16,10 @@ extern "C" {
 /* Generates and NVRTC-compiles (sm_100a, no GPU needed) the model-specialised
  * CG product kernel the engine would build for a model file (split: -1 as the
  * engine chooses, 0 never / 1 always the component-split kernel, 2 the
- * forward-over-reverse product kernel of the parameter gradients): info[0]
+ * forward-over-reverse product kernel of the parameter gradients, 3 the
+ * component-split kernel compiled as parallel relocatable units, as option
+ * sus2_sh_cg_whole=0 does; otherwise one program, through the engine's
+ * on-disk cache of one-program builds): info[0]
  * registers per thread, [1] spill store bytes, [2] emitted multiply-add terms,
  * [3] generate+compile ms, [4] cubin bytes, [5] 1 for a component-split
  * kernel, [6] device functions, [7] components, [8] threads per CTA, [9]

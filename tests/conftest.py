@@ -13,6 +13,11 @@ for p in (PKG, ORACLE):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); parity tests through the C-ABI")
+    # one-program CG kernel builds are kept on disk; the test session (and the
+    # processes it starts) shares a fresh cache instead of the user's
+    if "SUS2SH_CACHE_DIR" not in os.environ:
+        import tempfile
+        os.environ["SUS2SH_CACHE_DIR"] = tempfile.mkdtemp(prefix="sus2sh_cache_")
 
 
 @pytest.fixture(scope="session")

@@ -9,6 +9,7 @@ import ctypes
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -39,11 +40,60 @@ def test_l3k3_cg_kernel_compiles_without_spills(l3k3_path):
 
 def test_large_graph_gets_the_split_kernel(l4k4_path):
     # l4k4 body 5: 33,389 products in 116 (rank L, component M) components
-    rc, info, log = _info(l4k4_path, 1)
+    # (split=3: the parallel relocatable build, seconds instead of the
+    # one-program build's minute on the host)
+    rc, info, log = _info(l4k4_path, 1, split=3)
     assert rc == 0, _lib.load().sus2sh_last_error().decode()
     assert info["split"] == 1 and info["components"] == 116
     assert info["block"] == 128 and info["smem"] == 2 * 100 * 128 * 4
     assert info["spill"] == 0, log
+
+
+_CACHE_PROBE = r"""
+import ctypes, sys
+sys.path.insert(0, sys.argv[1])
+from sus2sh import _lib
+lib = _lib.load()
+info = (ctypes.c_int * 10)()
+rc = lib.sus2sh_cg_kernel_info(sys.argv[2].encode(), 1, int(sys.argv[3]), info, None, 0)
+print(rc, info[3], info[4])
+"""
+
+
+def _probe(path, split, cache_dir):
+    env = dict(os.environ, SUS2SH_CACHE_DIR=cache_dir)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpumd-sus2-sh_b200")
+    out = subprocess.run([sys.executable, "-c", _CACHE_PROBE, pkg, path, str(split)], env=env, check=True,
+                         capture_output=True, text=True).stdout.split()
+    return int(out[0]), int(out[1]), int(out[2])
+
+
+@pytest.mark.parametrize("split", [-1, 1], ids=["straight_line", "component_split"])
+def test_one_program_builds_go_through_the_disk_cache(l3k3_path, tmp_path, split):
+    # each process starts with an empty in-process cache: the first compiles
+    # and writes the cubin, the second reads it back, a damaged file is
+    # ignored and rewritten
+    cache = str(tmp_path / "cache")
+    rc, ms_first, size = _probe(l3k3_path, split, cache)
+    assert rc == 0 and size > 0
+    files = [f for f in os.listdir(cache) if f.startswith("cg_") and f.endswith(".cubin")]
+    assert len(files) == 1
+    fpath = os.path.join(cache, files[0])
+    with open(fpath, "rb") as f:
+        blob = f.read()
+    assert blob[:8] == b"SUS2CGB1" and len(blob) > size
+    rc, ms_cached, size2 = _probe(l3k3_path, split, cache)
+    assert rc == 0 and size2 == size and ms_cached < max(50, ms_first // 4), (ms_first, ms_cached)
+    with open(fpath, "wb") as f:
+        f.write(blob[: len(blob) // 2])  # truncated
+    rc, _, size3 = _probe(l3k3_path, split, cache)
+    assert rc == 0 and size3 == size
+    with open(fpath, "rb") as f:
+        again = f.read()  # rewritten whole (NVRTC output is not byte-stable: compare the header and length)
+    assert len(again) == len(blob) and again[:40] == blob[:40] and again[48:64] == blob[48:64]
+    assert not [f for f in os.listdir(cache) if ".tmp" in f]
+    rc, _, size4 = _probe(l3k3_path, split, "off")  # disabled
+    assert rc == 0 and size4 == size
 
 
 def test_large_graph_without_split_runs_the_interpreter(l4k4_path):

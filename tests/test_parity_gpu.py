@@ -191,7 +191,29 @@ def test_large_model_uses_split_kernel(l4k4_path):
     info = pot.info()
     pot.close()
     assert info["cg_kind"] == 2 and 0 < info["cg_loaded_registers"] <= 255
+    assert info["cg_build"] == 1  # one program (the default)
     assert info["cg_local_bytes"] <= 1024, info["cg_local_bytes"]
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_split_kernel_builds_agree_bit_for_bit(l4k4_path, fp64):
+    # the one-program build (default) and the parallel relocatable build
+    # (sus2_sh_cg_whole=0) compile the same source: identical site energies
+    # and per-atom virials (each a per-centre sum of the CG kernel's outputs);
+    # the forces are scattered with FP32 atomics, whose order varies from run
+    # to run, so they agree to FP32 rounding
+    box, types, pos = structures.random_insertion(2000, 0.06, 2.1, (1.0, 1.0, 1.0), (0.5, 0.35, 0.15), seed=9)
+    base = ("sus2_float=0",) if fp64 else ()
+    out = []
+    for opts in (base, base + ("sus2_sh_cg_whole=0",)):
+        out.append(engine_efs(l4k4_path, box, types, pos, opts, species=("Cu", "Zr", "Al")))
+        pot = SUS2_SH(l4k4_path, types.size, ["Cu", "Zr", "Al", *opts])
+        info = pot.info()
+        pot.close()
+        assert info["cg_kind"] == 2 and info["cg_build"] == (2 if "sus2_sh_cg_whole=0" in opts else 1), info
+    (pe0, f0, w0), (pe1, f1, w1) = out
+    assert np.array_equal(pe0, pe1) and np.array_equal(w0, w1)
+    assert np.abs(f0 - f1).max() <= 1e-6 * np.abs(f0).max()
 
 
 @pytest.mark.parametrize("fp64", [False, True])
