@@ -46,6 +46,31 @@ unsigned long long fnv1a(const std::string& s) {
 
 }  // namespace
 
+const char* const kCgStreamHelpers = R"(#ifdef __CUDA_ARCH__
+__device__ __forceinline__ unsigned long long sus2_pol() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float sus2_ld(const float* a, unsigned long long pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double sus2_ld(const double* a, unsigned long long pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void sus2_st(float* a, float v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void sus2_st(double* a, double v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+#endif
+)";
+
 CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_float,
                             const std::vector<int>& basic_canon, int ncanon) {
   const int M = m.moments, Bb = m.basic_count;
@@ -181,6 +206,7 @@ CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_flo
   out.kernel_name = "sus2sh_cg_" + tag;
   src << "// generated SUS2-SH CG product kernel (" << (use_float ? "FP32" : "FP64") << ")\n"
       << "struct D4 { double x, y, z, w; };\n"
+      << kCgStreamHelpers
       << "extern \"C\" __global__ void __launch_bounds__(128) " << out.kernel_name
       << "(int N, const D4* __restrict__ pos4, const " << T << "* __restrict__ B, " << T
       << "* __restrict__ G, const double* __restrict__ shift, const double* __restrict__ species, "
@@ -188,9 +214,10 @@ CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_flo
       << "  const int i = blockIdx.x * blockDim.x + threadIdx.x;\n"
       << "  if (i >= N) return;\n"
       << "  const size_t n = (size_t)N;\n"
+      << "  const unsigned long long pol = sus2_pol();\n"
       << "  double E = 0.0;\n";
   for (int b = 0; b < Bb; ++b) {
-    src << "  const " << T << " " << v(b) << " = __ldg(B + " << basic_canon[b] << " * n + i);\n";
+    src << "  const " << T << " " << v(b) << " = sus2_ld(B + " << basic_canon[b] << " * n + i, pol);\n";
     src << "  " << T << " " << a(b) << " = " << (weight[b] != 0.0 ? lit(weight[b], use_float) : (use_float ? "0.0f" : "0.0"))
         << ";\n";
     if (is_scalar[b] && weight[b] != 0.0)
@@ -205,8 +232,8 @@ CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_flo
   std::vector<int> canon_basic(ncanon, -1);
   for (int b = 0; b < Bb; ++b) canon_basic[basic_canon[b]] = b;
   for (int c = 0; c < ncanon; ++c) {
-    if (canon_basic[c] >= 0) src << "  G[" << c << " * n + i] = sc * " << a(canon_basic[c]) << ";\n";
-    else src << "  G[" << c << " * n + i] = (" << T << ")0;\n";
+    if (canon_basic[c] >= 0) src << "  sus2_st(G + " << c << " * n + i, sc * " << a(canon_basic[c]) << ", pol);\n";
+    else src << "  sus2_st(G + " << c << " * n + i, (" << T << ")0, pol);\n";
   }
   src << "}\n";
   out.code = src.str();

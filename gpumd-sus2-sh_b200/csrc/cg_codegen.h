@@ -32,6 +32,13 @@ struct CgSource {
   int components = 0;      // independent components (split kernels)
 };
 
+// Device helpers at the head of every generated kernel: sus2_pol() (an L2
+// evict-first cache policy), sus2_ld(p, pol) and sus2_st(p, v, pol) for the
+// basic moments read and their adjoints written, so that these streams do not
+// evict the kernel's own code from L2 (see edge::l2_evict_first).  Defined for
+// the device compiler only.
+extern const char* const kCgStreamHelpers;
+
 // Emits the kernel source.  basic_canon[b] is the canonical [k*C + l*l+l+m]
 // row of model basic b in the B/G arrays; ncanon = K*C.
 CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_float,

@@ -563,7 +563,8 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
       << "  const size_t n = (size_t)N;\n"
       << "  " << T << "* sv = reinterpret_cast<" << T << "*>(smem_raw) + threadIdx.x;\n"
       << "  " << T << "* sa = sv + " << nglob << " * " << block << ";\n";
-  for (int b = 0; b < Bb; ++b) src << "  " << sv(b) << " = __ldg(B + " << basic_canon[b] << " * n + i);\n";
+  src << "  const unsigned long long pol = sus2_pol();\n";
+  for (int b = 0; b < Bb; ++b) src << "  " << sv(b) << " = sus2_ld(B + " << basic_canon[b] << " * n + i, pol);\n";
   src << "  for (int s = 0; s < " << nglob << "; ++s) sa[s * " << block << "] = (" << T << ")0;\n"
       << "  double E = 0.0;\n"
       << calls.str()
@@ -575,14 +576,14 @@ bool generate_cg_split_source(const HostModel& m, const Layered& lay, bool use_f
   std::vector<int> canon_basic(ncanon, -1);
   for (int b = 0; b < Bb; ++b) canon_basic[basic_canon[b]] = b;
   for (int c = 0; c < ncanon; ++c) {
-    if (canon_basic[c] >= 0) src << "  G[" << c << " * n + i] = sc * " << sa(canon_basic[c]) << ";\n";
-    else src << "  G[" << c << " * n + i] = (" << T << ")0;\n";
+    if (canon_basic[c] >= 0) src << "  sus2_st(G + " << c << " * n + i, sc * " << sa(canon_basic[c]) << ", pol);\n";
+    else src << "  sus2_st(G + " << c << " * n + i, (" << T << ")0, pol);\n";
   }
   src << "}\n";
   std::ostringstream head;
   head << "// generated SUS2-SH component-split CG product kernel (" << (use_float ? "FP32" : "FP64") << ", "
        << comps.size() << " components, " << nglob << " shared-memory slots per atom)\n"
-       << "struct D4 { double x, y, z, w; };\n";
+       << "struct D4 { double x, y, z, w; };\n" << kCgStreamHelpers;
   // one translation unit, and the same program as parallel units: the kernel
   // with declarations, then the definitions in chunks of similar size
   out->units.clear();

@@ -99,11 +99,12 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
           acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], P[l * l + m], acc[k * C + l * l + m]);
   }
   if (cut) a.cut_count[i] = ncut;
+  const unsigned long long pol = l2_evict_first();
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int c = 0; c < C; ++c)
-      B[static_cast<size_t>(k * C + c) * a.N + i] = T(sh_poly_norm<L>(c)) * acc[k * C + c];
+      st_stream(B + static_cast<size_t>(k * C + c) * a.N + i, T(sh_poly_norm<L>(c)) * acc[k * C + c], pol);
 }
 
 // ---------------------------------------------------------------------------
@@ -151,11 +152,12 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
   // adjoints scaled by the harmonic normalisation, so every edge works with
   // the bare polynomials P_lm (Y_lm = c_lm P_lm)
   T g[NB];
+  const unsigned long long pol = l2_evict_first();
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int c = 0; c < C; ++c)
-      g[k * C + c] = (wscale * T(sh_poly_norm<L>(c))) * G[static_cast<size_t>(k * C + c) * a.N + i];
+      g[k * C + c] = (wscale * T(sh_poly_norm<L>(c))) * ld_stream(G + static_cast<size_t>(k * C + c) * a.N + i, pol);
   T fx = T(0), fy = T(0), fz = T(0);
   T w[9];
 #pragma unroll

@@ -119,6 +119,9 @@ _PRELUDE = r"""
 struct EmuDim { unsigned x; };
 static EmuDim threadIdx, blockIdx, blockDim;
 template <class T> static inline T __ldg(const T* p) { return *p; }
+static inline unsigned long long sus2_pol() { return 0; }
+template <class T> static inline T sus2_ld(const T* p, unsigned long long) { return *p; }
+template <class T> static inline void sus2_st(T* p, T v, unsigned long long) { *p = v; }
 static inline long long __double_as_longlong(double d) { long long v; std::memcpy(&v, &d, 8); return v; }
 using std::fma;
 using std::fmaf;
@@ -151,7 +154,7 @@ def _emulate(path, split, tmp_path, N=45, seed=3):
     assert rc == 0, _lib.load().sus2sh_last_error().decode()
     name = re.search(r"(sus2sh_cg\w+)\(int N", src).group(1)
     block = info["block"]
-    canon = dict((int(b), int(c)) for b, c in re.findall(r"(?:sv\[|v)(\d+)(?: \* \d+\])? = __ldg\(B \+ (\d+) \* n", src))
+    canon = dict((int(b), int(c)) for b, c in re.findall(r"(?:sv\[|v)(\d+)(?: \* \d+\])? = sus2_ld\(B \+ (\d+) \* n", src))
     cpp = tmp_path / "k.cpp"
     cpp.write_text(_PRELUDE + src.replace('extern "C" __global__', "__global__") + _DRIVER.replace("KERNEL", name))
     so = tmp_path / "k.so"
