@@ -453,6 +453,23 @@ struct Engine {
   CgBinary pg_bin;
   CgModule pg_mod;
   double cg_compile_ms = 0.0;
+  // fused persistent batch kernel (batch_fused.cuh, option
+  // sus2_sh_batch_fused=1): FP32 models with the straight-line CG kernel and
+  // model-specialised edge kernels, no gate and no ZBL; built, and its
+  // variant and tile size picked by timing, at the first batch call.  On the
+  // 4096-cell l3k3 batch it runs 3.53 ms per evaluation against 2.13 ms for
+  // the stage kernels (12 warps per SM at 168 registers, CTAs waiting at the
+  // per-tile barriers, lanes idle in a tile's last partial block), so the
+  // stage kernels are the default
+  std::vector<float> model_table;  // coefficient table of the model-specialised edge build
+  bool fused_tried = false;
+  std::shared_ptr<const FusedJitBinary> fused_bin;
+  std::vector<std::unique_ptr<CgModule>> fused_mods;  // one per compiled variant
+  int fused_variant = 0, fused_tile = 512;
+  bool fused_tuned = false;
+  double fused_compile_ms = 0.0;
+  DevBuf<int> d_tile_ctr;
+  int sm_count = 0;
 
   ~Engine() {
     if (nbr_exec) cudaGraphExecDestroy(nbr_exec);
@@ -589,6 +606,7 @@ struct Engine {
       // built on host threads while the CG kernel below compiles
       std::vector<float> table(kMaxCoef);
       table.resize(fill_coef(coef, dcoef, table.data()));
+      model_table = table;
       model_edges = std::async(std::launch::async, [l = model.l_max, k = model.k_max, rb = model.rb_size, table,
                                                     shared_xi = rs.shared_xi != 0, kind = rs.kind] {
         return compile_model_edge_kernels(l, k, rb, table, shared_xi, kind);
@@ -835,7 +853,7 @@ struct Engine {
   // with a given (N, ncells) nothing synchronises or allocates, so the call
   // can be captured in a CUDA graph.
   void prepare_batch(cudaStream_t s, int n, int ncells, const int* off, const double* cell_h, const int* cell_pbc,
-                     const int* type, const double* x) {
+                     const int* type, const double* x, bool fill_lists = true) {
     inner_valid = false;  // the batch list holds only pairs within rc
     cut_valid = false;  // new positions
     if (ncells <= 0) throw InputError("sus2sh batch: ncells must be positive.");
@@ -869,10 +887,133 @@ struct Engine {
       grow_capacity(st.max_count);
       launches += 2;
     }
-    launch_batch_fill(s, N, ncells, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nbr.p, ncount.p,
-                      cap, 0, d_status.p);
-    launches += 2;
+    if (fill_lists) {  // (the fused batch kernel fills them itself)
+      launch_batch_fill(s, N, ncells, off, d_batch_cell.p, pos4.p, cell_h, d_cell_reach.p, cutoff2, nbr.p,
+                        ncount.p, cap, 0, d_status.p);
+      launches += 2;
+    }
     ck(cudaGetLastError(), "batch neighbour build launch");
+  }
+
+  // The fused batch kernel for this model, built at the first batch call;
+  // false (stage kernels) when the model is not of the kind it covers, the
+  // option turns it off or its build fails.
+  bool fused_available() {
+    if (fused_tried) return fused_bin != nullptr;
+    fused_tried = true;
+    if (!opt.batch_fused || !use_float || gate || model.zbl_enabled || edge_jit != 2 || !ejit_bin ||
+        !ejit_bin->model_coef || cg_bin.cubin.empty() || cg_src.split || cg_src.device_fn.empty())
+      return false;
+    try {
+      const std::vector<std::pair<int, int>> variants = {{128, 3}, {128, 2}};
+      auto bin = compile_batch_fused(model.l_max, model.k_max, model.rb_size, model_table, rs.shared_xi != 0, rs.kind,
+                                     cg_src.device_fn, variants);
+      std::vector<std::unique_ptr<CgModule>> mods;
+      for (size_t v = 0; v < bin->names.size(); ++v) {
+        CgBinary cb;
+        cb.cubin = bin->cubin;
+        auto mod = std::make_unique<CgModule>();
+        std::string err;
+        if (!mod->load(cb, bin->names[v], &err, fused_smem(kFusedMaxTile))) throw CudaError(err);
+        mods.push_back(std::move(mod));
+      }
+      cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
+      d_tile_ctr.resize(2);
+      ck(cudaMemset(d_tile_ctr.p, 0, 2 * sizeof(int)), "memset");
+      fused_mods = std::move(mods);
+      fused_compile_ms = bin->compile_ms;
+      fused_bin = bin;
+    } catch (const std::exception&) {
+      fused_bin.reset();
+      fused_mods.clear();
+    }
+    return fused_bin != nullptr;
+  }
+
+  // Largest tile the timing picks from, and the shared memory of a tile size:
+  // the pair table and an FP32 force buffer of 2 tiles + 1024 atoms (a tile
+  // holds at most tile - 1 atoms plus its last cell).
+  static constexpr int kFusedMaxTile = 1024;
+  static int fused_buf_atoms(int tile) { return 2 * tile + 1024; }
+  size_t fused_smem(int tile) const {
+    return (edge_smem<float>() + 15) / 16 * 16 + 3 * sizeof(float) * static_cast<size_t>(fused_buf_atoms(tile));
+  }
+
+  void launch_fused(cudaStream_t s, int variant, int tile, int ncells, const int* off, const double* cell_h,
+                    double* pe, double* force, double* virial, double* cell_energy, double* cell_virial) {
+    EdgeArgs<float> a = edge_args<float>();
+    a.cut_nbr = nullptr;  // the batch list holds pairs within rc only
+    a.use_cut = 0;
+    batch::FusedArgs f{};
+    f.ncells = ncells;
+    f.ntiles = N / tile + 1;
+    f.tile_atoms = tile;
+    f.buf_atoms = fused_buf_atoms(tile);
+    f.off = off;
+    f.shift_coeffs = d_shift.p;
+    f.species_coeffs = d_species.p;
+    f.pe = pe;
+    f.force = force;
+    f.virial = virial;
+    f.cell_energy = cell_energy;
+    f.cell_virial = cell_virial;
+    f.tile_counter = d_tile_ctr.p;
+    f.fill = 1;
+    f.cell_h = cell_h;
+    f.cell_reach = d_cell_reach.p;
+    f.cutoff2 = list_cutoff * list_cutoff;
+    f.nbr = nbr.p;
+    f.ncount = ncount.p;
+    f.cap = cap;
+    f.st = d_status.p;
+    CgModule& mod = *fused_mods[variant];
+    const int block = fused_bin->blocks[variant];
+    const size_t smem = fused_smem(tile);
+    const int per_sm = std::max(1, mod.max_active_blocks(block, smem));
+    const unsigned grid = static_cast<unsigned>(std::min<long long>(f.ntiles, static_cast<long long>(per_sm) * sm_count));
+    void* args[] = {&a, &f};
+    std::string err;
+    if (!mod.launch_args(s, grid, static_cast<unsigned>(block), smem, args, &err)) throw CudaError(err);
+    launches += 1;
+  }
+
+  // Variant and tile size of the fused kernel, timed once per handle on the
+  // first batch (scratch outputs; this call synchronises anyway, for the
+  // neighbour capacity); sus2_sh_batch_tile fixes the tile size.
+  void tune_fused(cudaStream_t s, int ncells, const int* off, const double* cell_h) {
+    DevBuf<double> pe_s, f_s, w_s, ce_s, cw_s;
+    pe_s.resize(N);
+    f_s.resize(3ull * N);
+    w_s.resize(9ull * N);
+    ce_s.resize(ncells);
+    cw_s.resize(9ull * ncells);
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "cudaEventCreate");
+    ck(cudaEventCreate(&e1), "cudaEventCreate");
+    std::vector<int> tiles = {256, 512, kFusedMaxTile};
+    if (opt.batch_tile > 0) tiles = {std::min(opt.batch_tile, kFusedMaxTile)};
+    float best = 1e30f;
+    for (size_t v = 0; v < fused_mods.size(); ++v)
+      for (int tile : tiles) {
+        auto run = [&] {
+          launch_fused(s, static_cast<int>(v), tile, ncells, off, cell_h, pe_s.p, f_s.p, w_s.p, ce_s.p, cw_s.p);
+        };
+        run();  // warm
+        ck(cudaEventRecord(e0, s), "cudaEventRecord");
+        run();
+        ck(cudaEventRecord(e1, s), "cudaEventRecord");
+        ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+        float ms = 0.0f;
+        ck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+        if (ms < best) {
+          best = ms;
+          fused_variant = static_cast<int>(v);
+          fused_tile = tile;
+        }
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ck(cudaGetLastError(), "fused batch tuning");
   }
 
   // Positions -> pos4, conditional neighbour build.
@@ -1441,7 +1582,20 @@ int sus2sh_compute_batch(sus2sh_handle* h, int N, int ncells, const int* cell_of
   return guarded([&] {
     sus2sh::Engine& e = h->e;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    e.prepare_batch(s, N, ncells, cell_offset, cell_h, cell_pbc, type, position);
+    const bool fused = e.fused_available();
+    e.prepare_batch(s, N, ncells, cell_offset, cell_h, cell_pbc, type, position, !fused);
+    if (fused) {
+      // one persistent launch: neighbour fill, moments, CG products, forces,
+      // per-cell sums
+      if (!e.fused_tuned) {
+        e.fused_tuned = true;
+        e.tune_fused(s, ncells, cell_offset, cell_h);
+      }
+      e.launch_fused(s, e.fused_variant, e.fused_tile, ncells, cell_offset, cell_h, potential, force, virial,
+                     cell_energy, cell_virial);
+      e.finish(s);
+      return;
+    }
     if (e.use_float) {
       e.forward_impl<float>(s, potential, 0);
       e.backward_impl<float>(s, nullptr, force, virial, 1.0);
@@ -1548,7 +1702,7 @@ int sus2sh_sync(sus2sh_handle* h, int* status_flags) {
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
   if (!h || !out) return 0;
   const sus2sh::Engine& e = h->e;
-  const int v[36] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
+  const int v[41] = {e.model.species_count, e.model.l_max, e.model.k_max, e.model.body_order,
                      e.model.rb_size, e.model.basic_count, e.model.moments,
                      static_cast<int>(e.model.products.size()), e.model.scalar_count,
                      static_cast<int>(e.lay.rows.size()), e.lay.max_layer, e.prog.terminal_rows,
@@ -1562,8 +1716,12 @@ int sus2sh_model_info(const sus2sh_handle* h, int* out, int n) {
                      e.gate ? static_cast<int>(e.model.gate.mode) : 0,
                      e.cg_bin.cubin.empty() ? 0 : (e.cg_src.split ? 2 : 1),
                      e.cg_mod.registers(), e.cg_mod.local_bytes(),
-                     e.cg_bin.cubin.empty() ? 0 : (e.cg_bin.whole ? 1 : 2), e.cg_bin.from_disk ? 1 : 0};
-  const int k = std::min(n, 36);
+                     e.cg_bin.cubin.empty() ? 0 : (e.cg_bin.whole ? 1 : 2), e.cg_bin.from_disk ? 1 : 0,
+                     e.fused_bin ? 1 : 0,
+                     e.fused_bin ? e.fused_bin->registers[e.fused_variant] : -1,
+                     e.fused_bin ? e.fused_bin->blocks[e.fused_variant] * 100 + e.fused_bin->min_blocks[e.fused_variant] : 0,
+                     e.fused_bin ? e.fused_tile : 0, static_cast<int>(e.fused_compile_ms)};
+  const int k = std::min(n, 41);
   for (int i = 0; i < k; ++i) out[i] = v[i];
   return k;
 }
@@ -1664,21 +1822,35 @@ int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_r
   });
 }
 
+}  // extern "C"
+
+namespace {
+// The model-specialised edge build's inputs for a model file, as the engine
+// derives them at load: the coefficient table (c[mu][n], then the derivative
+// series when it fits) and whether every radial function of every pair has
+// the (scal, shift) of the pair's first function.
+void model_edge_inputs(const sus2sh::HostModel& m, std::vector<float>* table, bool* shared) {
+  const std::vector<double> dc = sus2sh::radial_derivative(m.radial_map, m.radial_coeffs, m.radial_funcs, m.rb_size);
+  table->assign(sus2sh::kMaxCoef, 0.0f);
+  table->resize(sus2sh::Engine::fill_coef(m.radial_coeffs, dc, table->data()));
+  const int S = m.species_count, kmu = m.radial_funcs;
+  *shared = true;
+  for (int p = 0; p < S * S; ++p)
+    for (int mu = 0; mu < kmu; ++mu)
+      *shared = *shared && m.scal_coeffs[2 * mu * S * S + p] == m.scal_coeffs[p] &&
+                m.scal_coeffs[2 * mu * S * S + S * S + p] == m.scal_coeffs[S * S + p];
+}
+}  // namespace
+
+extern "C" {
+
 int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t log_len) {
   if (!path || !info) return SUS2SH_E_ARG;
   return guarded([&] {
     const sus2sh::HostModel m = sus2sh::load_model(path);
-    const std::vector<double> dc = sus2sh::radial_derivative(m.radial_map, m.radial_coeffs, m.radial_funcs, m.rb_size);
-    std::vector<float> table(sus2sh::kMaxCoef);
-    table.resize(sus2sh::Engine::fill_coef(m.radial_coeffs, dc, table.data()));
-    // one radial argument per pair when every function of every pair has the
-    // (scal, shift) of the pair's first function (as the engine finds at load)
-    const int S = m.species_count, kmu = m.radial_funcs;
+    std::vector<float> table;
     bool shared = true;
-    for (int p = 0; p < S * S; ++p)
-      for (int mu = 0; mu < kmu; ++mu)
-        shared = shared && m.scal_coeffs[2 * mu * S * S + p] == m.scal_coeffs[p] &&
-                 m.scal_coeffs[2 * mu * S * S + S * S + p] == m.scal_coeffs[S * S + p];
+    model_edge_inputs(m, &table, &shared);
     const auto bin = sus2sh::compile_model_edge_kernels(m.l_max, m.k_max, m.rb_size, table, shared,
                                                         static_cast<int>(m.radial_map));
     info[0] = bin->basic_registers;
@@ -1689,6 +1861,33 @@ int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t
     size_t bytes = 0;
     for (const auto& c : bin->cubins) bytes += c.size();
     info[5] = static_cast<int>(bytes);
+    if (log && log_len) {
+      std::strncpy(log, bin->log.c_str(), log_len - 1);
+      log[log_len - 1] = '\0';
+    }
+  });
+}
+
+int sus2sh_batch_kernel_info(const char* path, int* info, char* log, size_t log_len) {
+  if (!path || !info) return SUS2SH_E_ARG;
+  return guarded([&] {
+    const sus2sh::HostModel m = sus2sh::load_model(path);
+    const sus2sh::Layered lay = sus2sh::layer_products(m);
+    const sus2sh::ProgramHost prog = sus2sh::compile_program(m, lay);
+    sus2sh::CgSource src;
+    std::string why;
+    if (!sus2sh::choose_cg_source(m, lay, prog.basic_canon, prog.ncanon, true, -1, &src, &why) || src.split ||
+        src.device_fn.empty())
+      throw sus2sh::InputError("no fused batch kernel for this model: its CG graph takes the component-split kernel");
+    std::vector<float> table;
+    bool shared = true;
+    model_edge_inputs(m, &table, &shared);
+    const auto bin = sus2sh::compile_batch_fused(m.l_max, m.k_max, m.rb_size, table, shared,
+                                                 static_cast<int>(m.radial_map), src.device_fn, {{128, 3}, {128, 2}});
+    info[0] = bin->registers[0];
+    info[1] = bin->registers[1];
+    info[2] = static_cast<int>(bin->compile_ms);
+    info[3] = static_cast<int>(bin->cubin.size());
     if (log && log_len) {
       std::strncpy(log, bin->log.c_str(), log_len - 1);
       log[log_len - 1] = '\0';

@@ -238,6 +238,27 @@ CgSource generate_cg_source(const HostModel& m, const Layered& lay, bool use_flo
   src << "}\n";
   out.code = src.str();
   out.fp_terms = terms;
+  // the same body as a device function on register arrays (canonical order)
+  // for kernels that produce the basics and consume the adjoints themselves
+  std::ostringstream fn;
+  fn << "namespace sus2sh {\nnamespace batch {\n"
+     << "__device__ __forceinline__ double cg_atom(const " << T << " (&B)[" << ncanon << "], " << T << " (&G)["
+     << ncanon << "], " << T << " sc) {\n"
+     << "  double E = 0.0;\n";
+  for (int b = 0; b < Bb; ++b) {
+    fn << "  const " << T << " " << v(b) << " = B[" << basic_canon[b] << "];\n";
+    fn << "  " << T << " " << a(b) << " = " << (weight[b] != 0.0 ? lit(weight[b], use_float) : (use_float ? "0.0f" : "0.0"))
+       << ";\n";
+    if (is_scalar[b] && weight[b] != 0.0)
+      fn << "  E += (double)(" << lit(weight[b], use_float) << " * " << v(b) << ");\n";
+  }
+  fn << body.str();
+  for (int c = 0; c < ncanon; ++c) {
+    if (canon_basic[c] >= 0) fn << "  G[" << c << "] = sc * " << a(canon_basic[c]) << ";\n";
+    else fn << "  G[" << c << "] = (" << T << ")0;\n";
+  }
+  fn << "  return E;\n}\n}  // namespace batch\n}  // namespace sus2sh\n";
+  out.device_fn = fn.str();
   return out;
 }
 
@@ -792,6 +813,14 @@ bool CgModule::load(const CgBinary& bin, const std::string& kernel_name, std::st
   module_ = mod;
   func_ = f;
   return true;
+}
+
+int CgModule::max_active_blocks(int block, size_t smem_bytes) const {
+  using PFN_occ = CUresult (*)(int*, CUfunction, int, size_t);
+  static PFN_occ occ = entry<PFN_occ>("cuOccupancyMaxActiveBlocksPerMultiprocessor");
+  int n = 0;
+  if (!occ || !func_ || occ(&n, static_cast<CUfunction>(func_), block, smem_bytes) != CUDA_SUCCESS) return 0;
+  return n;
 }
 
 bool CgModule::launch_args(void* stream, unsigned grid, unsigned block, size_t smem_bytes, void** args,

@@ -30,6 +30,11 @@ struct CgSource {
   bool split = false;      // component-split kernel (generate_cg_split_source)
   int functions = 1;       // device functions in the program
   int components = 0;      // independent components (split kernels)
+  // straight-line kernels only: the same contraction as a device function
+  // sus2sh::batch::cg_atom(const T (&B)[ncanon], T (&G)[ncanon], T sc) ->
+  // sum of the weighted moments, on the normalised basics B and writing
+  // G = sc * dE/dB (canonical order), for the fused batch kernel
+  std::string device_fn;
 };
 
 // Device helpers at the head of every generated kernel: sus2_pol() (an L2
@@ -114,6 +119,9 @@ class CgModule {
   // the loaded kernel, call tree included (-1 before load).
   int registers() const { return regs_; }
   int local_bytes() const { return local_; }
+  // Resident CTAs per SM of the loaded kernel at this CTA size and dynamic
+  // shared memory (0 on error).
+  int max_active_blocks(int block, size_t smem_bytes) const;
   // Launches with an explicit parameter array.
   bool launch_args(void* stream, unsigned grid, unsigned block, size_t smem_bytes, void** args, std::string* err);
   // Launches with params: N, pos4, B, G, shift, species, pe, pe_assign, on

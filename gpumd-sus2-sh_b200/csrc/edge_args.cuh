@@ -57,4 +57,48 @@ struct EdgeArgs {
   T coef[kMaxCoef];
 };
 
+// Neighbour and input status flags of one engine handle (device, sticky).
+struct Status {
+  unsigned int maxdisp2_bits;  // max |u - ref|^2 since last build (float bits)
+  int rebuilt;                 // a build happened in this call
+  int overflow;                // neighbour capacity exceeded (sticky)
+  int max_count;               // largest neighbour count seen at a build
+  int builds;                  // number of builds
+  int bad_type;                // a species index outside [0, species_count) was seen (sticky)
+  int thin_cell;               // a batch cell thinner than half the cutoff (sticky)
+  int pad;
+};
+
+namespace batch {
+
+// Arguments of the fused batch kernel (batch_fused.cuh) beside its EdgeArgs.
+struct FusedArgs {
+  int ncells;
+  int ntiles;      // N / tile_atoms + 1
+  int tile_atoms;  // TA
+  int buf_atoms;   // capacity of the shared-memory force buffer (atoms)
+  const int* off;  // cell offsets [ncells + 1]
+  const double* shift_coeffs;    // per-species energy shift
+  const double* species_coeffs;  // per-species c_t
+  double* pe;                    // [N], accumulated
+  double* force;                 // [3][N], accumulated
+  double* virial;                // [9][N], accumulated (may be NULL)
+  double* cell_energy;           // [ncells], assigned (may be NULL)
+  double* cell_virial;           // [9 ncells], assigned (may be NULL)
+  int* tile_counter;             // [2]: next tile, CTAs done; zero between launches
+  // fill = 1: each tile first builds its cells' neighbour lists (the batch
+  // fill of batch_fill.cuh, into nbr / ncount with capacity cap, cutoff^2
+  // cutoff2, status flags in st); 0: the lists are already built
+  int fill;
+  const double* cell_h;          // [9 ncells]
+  const int* cell_reach;         // [3 ncells]
+  double cutoff2;
+  int* nbr;                      // [cap][N]
+  int* ncount;                   // [N]
+  int cap;
+  Status* st;
+};
+
+}  // namespace batch
+
 }  // namespace sus2sh

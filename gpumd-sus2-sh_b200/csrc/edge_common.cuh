@@ -231,8 +231,8 @@ struct NeighborStream {
 
   __device__ __forceinline__ NeighborStream(const int* nb, const double4* p4, int N, int i, int count)
       : nbr(nb + i), pos4(p4), stride(static_cast<size_t>(N)), cnt(count) {
-    w_next = cnt > 0 ? __ldg(nbr) : 0;
-    w_next2 = cnt > 1 ? __ldg(nbr + stride) : 0;
+    w_next = cnt > 0 ? word(nbr) : 0;
+    w_next2 = cnt > 1 ? word(nbr + stride) : 0;
     p_next = cnt > 0 ? pos4[w_next & 0xFFFFFF] : make_double4(0.0, 0.0, 0.0, 0.0);
   }
   // Returns edge n's word and position and issues the loads for n+1 / n+2.
@@ -241,7 +241,17 @@ struct NeighborStream {
     pj = p_next;
     w_next = w_next2;
     if (n + 1 < cnt) p_next = pos4[w_next & 0xFFFFFF];
-    if (n + 2 < cnt) w_next2 = __ldg(nbr + static_cast<size_t>(n + 2) * stride);
+    if (n + 2 < cnt) w_next2 = word(nbr + static_cast<size_t>(n + 2) * stride);
+  }
+  // Neighbour words through the read-only data path, or, in a kernel that
+  // writes the lists itself before reading them (SUS2_NBR_WRITTEN_IN_KERNEL),
+  // through plain loads, which see the kernel's own earlier writes.
+  __device__ __forceinline__ static int word(const int* p) {
+#ifdef SUS2_NBR_WRITTEN_IN_KERNEL
+    return *p;
+#else
+    return __ldg(p);
+#endif
   }
 };
 

@@ -222,6 +222,60 @@ std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k
   });
 }
 
+std::shared_ptr<const FusedJitBinary> compile_batch_fused(int l_max, int k_max, int rb, const std::vector<float>& coef,
+                                                          bool shared_xi, int radial_kind, const std::string& cg_fn,
+                                                          const std::vector<std::pair<int, int>>& variants) {
+  static std::mutex mu;
+  static std::map<std::string, std::shared_ptr<const FusedJitBinary>> done;
+  const std::string src = coef_prelude(coef, shared_xi, radial_kind) + "#include \"edge_kernels.cuh\"\n" + cg_fn +
+                          "#include \"batch_fused.cuh\"\n";
+  std::vector<std::string> expr;
+  for (const auto& v : variants)
+    expr.push_back("&sus2sh::batch::k_batch_fused<" + std::to_string(l_max) + ", " + std::to_string(k_max) + ", " +
+                   std::to_string(rb) + ", " + std::to_string(v.first) + ", " + std::to_string(v.second) + ">");
+  std::string key = src;
+  for (const std::string& e : expr) key += "\n" + e;
+  std::lock_guard<std::mutex> lock(mu);  // one build at a time; later handles of the model reuse it
+  auto it = done.find(key);
+  if (it != done.end()) return it->second;
+  const auto t0 = std::chrono::steady_clock::now();
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, src.c_str(), "sus2sh_batch_fused.cu", kJitHeaderCount, kJitHeaderSources,
+                         kJitHeaderNames) != NVRTC_SUCCESS)
+    throw InputError("NVRTC could not create the fused batch program.");
+  for (const std::string& e : expr) nvrtcAddNameExpression(prog, e.c_str());
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=true", "--ptxas-options=--verbose",
+                        "--generate-line-info"};
+  const nvrtcResult rc = nvrtcCompileProgram(prog, 5, opts);
+  auto out = std::make_shared<FusedJitBinary>();
+  size_t log_size = 0;
+  nvrtcGetProgramLogSize(prog, &log_size);
+  if (log_size > 1) {
+    out->log.resize(log_size);
+    nvrtcGetProgramLog(prog, &out->log[0]);
+    out->log.resize(std::strlen(out->log.c_str()));
+  }
+  if (rc != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    throw InputError("NVRTC failed to compile the fused batch kernel: " + out->log.substr(0, 2000));
+  }
+  for (size_t v = 0; v < variants.size(); ++v) {
+    const char* lowered = nullptr;
+    nvrtcGetLoweredName(prog, expr[v].c_str(), &lowered);
+    out->names.push_back(lowered ? lowered : "");
+    out->blocks.push_back(variants[v].first);
+    out->min_blocks.push_back(variants[v].second);
+    out->registers.push_back(registers_of(out->log, out->names.back()));
+  }
+  size_t n = 0;
+  nvrtcGetCUBINSize(prog, &n);
+  out->cubin.resize(n);
+  nvrtcGetCUBIN(prog, out->cubin.data());
+  nvrtcDestroyProgram(&prog);
+  out->compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return done.emplace(key, out).first->second;
+}
+
 using namespace drv;
 
 EdgeJitModule::~EdgeJitModule() {

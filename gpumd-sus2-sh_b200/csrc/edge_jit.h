@@ -11,6 +11,7 @@
 
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace sus2sh {
@@ -45,6 +46,24 @@ std::shared_ptr<const EdgeJitBinary> compile_edge_kernels(bool fp32, int l_max, 
 std::shared_ptr<const EdgeJitBinary> compile_model_edge_kernels(int l_max, int k_max, int rb,
                                                                 const std::vector<float>& coef, bool shared_xi,
                                                                 int radial_kind);
+
+// The fused batch kernel k_batch_fused<L, K, RB, BLOCK, MIN_BLOCKS>
+// (batch_fused.cuh) of one FP32 model: the radial coefficients, shared-
+// argument flag and radial kind compiled in as for
+// compile_model_edge_kernels, and cg_fn, the model's straight-line CG
+// contraction as a device function (CgSource::device_fn).  One NVRTC program
+// with a kernel per (BLOCK, MIN_BLOCKS) variant; cached per process by its
+// source.
+struct FusedJitBinary {
+  std::vector<char> cubin;
+  std::vector<std::string> names;  // lowered kernel names, one per variant
+  std::vector<int> blocks, min_blocks, registers;
+  std::string log;
+  double compile_ms = 0.0;
+};
+std::shared_ptr<const FusedJitBinary> compile_batch_fused(int l_max, int k_max, int rb, const std::vector<float>& coef,
+                                                          bool shared_xi, int radial_kind, const std::string& cg_fn,
+                                                          const std::vector<std::pair<int, int>>& variants);
 
 // Module of one compiled shape, loaded into the current context.
 class EdgeJitModule {

@@ -35,19 +35,13 @@ namespace edge {
 // ---------------------------------------------------------------------------
 // GATE: two-layer gate models' main pass, every R_mu of neighbour j scaled by
 // the gate multiplier G_{j,mu} (gpu_sh_compute_basic_gate_main, sus2_sh.cu:4247-4314).
-template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
-__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1) <= 64 &&
-                                                 SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1
-                                             ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK
-                                             : 1)
-    k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_tab = reinterpret_cast<T*>(smem_raw);
-  load_pair_table(a, s_tab);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
+// Unnormalised basic moments acc[k*C + l*l + m] = sum_j R_kl P_lm of centre
+// i over its list (the inner list when the engine keeps one); the pairs
+// inside rc are appended to the atom's cut_nbr column when it is set.
+template <typename T, int L, int K, int RB, bool GATE>
+__device__ __forceinline__ void atom_basic(const EdgeArgs<T>& a, const T* __restrict__ s_tab, int i,
+                                           T (&acc)[K * (L + 1) * (L + 1)]) {
   constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
-  T acc[NB];
 #pragma unroll
   for (int b = 0; b < NB; ++b) acc[b] = T(0);
   const double4 pi = a.pos4[i];
@@ -99,6 +93,22 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
           acc[k * C + l * l + m] = fma(R[k * (L + 1) + l], P[l * l + m], acc[k * C + l * l + m]);
   }
   if (cut) a.cut_count[i] = ncut;
+}
+
+template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
+__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1) <= 64 &&
+                                                 SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK > 1
+                                             ? SUS2_BASIC_MIN_BLOCKS * 128 / BLOCK
+                                             : 1)
+    k_basic(const EdgeArgs<T> a, T* __restrict__ B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_tab = reinterpret_cast<T*>(smem_raw);
+  load_pair_table(a, s_tab);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  constexpr int C = (L + 1) * (L + 1), NB = K * C;
+  T acc[NB];
+  atom_basic<T, L, K, RB, GATE>(a, s_tab, i, acc);
   const unsigned long long pol = l2_evict_first();
 #pragma unroll
   for (int k = 0; k < K; ++k)
@@ -134,32 +144,17 @@ struct Scatter<double> {
 // R_mu sum_m g_{mu,m} Y_m accumulated on the neighbour.
 // The register cap applies to shapes whose adjoints fit it (K (L+1)^2 <= 64);
 // larger shapes keep up to 255 registers.  The same holds for k_basic.
-template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
-__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1) <= 64 &&
-                                                 SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1
-                                             ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK
-                                             : 1)
-    k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
-            void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
-            double sign) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_tab = reinterpret_cast<T*>(smem_raw);
-  load_pair_table(a, s_tab);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
-  constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1), NB = K * C;
-  const T wscale = weight ? static_cast<T>(weight[i]) : T(1);
-  // adjoints scaled by the harmonic normalisation, so every edge works with
-  // the bare polynomials P_lm (Y_lm = c_lm P_lm)
-  T g[NB];
-  const unsigned long long pol = l2_evict_first();
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-#pragma unroll
-    for (int c = 0; c < C; ++c)
-      g[k * C + c] = (wscale * T(sh_poly_norm<L>(c))) * ld_stream(G + static_cast<size_t>(k * C + c) * a.N + i, pol);
-  T fx = T(0), fy = T(0), fz = T(0);
-  T w[9];
+// Force and virial of centre i's edges from its adjoints g, pre-scaled by the
+// harmonic normalisation (g'_klm = c_lm g_klm, so every edge works with the
+// bare polynomials P_lm): the self force is summed into fx, fy, fz, the
+// per-atom virial into w, and each neighbour's reaction -dE goes to
+// scatter(j, x, y, z).
+template <typename T, int L, int K, int RB, bool GATE, class Scatter_>
+__device__ __forceinline__ void atom_force(const EdgeArgs<T>& a, const T* __restrict__ s_tab, int i,
+                                           const T (&g)[K * (L + 1) * (L + 1)], T& fx, T& fy, T& fz, T (&w)[9],
+                                           Scatter_ scatter) {
+  constexpr int C = (L + 1) * (L + 1), KMU = K * (L + 1);
+  fx = fy = fz = T(0);
 #pragma unroll
   for (int q = 0; q < 9; ++q) w[q] = T(0);
   const double4 pi = a.pos4[i];
@@ -282,7 +277,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
     fx += dEx;
     fy += dEy;
     fz += dEz;
-    Scatter<T>::add(ftmp, j, -dEx, -dEy, -dEz);
+    scatter(j, -dEx, -dEy, -dEz);
     w[0] -= e.dx * dEx;
     w[1] -= e.dy * dEy;
     w[2] -= e.dz * dEz;
@@ -293,6 +288,34 @@ __global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1)
     w[7] -= e.dz * dEx;
     w[8] -= e.dz * dEy;
   }
+}
+
+template <typename T, int L, int K, int RB, int BLOCK, bool GATE = false>
+__global__ void __launch_bounds__(BLOCK, sizeof(T) == 4 && K * (L + 1) * (L + 1) <= 64 &&
+                                                 SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK > 1
+                                             ? SUS2_FORCE_MIN_BLOCKS * 128 / BLOCK
+                                             : 1)
+    k_force(const EdgeArgs<T> a, const T* __restrict__ G, const double* __restrict__ weight,
+            void* __restrict__ ftmp, double* __restrict__ force, double* __restrict__ virial,
+            double sign) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_tab = reinterpret_cast<T*>(smem_raw);
+  load_pair_table(a, s_tab);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  constexpr int C = (L + 1) * (L + 1), NB = K * C;
+  const T wscale = weight ? static_cast<T>(weight[i]) : T(1);
+  T g[NB];
+  const unsigned long long pol = l2_evict_first();
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+      g[k * C + c] = (wscale * T(sh_poly_norm<L>(c))) * ld_stream(G + static_cast<size_t>(k * C + c) * a.N + i, pol);
+  T fx, fy, fz;
+  T w[9];
+  atom_force<T, L, K, RB, GATE>(a, s_tab, i, g, fx, fy, fz, w,
+                                [ftmp](int j, T x, T y, T z) { Scatter<T>::add(ftmp, j, x, y, z); });
   force[i] += sign * static_cast<double>(fx);
   force[i + a.N] += sign * static_cast<double>(fy);
   force[i + 2 * a.N] += sign * static_cast<double>(fz);

@@ -31,17 +31,6 @@ struct BoxGeom {
   double shift[125][3];  // Cartesian image vectors of codes (base 5, -2..2)
 };
 
-struct Status {
-  unsigned int maxdisp2_bits;  // max |u - ref|^2 since last build (float bits)
-  int rebuilt;                 // a build happened in this call
-  int overflow;                // neighbour capacity exceeded (sticky)
-  int max_count;               // largest neighbour count seen at a build
-  int builds;                  // number of builds
-  int bad_type;                // a species index outside [0, species_count) was seen (sticky)
-  int thin_cell;               // a batch cell thinner than half the cutoff (sticky)
-  int pad;
-};
-
 struct ProgramDev {
   int nrows;
   int nvalue;         // value slots; grad slot of v is v + nvalue

@@ -922,6 +922,12 @@ Options parse_options(const HostModel& m, int nopts, const char** opts) {
       o.model_edges = parse_bool(val, key);
     } else if (key == "sus2_sh_neighbor_graph") {
       o.neighbor_graph = parse_bool(val, key);
+    } else if (key == "sus2_sh_batch_fused") {
+      o.batch_fused = parse_bool(val, key);
+    } else if (key == "sus2_sh_batch_tile") {
+      o.batch_tile = std::atoi(val.c_str());
+      if (o.batch_tile < 0 || o.batch_tile > (1 << 20))
+        throw InputError("sus2_sh_batch_tile must be between 0 and 1048576 atoms.");
     } else if (key == "sus2_sh_cg_jit") {
       o.cg_jit = parse_bool(val, key);
     } else if (key == "sus2_sh_cg_split") {

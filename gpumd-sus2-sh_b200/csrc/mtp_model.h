@@ -148,6 +148,11 @@ struct Options {
                                     // the radial coefficients from their parameters
   bool neighbor_graph = true;       // sus2_sh_neighbor_graph=0 launches the neighbour-build kernels
                                     // on every call instead of a graph that skips them
+  bool batch_fused = false;         // sus2_sh_batch_fused=1 evaluates batches of cells with the
+                                    // fused persistent kernel instead of the stage kernels
+                                    // (measured slower on the 4096-cell batch: 3.53 vs 2.13 ms)
+  int batch_tile = 0;               // sus2_sh_batch_tile=<atoms>: tile size of the fused batch
+                                    // kernel (0: picked by timing at the first batch call)
 };
 // Options start after the species symbols (sus2_sh.cu:527); unknown tokens of
 // the reference's tuning switches are accepted and ignored.

@@ -18,7 +18,7 @@ EXPORTS = (
     "sus2sh_compute_host", "sus2sh_model_info", "sus2sh_profile", "sus2sh_profile_read",
     "sus2sh_cg_energy_noalloc", "sus2sh_param_grad", "sus2sh_compute_batch", "sus2sh_param_grad_batch",
     "sus2sh_cg_kernel_info", "sus2sh_zbl_pair", "sus2sh_real_sh", "sus2sh_edge_kernel_info",
-    "sus2sh_model_edge_kernel_info",
+    "sus2sh_model_edge_kernel_info", "sus2sh_batch_kernel_info",
 )
 TOOLS_EXPORTS = (
     "sus2sh_tools_last_error", "sus2sh_write_synthetic_model", "sus2sh_standard_graph_counts",
@@ -66,6 +66,7 @@ def load() -> ctypes.CDLL:
         "sus2sh_real_sh": (I, [I, D, D, D, P, P, P]),
         "sus2sh_edge_kernel_info": (I, [I, I, I, I, P, P, P, ctypes.c_char_p, ctypes.c_size_t]),
         "sus2sh_model_edge_kernel_info": (I, [S, P, ctypes.c_char_p, ctypes.c_size_t]),
+        "sus2sh_batch_kernel_info": (I, [S, P, ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

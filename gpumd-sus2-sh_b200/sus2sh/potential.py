@@ -24,7 +24,8 @@ MODEL_INFO_FIELDS = (
     "shared_xi", "product_slots_in_hbm", "cg_jit", "cg_jit_registers", "cg_jit_compile_ms",
     "basic_block", "force_block", "edge_jit", "edge_jit_basic_registers", "edge_jit_force_registers",
     "edge_jit_compile_ms", "gate_mode", "cg_kind", "cg_loaded_registers", "cg_local_bytes", "cg_build",
-    "cg_from_disk_cache",
+    "cg_from_disk_cache", "batch_fused", "batch_fused_registers", "batch_fused_shape", "batch_fused_tile",
+    "batch_fused_compile_ms",
 )
 
 

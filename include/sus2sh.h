@@ -114,7 +114,11 @@ int sus2sh_param_grad(sus2sh_handle* h, int N, const double box_h[9], const int 
  * like sus2sh_compute; cell_energy [ncells] and cell_virial [9 ncells] (NULL
  * to skip) are assigned.  After the first call with a given (N, ncells) the
  * call neither allocates nor synchronises, so it can be captured in a CUDA
- * graph and replayed.  The reference evaluates one box per call
+ * graph and replayed.  With the option sus2_sh_batch_fused=1, FP32 models
+ * with the straight-line CG kernel (no gate, no ZBL) are evaluated by one
+ * persistent kernel instead of the stage kernels (neighbour fill, moments,
+ * CG products, forces, per-cell sums), built with NVRTC and tuned at the
+ * first batch call.  The reference evaluates one box per call
  * (SUS2_SH::compute, src/force/sus2_sh.cu:9620). */
 int sus2sh_compute_batch(sus2sh_handle* h, int N, int ncells, const int* cell_offset,
                          const double* cell_h, const int* cell_pbc, const int* type,
@@ -199,8 +203,14 @@ int sus2sh_cg_energy_noalloc(const sus2sh_handle* h, int N, const int* type, con
  * by nvJitLink: option sus2_sh_cg_whole=0 for component-split kernels)
  * [35] 1 when that program was read from the on-disk cache of one-program
  * builds ($SUS2SH_CACHE_DIR, else $XDG_CACHE_HOME/sus2sh or
- * ~/.cache/sus2sh; SUS2SH_CACHE_DIR=off disables it).  Returns the number
- * written. */
+ * ~/.cache/sus2sh; SUS2SH_CACHE_DIR=off disables it)
+ * [36] 1 when batches run the fused persistent kernel (valid after the first
+ * sus2sh_compute_batch: option sus2_sh_batch_fused=1, FP32 models with the
+ * straight-line CG kernel and model-specialised edge kernels, no gate, no
+ * ZBL) [37] its registers per thread [38] its CTA shape (threads x
+ * 100 + minimum resident CTAs per SM) [39] its tile size in atoms (picked by
+ * timing at the first batch call, or sus2_sh_batch_tile=<atoms>) [40] its
+ * NVRTC compile time (ms).  Returns the number written. */
 int sus2sh_model_info(const sus2sh_handle* h, int* out, int n);
 
 #ifdef __cplusplus

@@ -48,6 +48,16 @@ int sus2sh_edge_kernel_info(int fp32, int l_max, int k_max, int rb, int* basic_r
  * GPU.  No reference counterpart. */
 int sus2sh_model_edge_kernel_info(const char* path, int* info, char* log, size_t log_len);
 
+/* Compiles, as the first sus2sh_compute_batch of an FP32 handle with option
+ * sus2_sh_batch_fused=1 does, the fused persistent batch kernel of a model
+ * file (its radial coefficients and
+ * straight-line CG contraction compiled in; 128-thread CTAs with 3 and with
+ * 2 resident CTAs per SM).  info[0] [1] registers per thread of the two
+ * variants, [2] compile ms, [3] cubin bytes.  An input error for models whose
+ * graph takes the component-split CG kernel.  log (if not NULL) receives the
+ * ptxas report.  Needs no GPU.  No reference counterpart. */
+int sus2sh_batch_kernel_info(const char* path, int* info, char* log, size_t log_len);
+
 /* The engine's real spherical harmonics, evaluated on the host in FP64: Y at
  * the unit vector (x, y, z) for every l <= l_max (l_max <= 6, flat index
  * l*l + l + m) and, when G and V are non-NULL, V = sum_lm G[lm] grad P_lm

@@ -237,3 +237,109 @@ def test_param_grad_batch_equals_sum_over_cells(l3k3_path, batch):
     assert np.abs(gw.cpu().numpy() - sw).max() < 1e-9 * max(1.0, np.abs(sw).max())
     assert np.abs(gc.cpu().numpy() - sc).max() < 1e-9 * max(1.0, np.abs(sc).max())
     pot.close()
+
+
+def _cells(specs, seed):
+    """Concatenated random-insertion cells: specs = [(atoms, density, ratios)]."""
+    cells = [structures.random_insertion(n, rho, 2.1, ratios, seed=seed + k) for k, (n, rho, ratios) in
+             enumerate(specs)]
+    boxes = [c[0] for c in cells]
+    types = np.concatenate([c[1] for c in cells]).astype(np.int32)
+    pos = np.concatenate([c[2] for c in cells], axis=1)
+    off = np.concatenate([[0], np.cumsum([c[1].size for c in cells])]).astype(np.int32)
+    H = np.stack([b.cpu_h.reshape(9) for b in boxes])
+    return off, H, boxes, types, pos
+
+
+@pytest.mark.parametrize("tile", [0, 256])
+def test_fused_batch_kernel_matches_stage_kernels_and_oracle(l3k3_path, batch, tile):
+    """The fused persistent batch kernel (sus2_sh_batch_fused=1) against the
+    stage kernels (the default) on the same batch, and against
+    the oracle cell by cell; tile 256 gives cells of up to 512 atoms
+    several tiles' worth of atoms, so most tiles hold one or two cells."""
+    off, H, boxes, types, pos = batch
+    dev = torch.device("cuda")
+    opts = ["Cu", "Zr", "sus2_sh_batch_fused=1"] + ([f"sus2_sh_batch_tile={tile}"] if tile else [])
+    fused = SUS2_SH(l3k3_path, types.size, opts)
+    stage = SUS2_SH(l3k3_path, types.size, ["Cu", "Zr"])
+    a = _run(fused, off, H, types, pos, dev)
+    b = _run(stage, off, H, types, pos, dev)
+    info, info0 = fused.info(), stage.info()
+    assert info["batch_fused"] == 1 and info0["batch_fused"] == 0
+    if tile:
+        assert info["batch_fused_tile"] == tile
+    fused.close()
+    stage.close()
+    pe, f, w, ce, cw = a
+    # same per-atom arithmetic; forces and virials differ by FP32 summation order
+    assert np.abs(pe - b[0]).max() < 1e-9
+    assert np.sqrt(((f - b[1]) ** 2).mean()) < 1e-6
+    assert np.sqrt(((w - b[2]) ** 2).mean()) < 1e-6
+    assert np.abs(ce - b[3]).max() < 1e-8
+    assert np.abs(cw - b[4]).max() < 1e-5
+    orc = O.Oracle(l3k3_path)
+    for c, box in enumerate(boxes):
+        lo, hi = off[c], off[c + 1]
+        pe0, f0, w0 = orc.efs(box.cpu_h, box.pbc, types[lo:hi], pos[:, lo:hi])
+        assert np.abs(pe[lo:hi] - pe0).max() < 1e-6
+        assert np.sqrt(((f[:, lo:hi] - f0) ** 2).mean()) < 1e-5
+        assert np.sqrt(((w[:, lo:hi] - w0) ** 2).mean()) < 1e-5
+        assert abs(ce[c] - pe0.sum()) < 1e-6 * (hi - lo)
+
+
+def test_fused_batch_kernel_large_and_tiny_cells(l3k3_path):
+    """Tiles whose atoms exceed the shared-memory force buffer (a 1,700-atom
+    cell at tile 256: buffer of 1,536 atoms) take the FP64-atomic path; cells
+    of one to three atoms (no neighbour within the cutoff) and an empty cell
+    get their sums; outputs accumulate into non-zero arrays and the per-cell
+    sums are assigned, as in the stage path; two calls in a row agree."""
+    off, H, boxes, types, pos = _cells([(40, 0.06, (1.0, 1.0, 1.0)), (1700, 0.06, (1.0, 1.1, 0.9)),
+                                        (300, 0.06, (1.2, 1.0, 1.0))], seed=71)
+    # cells of 1, 3 and 0 atoms: 20 A cubes
+    tiny = [np.zeros((3, 1)) + 3.0, np.array([[1.0, 8.0, 15.0], [2.0, 2.0, 9.0], [3.0, 14.0, 3.0]]),
+            np.zeros((3, 0))]
+    for p in tiny:
+        boxes.append(Box.orthorhombic(20.0, 20.0, 20.0))
+        H = np.vstack([H, boxes[-1].cpu_h.reshape(1, 9)])
+        types = np.concatenate([types, np.arange(p.shape[1], dtype=np.int32) % 2])
+        pos = np.concatenate([pos, p], axis=1)
+        off = np.concatenate([off, [off[-1] + p.shape[1]]]).astype(np.int32)
+    N, ncells = types.size, off.size - 1
+    dev = torch.device("cuda")
+    fused = SUS2_SH(l3k3_path, N, ["Cu", "Zr", "sus2_sh_batch_fused=1", "sus2_sh_batch_tile=256"])
+    stage = SUS2_SH(l3k3_path, N, ["Cu", "Zr"])
+    rng = np.random.default_rng(5)
+    start = [rng.normal(size=N), rng.normal(size=3 * N), rng.normal(size=9 * N)]
+    outs = []
+    for pot in (fused, fused, stage):
+        t = torch.as_tensor(types, device=dev)
+        x = torch.as_tensor(pos.reshape(-1).copy(), device=dev)
+        o = torch.as_tensor(off, device=dev)
+        h = torch.as_tensor(H.reshape(-1).copy(), device=dev)
+        pe, f, w = (torch.as_tensor(v, device=dev) for v in start)
+        ce = torch.full((ncells,), 7.0, dtype=torch.float64, device=dev)
+        cw = torch.full((9 * ncells,), 7.0, dtype=torch.float64, device=dev)
+        pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce, cell_virial=cw)
+        torch.cuda.synchronize()
+        assert pot.sync() == 0
+        outs.append([v.cpu().numpy() for v in (pe, f, w, ce, cw)])
+    assert fused.info()["batch_fused"] == 1
+    fused.close()
+    stage.close()
+    (pe1, f1, w1, ce1, cw1), (pe2, f2, w2, ce2, cw2), (pe0, f0, w0, ce0, cw0) = outs
+    assert np.array_equal(pe1, pe2) and np.array_equal(ce1, ce2)
+    assert np.abs(pe1 - pe0).max() < 1e-9
+    assert np.sqrt(((f1 - f0) ** 2).mean()) < 1e-6 and np.sqrt(((f2 - f0) ** 2).mean()) < 1e-6
+    assert np.sqrt(((w1 - w0) ** 2).mean()) < 1e-6
+    assert np.abs(ce1 - ce0).max() < 1e-8 and np.abs(cw1 - cw0).max() < 1e-5
+    assert ce1[-1] == 0.0 and (cw1[-9:] == 0.0).all()  # the empty cell
+    # the isolated atoms' site energies are the species terms alone
+    orc = O.Oracle(l3k3_path)
+    for c in range(ncells):
+        lo, hi = off[c], off[c + 1]
+        if hi == lo:
+            continue
+        pe_o, f_o, _ = orc.efs(boxes[c].cpu_h, boxes[c].pbc, types[lo:hi], pos[:, lo:hi])
+        assert np.abs(pe1[lo:hi] - start[0][lo:hi] - pe_o).max() < 1e-6
+        fd = f1.reshape(3, N)[:, lo:hi] - start[1].reshape(3, N)[:, lo:hi]
+        assert np.sqrt(((fd - f_o) ** 2).mean()) < 1e-5

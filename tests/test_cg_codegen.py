@@ -38,6 +38,25 @@ def test_l3k3_cg_kernel_compiles_without_spills(l3k3_path):
     assert info["cubin"] > 0
 
 
+def test_fused_batch_kernel_compiles_without_spills(l3k3_path, l4k4_path):
+    """The fused persistent batch kernel of the l3k3 model (moments, the
+    straight-line CG contraction and the force loop in one kernel) builds
+    without a GPU: the 3-CTA-per-SM variant stays within 170 registers and
+    neither variant spills.  A graph that takes the component-split CG kernel
+    has no fused kernel (its batches always run the stage kernels)."""
+    lib = _lib.load()
+    info = (ctypes.c_int * 4)()
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = lib.sus2sh_batch_kernel_info(l3k3_path.encode(), info, log, len(log))
+    assert rc == 0, lib.sus2sh_last_error().decode()
+    assert 0 < info[0] <= 170 and 0 < info[1] <= 255 and info[3] > 0
+    text = log.value.decode()
+    assert len(re.findall(r"Compiling entry function '\w*k_batch_fused", text)) == 2
+    assert "bytes spill stores" in text and not re.search(r"[1-9]\d* bytes spill stores", text), text
+    rc = lib.sus2sh_batch_kernel_info(l4k4_path.encode(), info, None, 0)
+    assert rc == -1 and "component-split" in lib.sus2sh_last_error().decode()
+
+
 def test_large_graph_gets_the_split_kernel(l4k4_path):
     # l4k4 body 5: 33,389 products in 116 (rank L, component M) components
     # (split=3: the parallel relocatable build, seconds instead of the

@@ -7,7 +7,7 @@ around the cutoff (or everything beyond a coordinate limit) to the FP64 test:
   corner (FP64 test beyond kRelLimit) plus an FP32 cell-to-cell offset (FP64
   test beyond kOffLimit); in below cutoff2 - m, out above cutoff2 + m, with
   m = 0.01 + 1e-3 cutoff2 A^2;
-* batch cells wider than twice the cutoff (`k_batch_fill_ortho`, batch.cu):
+* batch cells wider than twice the cutoff (`fill_cell_ortho`, batch_fill.cuh):
   FP32 positions relative to the cell's first atom, nearest image by rounding,
   the same band;
 * narrower batch cells: a nearest-image pre-test and per-axis image ranges
@@ -40,7 +40,7 @@ def _const(fname, name):
 
 K_REL = _const("engine.cu", "kRelLimit")
 K_OFF = _const("engine.cu", "kOffLimit")
-K_COMPACT = _const("batch.cu", "kCompact")
+K_COMPACT = _const("batch_fill.cuh", "kCompact")
 
 
 def fma(a, b, c):

@@ -1,8 +1,8 @@
 """sus2sh_cg_energy_noalloc: the CG product stage without device allocation.
 
 This entry point serves callers that cannot call cudaMalloc when they need
-the contraction (inside a stream capture, or under an MD code's fixed memory
-pool).  It is checked through the C-ABI against the regular entry point
+the contraction (an MD code that holds all device memory in its own fixed
+pool and forbids allocation during a run).  It is checked through the C-ABI against the regular entry point
 sus2sh_forward on the same structure, on two calls in a row (the second call
 reuses the fixed work area the first one left behind), and its adjoints
 against the FP64 oracle.  The file is named so that pytest collects it last.
