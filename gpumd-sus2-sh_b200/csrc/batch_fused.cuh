@@ -160,15 +160,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batch_fused(const EdgeArgs<floa
     }
     __syncthreads();  // the buffer and s_tile are free for the next tile
   }
-  // the last CTA to leave resets the counter for the next launch (every CTA
-  // has drawn its final ticket before it counts itself out)
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(f.tile_counter + 1, 1) == static_cast<int>(gridDim.x) - 1) {
-      f.tile_counter[0] = 0;
-      f.tile_counter[1] = 0;
-    }
-  }
 }
 
 }  // namespace batch

@@ -918,8 +918,7 @@ struct Engine {
         mods.push_back(std::move(mod));
       }
       cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
-      d_tile_ctr.resize(2);
-      ck(cudaMemset(d_tile_ctr.p, 0, 2 * sizeof(int)), "memset");
+      d_tile_ctr.resize(1);
       fused_mods = std::move(mods);
       fused_compile_ms = bin->compile_ms;
       fused_bin = bin;
@@ -973,6 +972,7 @@ struct Engine {
     const unsigned grid = static_cast<unsigned>(std::min<long long>(f.ntiles, static_cast<long long>(per_sm) * sm_count));
     void* args[] = {&a, &f};
     std::string err;
+    ck(cudaMemsetAsync(d_tile_ctr.p, 0, sizeof(int), s), "memset");
     if (!mod.launch_args(s, grid, static_cast<unsigned>(block), smem, args, &err)) throw CudaError(err);
     launches += 1;
   }

@@ -85,7 +85,7 @@ struct FusedArgs {
   double* virial;                // [9][N], accumulated (may be NULL)
   double* cell_energy;           // [ncells], assigned (may be NULL)
   double* cell_virial;           // [9 ncells], assigned (may be NULL)
-  int* tile_counter;             // [2]: next tile, CTAs done; zero between launches
+  int* tile_counter;             // next tile to draw; zeroed before every launch
   // fill = 1: each tile first builds its cells' neighbour lists (the batch
   // fill of batch_fill.cuh, into nbr / ncount with capacity cap, cutoff^2
   // cutoff2, status flags in st); 0: the lists are already built
