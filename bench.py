@@ -226,6 +226,7 @@ def run_md(torch, path, box, types, pos, vel, masses, steps, warmup, fp64, world
     flags = pot.sync()
     if flags:
         raise RuntimeError(f"neighbour list status {flags} during timed steps")
+    timed_frame = md.pos.clone()  # the final frame of the timed steps (accuracy, CPU baseline, e2e)
     clk = None
     if clocks:
         # a timed region of a few tens of ms ends before nvidia-smi's first
@@ -243,7 +244,7 @@ def run_md(torch, path, box, types, pos, vel, masses, steps, warmup, fp64, world
     if world > 1:
         torch.distributed.barrier()
     ms = s.elapsed_time(e)
-    return pot, md, ms, prof, launches, clk
+    return pot, md, ms, prof, launches, clk, timed_frame
 
 
 def force_error_vs_fp64(torch, path, box, types, x_dev):
@@ -573,17 +574,17 @@ def main():
         path, box, types, pos, vel, masses = make_workload(d, rank)
         N = types.size
         clocks = ClockSampler(local)
-        pot, md, ms, prof, launches, clk = run_md(torch, path, box, types, pos, vel, masses, args.steps,
+        pot, md, ms, prof, launches, clk, frame = run_md(torch, path, box, types, pos, vel, masses, args.steps,
                                                   args.warmup, False, world, clocks)
         # FP64 engine on the same workload
         pot64 = md64 = None
         ms64 = None
         if args.fp64_steps > 0:
-            pot64, md64, ms64, prof64, _, _ = run_md(torch, path, box, types, pos, vel, masses, args.fp64_steps,
+            pot64, md64, ms64, prof64, _, _, _ = run_md(torch, path, box, types, pos, vel, masses, args.fp64_steps,
                                                      min(args.warmup, 3), True, world)
-        frms, de, de_total, final32 = force_error_vs_fp64(torch, path, box, types, md.pos)
-        final_pos = md.pos.view(3, N).cpu().numpy()
-        e2e_val, h2d, d2h = e2e_run(torch, pot, box, types, md.pos, args.e2e_steps)
+        frms, de, de_total, final32 = force_error_vs_fp64(torch, path, box, types, frame)
+        final_pos = frame.view(3, N).cpu().numpy()
+        e2e_val, h2d, d2h = e2e_run(torch, pot, box, types, frame, args.e2e_steps)
         ms_max, ms64_max, inv_e2e = max_over_ranks(torch, [ms, ms64 or 0.0, 1.0 / max(e2e_val, 1e-30)], world,
                                                    "cuda")
         if rank == 0:
