@@ -640,7 +640,16 @@ def main():
             }
             if world == 1 and not args.no_extra:
                 line["batch_cells"] = batch_cells_run(torch, path)
-                line["large_model"] = large_model_run(torch, d)
+                line["large_model"] = lm = large_model_run(torch, d)
+                # the component-split CG kernel against the FP32 peak: the
+                # counting rule's 9 flop per product (3 forward, 6 reverse)
+                prod_ms = lm["stage_ms_per_eval"].get("product_ms", 0.0)
+                if prod_ms > 0 and fp32_peak > 0:
+                    tf = lm["atoms"] * 9 * 33389 / (prod_ms * 1e-3) / 1e12
+                    lm["product_roofline"] = {"kernel": "component-split CG kernel", "bound": "fp32",
+                                              "achieved": tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                                              "frac": tf / fp32_peak,
+                                              "flop_rule": "9 per product per atom (33,389 products)"}
             if world == 1 and not args.no_cpu_baseline:
                 line["cpu_baseline"], acc_oracle = cpu_baseline_leg(path, box, types, final_pos, final32)
                 line["accuracy"].update(acc_oracle)
