@@ -343,3 +343,42 @@ def test_fused_batch_kernel_large_and_tiny_cells(l3k3_path):
         assert np.abs(pe1[lo:hi] - start[0][lo:hi] - pe_o).max() < 1e-6
         fd = f1.reshape(3, N)[:, lo:hi] - start[1].reshape(3, N)[:, lo:hi]
         assert np.sqrt(((fd - f_o) ** 2).mean()) < 1e-5
+
+
+@pytest.mark.parametrize("fused", [False, True], ids=["stage", "fused"])
+def test_batch_neighbor_overflow_is_reported_and_recovered(l3k3_path, fused):
+    """The lists are sized at the first call of a given (N, ncells); a later
+    call whose cells are compressed has more neighbours than they hold.  The
+    fill (the stage kernels', or the fused kernel's own) stops at the
+    capacity, sus2sh_sync reports the overflow and grows the lists, and the
+    next call matches the oracle."""
+    off, H, boxes, types, pos = _cells([(150, 0.03, (1.0, 1.0, 1.0)), (120, 0.03, (1.1, 1.0, 0.9))], seed=81)
+    N, ncells = types.size, off.size - 1
+    dev = torch.device("cuda")
+    pot = SUS2_SH(l3k3_path, N, ["Cu", "Zr"] + (["sus2_sh_batch_fused=1"] if fused else []))
+    t = torch.as_tensor(types, device=dev)
+    o = torch.as_tensor(off, device=dev)
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def call(scale):
+        h = torch.as_tensor((H * scale).reshape(-1).copy(), device=dev)
+        x = torch.as_tensor((pos * scale).reshape(-1).copy(), device=dev)
+        pe, f, w, ce = z(N), z(3 * N), z(9 * N), z(ncells)
+        pot.compute_batch(o, h, t, x, pe, f, w, cell_energy=ce)
+        torch.cuda.synchronize()
+        return pot.sync(), pe.cpu().numpy(), ce.cpu().numpy()
+
+    assert call(1.0)[0] == 0
+    assert call(0.75)[0] & 1  # overflow flagged, capacity grown
+    flags, pe, ce = call(0.75)
+    assert flags == 0
+    assert pot.info()["batch_fused"] == (1 if fused else 0)
+    pot.close()
+    orc = O.Oracle(l3k3_path)
+    for c in range(ncells):
+        lo, hi = off[c], off[c + 1]
+        pe0, _, _ = orc.efs(boxes[c].cpu_h * 0.75, boxes[c].pbc, types[lo:hi], pos[:, lo:hi] * 0.75)
+        scale = max(1.0, np.abs(pe0).max())
+        # (FP32 bars relative to the site energies of this compressed packing)
+        assert np.abs(pe[lo:hi] - pe0).max() < 1e-5 * scale
+        assert abs(ce[c] - pe0.sum()) < 1e-5 * scale * (hi - lo)
