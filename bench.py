@@ -604,7 +604,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded 80x80x40 FCC Cu-Zr 64/36, MB velocities 200 K; seeded random l3k3 model)",
-                "config": {"workload": "1.024M-atom l3k3 Cu-Zr NVE MD, FP32 engine", "atoms_per_gpu": N,
+                "config": {"workload": (f"{N / 1e6:.3f}M-atom" if N != 1024000 else "1.024M-atom")
+                                       + " l3k3 Cu-Zr NVE MD, FP32 engine", "atoms_per_gpu": N,
                            "dt_fs": DT, "skin_A": SKIN, "rebuild_every": REBUILD, "rc_A": pot.rc,
                            "model": "SUS2-SH L3 K3 body4 rb8 (248 moments, 806 products)",
                            "l2": "inputs larger than L2 (positions+neighbour list+moments > 126 MB)",
